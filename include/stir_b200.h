@@ -1,0 +1,189 @@
+/*
+ * stir_b200.h -- C ABI of the B200 ray-tracing projector pair and OSMAPOSL
+ * sub-iteration for STIR.
+ *
+ * This is the drop-in boundary a STIR plug-in (a ProjectorByBinPair
+ * registered under its own parsing keyword) binds to.  Every entry point uses
+ * plain pointers, sizes and status codes; no C++ or torch type crosses it.
+ *
+ * Conventions
+ *  - Every function returns B200RT_OK (0) or a negative status.  The message
+ *    of the last failure on a handle is returned by b200rt_last_error().
+ *  - Geometry follows STIR: projection data ProjDataInfoCylindrical{NoArcCorr,
+ *    ArcCorr} built from Scanner parameters (src/buildblock/ProjDataInfo.cxx),
+ *    images VoxelsOnCartesianGrid (src/buildblock/VoxelsOnCartesianGrid.cxx),
+ *    matrix ProjMatrixByBinUsingRayTracing
+ *    (src/recon_buildblock/ProjMatrixByBinUsingRayTracing.cxx).
+ *  - Host arrays use STIR's own memory order:
+ *      image       [z][y][x], x fastest (Array<3,float> of VoxelsOnCartesianGrid)
+ *      projdata    ProjDataInMemory order: segment 0,+1,-1,+2,-2,... then
+ *                  axial position, view, tangential position (tangential fastest)
+ *                  (src/buildblock/ProjDataInMemory.cxx:190-235,
+ *                   src/buildblock/ProjData.cxx:641-661)
+ *  - Device arrays passed to the *_dev entry points use the device layout:
+ *      image       [y][x][z], z fastest ("z-columns")
+ *      projdata    [segment][view][tangential][axial], axial fastest
+ *                  (segments in the order -S..+S)
+ *    b200rt_image_to_device_layout() and friends convert between the two.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ */
+#ifndef STIR_B200_H
+#define STIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200RT_ABI_VERSION 1
+#define B200RT_MAX_SEGMENTS 255
+
+/* status codes */
+#define B200RT_OK 0
+#define B200RT_ERR_INVALID_ARGUMENT (-1)
+#define B200RT_ERR_UNSUPPORTED (-2)
+#define B200RT_ERR_CUDA (-3)
+#define B200RT_ERR_OUT_OF_MEMORY (-4)
+#define B200RT_ERR_STATE (-5)
+#define B200RT_ERR_TIMEOUT (-6)
+#define B200RT_ERR_TOO_LARGE (-7)
+
+/* back-projection accumulation modes */
+#define B200RT_BACKPROJECT_ATOMIC 0        /* scatter with float atomics (fast)        */
+#define B200RT_BACKPROJECT_DETERMINISTIC 1 /* voxel-driven gather, fixed summation order */
+
+/* priors (src/recon_buildblock/QuadraticPrior.cxx, RelativeDifferencePrior.cxx) */
+#define B200RT_PRIOR_NONE 0
+#define B200RT_PRIOR_QUADRATIC 1
+#define B200RT_PRIOR_RELATIVE_DIFFERENCE 2
+
+/* OSMAPOSL MAP models (src/iterative/OSMAPOSL/OSMAPOSLReconstruction.cxx:415-456) */
+#define B200RT_MAP_ADDITIVE 0
+#define B200RT_MAP_MULTIPLICATIVE 1
+
+/*
+ * Geometry descriptor: the primary parameters from which STIR derives every
+ * projector quantity.  Derived values (azimuthal sampling/offset, m offsets,
+ * tan(theta), symmetry tables ...) are computed by the library with STIR's own
+ * float arithmetic.
+ */
+typedef struct b200rt_geometry {
+  /* Scanner (src/include/stir/Scanner.h) */
+  int32_t num_rings;
+  int32_t num_detectors_per_ring;
+  float inner_ring_radius_mm;
+  float average_depth_of_interaction_mm;
+  float ring_spacing_mm;
+  float default_bin_size_mm;
+  float intrinsic_azimuthal_tilt_rad;
+  float timing_resolution_ps;  /* TOF: coincidence timing FWHM, 0 for non-TOF */
+  float size_of_timing_pos_ps; /* TOF: width of one unmashed timing position   */
+  int32_t max_num_timing_poss; /* TOF: number of unmashed timing positions      */
+  /* ProjDataInfoCylindrical (src/include/stir/ProjDataInfoCylindrical.h) */
+  int32_t arc_corrected;      /* 0: NoArcCorr (s = R sin(t*pi/ndet)), 1: ArcCorr (s = t*bin) */
+  float arccorr_bin_size_mm;  /* only for arc_corrected */
+  int32_t num_views;
+  int32_t num_tangential_poss;
+  int32_t max_segment_num;    /* segments -max..+max */
+  int32_t tof_mash_factor;    /* 0: non-TOF data; >0: TOF data with this mashing */
+  int32_t min_ring_diff[B200RT_MAX_SEGMENTS]; /* index: segment + max_segment_num */
+  int32_t max_ring_diff[B200RT_MAX_SEGMENTS];
+  int32_t num_axial_poss[B200RT_MAX_SEGMENTS];
+  /* VoxelsOnCartesianGrid (src/include/stir/VoxelsOnCartesianGrid.h) */
+  int32_t nz, ny, nx;
+  int32_t min_z, min_y, min_x; /* first index of each dimension */
+  float voxel_size_z, voxel_size_y, voxel_size_x;
+  float origin_z, origin_y, origin_x;
+  /* ProjMatrixByBinUsingRayTracing keys (ProjMatrixByBinUsingRayTracing.cxx:75-104) */
+  int32_t num_tangential_LORs;
+  int32_t restrict_to_cylindrical_FOV;
+  int32_t do_symmetry_90degrees_min_phi;
+  int32_t do_symmetry_180degrees_min_phi;
+  int32_t do_symmetry_swap_segment;
+  int32_t do_symmetry_swap_s;
+  int32_t do_symmetry_shift_z;
+} b200rt_geometry;
+
+/* sizes and statistics of a set-up projector */
+typedef struct b200rt_info {
+  int64_t num_bins;          /* projection-data elements (all TOF bins)          */
+  int64_t num_image_voxels;  /* nz*ny*nx                                         */
+  int64_t num_basic_bins;    /* rows traced (STIR's basic bins)                  */
+  int64_t num_row_elements;  /* stored elements of all basic rows                */
+  int64_t total_nnz;         /* sum over all bins of their row length            */
+  int32_t num_tof_bins;      /* 1 for non-TOF                                    */
+  int32_t num_basic_views;
+  int32_t symmetries_used;   /* bit 0: 90-phi, 1: 180-phi, 2: swap seg, 3: swap s, 4: shift z */
+  int32_t reserved;
+} b200rt_info;
+
+typedef struct b200rt_prior {
+  int32_t type;              /* B200RT_PRIOR_*                                   */
+  float penalisation_factor; /* beta                                             */
+  float gamma;               /* RDP gamma (STIR default 2)                       */
+  float epsilon;             /* RDP epsilon (STIR default 0)                     */
+  int32_t only_2D;           /* 1: 3x3 in-plane neighbourhood only               */
+  int32_t map_model;         /* B200RT_MAP_*                                     */
+  const float* kappa_dev;    /* optional kappa image (device layout) or NULL     */
+} b200rt_prior;
+
+typedef struct b200rt_projector b200rt_projector;
+
+/* ---- life cycle --------------------------------------------------------- */
+
+/* ProjectorByBinPair::set_up (src/include/stir/recon_buildblock/ProjectorByBinPair.h:60)
+ * together with ProjMatrixByBinUsingRayTracing::set_up
+ * (src/recon_buildblock/ProjMatrixByBinUsingRayTracing.cxx:238-407): validates the
+ * geometry with STIR's rules, derives the symmetry tables and traces every
+ * basic row on `device` (STIR's basic-bin cache, ProjMatrixByBin.inl:48-113). */
+int b200rt_create(const b200rt_geometry* geometry, int device, b200rt_projector** out);
+void b200rt_destroy(b200rt_projector* h);
+/* message of the last failure on h (or of the last failed b200rt_create if h is NULL) */
+const char* b200rt_last_error(const b200rt_projector* h);
+int b200rt_get_info(const b200rt_projector* h, b200rt_info* out);
+/* size in elements of projection data / image for this geometry */
+int64_t b200rt_projdata_size(const b200rt_projector* h);
+int64_t b200rt_image_size(const b200rt_projector* h);
+
+/* One basic row (ProjMatrixByBin::get_proj_matrix_elems_for_one_bin,
+ * src/include/stir/recon_buildblock/ProjMatrixByBin.inl:48-113) of bin
+ * (segment, view, axial, tangential, timing): copies up to `capacity` elements
+ * as (z,y,x) triples and values into host arrays; returns the row length
+ * through *length.  Used by tests to compare rows with STIR's. */
+int b200rt_get_row(b200rt_projector* h, int segment, int view, int axial, int tangential, int timing,
+                   int32_t* coords_zyx, float* values, int64_t capacity, int64_t* length);
+
+/* ---- layout conversion (device to device) ------------------------------- */
+int b200rt_image_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream);
+int b200rt_image_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream);
+int b200rt_projdata_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream);
+int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream);
+
+/* ---- projectors on device-resident data (device layouts) ---------------- */
+
+/* ForwardProjectorByBin::forward_project(ProjData&, image, subset_num, num_subsets, zero)
+ * (src/include/stir/recon_buildblock/ForwardProjectorByBin.h:108): writes the
+ * bins of the views in subset `subset_num` of `num_subsets`
+ * (detail::find_basic_vs_nums_in_subset, find_basic_vs_nums_in_subset.cxx:32-70);
+ * num_subsets=1 projects everything.  Bins of other subsets are left as they are. */
+int b200rt_forward_project_dev(b200rt_projector* h, const float* image_dev, float* projdata_dev,
+                               int subset_num, int num_subsets, void* stream);
+
+/* BackProjectorByBin::back_project(image, const ProjData&, subset_num, num_subsets)
+ * (src/include/stir/recon_buildblock/BackProjectorByBin.h:111): image_dev is
+ * overwritten with A^T of the subset's bins. */
+int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, float* image_dev,
+                            int subset_num, int num_subsets, int mode, void* stream);
+
+/* ---- projectors on host arrays in STIR order (copies included) ---------- */
+int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host,
+                           int subset_num, int num_subsets);
+int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* image_host,
+                        int subset_num, int num_subsets, int mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STIR_B200_H */

@@ -1,0 +1,234 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so) and of oracle/_ref.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, as the checker.  The product
+(stir_b200) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from stir_b200 import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_raytrace.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_F = ctypes.c_float
+
+
+def build():
+    """Compile liboracle.so (and oracle/_ref when STIR's sources are present)."""
+    subprocess.run(["make", "-C", HERE, "-s", "all"], check=True)
+
+
+def _load():
+    if not os.path.exists(LIB):
+        build()
+    lib = ctypes.CDLL(LIB)
+    sig = {
+        "or_create": (_P, [ctypes.POINTER(_abi.Geometry), _I, ctypes.c_char_p, _I]),
+        "or_destroy": (None, [_P]),
+        "or_projdata_size": (_I64, [_P]),
+        "or_image_size": (_I64, [_P]),
+        "or_num_tof_bins": (_I, [_P]),
+        "or_symmetries_used": (_I, [_P]),
+        "or_num_basic_views": (_I, [_P]),
+        "or_get_row": (_I64, [_P, _I, _I, _I, _I, _I, _P, _P, _I64]),
+        "or_total_nnz": (_I64, [_P, _I]),
+        "or_basic_row_elements": (_I64, [_P, _I, ctypes.POINTER(_I64)]),
+        "or_forward_project_f32": (_I, [_P, _P, _P, _I, _I, _I]),
+        "or_back_project_f32": (_I, [_P, _P, _P, _I, _I, _I]),
+        "or_forward_project_f64": (_I, [_P, _P, _P, _I, _I, _I]),
+        "or_back_project_f64": (_I, [_P, _P, _P, _I, _I, _I]),
+        "or_sensitivity_f32": (_I, [_P, _P, _P, _I, _I, _I, _I]),
+        "or_osmaposl_update_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F, _I,
+                                        ctypes.POINTER(_I)]),
+        "or_log_likelihood_f32": (_D, [_P, _P, _P, _P, _P, _I, _I, _I, _I]),
+        "or_prior_gradient_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+        "or_prior_value_f32": (_D, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F]),
+        "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def default_threads():
+    return os.cpu_count() or 1
+
+
+class Oracle:
+    """CPU restatement of STIR's ray-tracing projector pair for one geometry."""
+
+    def __init__(self, geometry: _abi.Geometry, precision: int = 32):
+        self.precision = precision
+        err = ctypes.create_string_buffer(512)
+        self.h = lib().or_create(ctypes.byref(geometry), precision, err, 512)
+        if not self.h:
+            raise ValueError(f"oracle geometry rejected: {err.value.decode()}")
+        self.geometry = geometry
+        self.dtype = np.float64 if precision == 64 else np.float32
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().or_destroy(h)
+            self.h = None
+
+    @property
+    def projdata_size(self):
+        return lib().or_projdata_size(self.h)
+
+    @property
+    def image_shape(self):
+        g = self.geometry
+        return (g.nz, g.ny, g.nx)
+
+    @property
+    def symmetries_used(self):
+        return lib().or_symmetries_used(self.h)
+
+    @property
+    def num_tof_bins(self):
+        return lib().or_num_tof_bins(self.h)
+
+    def row(self, seg, view, ax, tang, tof=0, capacity=1 << 16):
+        c = np.zeros((capacity, 3), np.int32)
+        v = np.zeros(capacity, np.float64)
+        n = lib().or_get_row(self.h, seg, view, ax, tang, tof, _ptr(c), _ptr(v), capacity)
+        if n < 0:
+            raise RuntimeError("oracle row failed")
+        n = min(n, capacity)
+        return c[:n].copy(), v[:n].copy()
+
+    def total_nnz(self, nthreads=None):
+        return lib().or_total_nnz(self.h, nthreads or default_threads())
+
+    def basic_row_elements(self, nthreads=None):
+        n = _I64(0)
+        e = lib().or_basic_row_elements(self.h, nthreads or default_threads(), ctypes.byref(n))
+        return n.value, e
+
+    def forward(self, image, subset=0, nsub=1, nthreads=None, out=None):
+        image = np.ascontiguousarray(image, self.dtype).reshape(self.image_shape)
+        pd = np.zeros(self.projdata_size, self.dtype) if out is None else out
+        f = lib().or_forward_project_f64 if self.precision == 64 else lib().or_forward_project_f32
+        if f(self.h, _ptr(image), _ptr(pd), subset, nsub, nthreads or default_threads()) != 0:
+            raise RuntimeError("oracle forward projection failed")
+        return pd
+
+    def back(self, projdata, subset=0, nsub=1, nthreads=None):
+        projdata = np.ascontiguousarray(projdata, self.dtype).ravel()
+        img = np.zeros(self.image_shape, self.dtype)
+        f = lib().or_back_project_f64 if self.precision == 64 else lib().or_back_project_f32
+        if f(self.h, _ptr(projdata), _ptr(img), subset, nsub, nthreads or default_threads()) != 0:
+            raise RuntimeError("oracle back projection failed")
+        return img
+
+    def sensitivity(self, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False, nthreads=None):
+        m = None if mult is None else np.ascontiguousarray(mult, np.float32).ravel()
+        img = np.zeros(self.image_shape, np.float32)
+        if lib().or_sensitivity_f32(self.h, _ptr(m), _ptr(img), subset, nsub, int(zero_seg0_end_planes),
+                                    nthreads or default_threads()) != 0:
+            raise RuntimeError("oracle sensitivity failed")
+        return img
+
+    def osmaposl_update(self, estimate, y, additive, sens, subset, nsub, subiteration_num, prior=None, kappa=None,
+                        min_rel=0.0, max_rel=1e37, zero_seg0_end_planes=False, nthreads=None):
+        x = np.ascontiguousarray(estimate, np.float32).copy().reshape(self.image_shape)
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+        s = np.ascontiguousarray(sens, np.float32).ravel()
+        k = None if kappa is None else np.ascontiguousarray(kappa, np.float32).ravel()
+        p = prior if prior is not None else _abi.Prior(type=_abi.PRIOR_NONE)
+        cancelled = ctypes.c_int(0)
+        st = lib().or_osmaposl_update_f32(self.h, _ptr(x), _ptr(y), _ptr(a), _ptr(s), subset, nsub, subiteration_num,
+                                          int(zero_seg0_end_planes), ctypes.byref(p), _ptr(k), float(min_rel),
+                                          float(max_rel), nthreads or default_threads(), ctypes.byref(cancelled))
+        if st != 0:
+            raise RuntimeError("oracle OSMAPOSL update failed")
+        return x, cancelled.value
+
+    def log_likelihood(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
+                       nthreads=None):
+        x = np.ascontiguousarray(image, np.float32).ravel()
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+        m = None if mult is None else np.ascontiguousarray(mult, np.float32).ravel()
+        return lib().or_log_likelihood_f32(self.h, _ptr(x), _ptr(y), _ptr(a), _ptr(m), subset, nsub,
+                                           int(zero_seg0_end_planes), nthreads or default_threads())
+
+
+def prior_gradient(prior: _abi.Prior, image, voxel_size, kappa=None):
+    image = np.ascontiguousarray(image, np.float32)
+    nz, ny, nx = image.shape
+    g = np.zeros_like(image)
+    k = None if kappa is None else np.ascontiguousarray(kappa, np.float32)
+    lib().or_prior_gradient_f32(ctypes.byref(prior), _ptr(image), _ptr(k), nz, ny, nx, *map(float, voxel_size), _ptr(g))
+    return g
+
+
+def prior_value(prior: _abi.Prior, image, voxel_size, kappa=None):
+    image = np.ascontiguousarray(image, np.float32)
+    nz, ny, nx = image.shape
+    k = None if kappa is None else np.ascontiguousarray(kappa, np.float32)
+    return lib().or_prior_value_f32(ctypes.byref(prior), _ptr(image), _ptr(k), nz, ny, nx, *map(float, voxel_size))
+
+
+def ray_trace(start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity=1 << 14):
+    """Oracle restatement of RayTraceVoxelsOnCartesianGrid."""
+    return _trace(lib().or_ray_trace, start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity)
+
+
+def _trace(fn, start, stop, vox, norm_const, capacity):
+    s = np.asarray(start, np.float32)
+    e = np.asarray(stop, np.float32)
+    v = np.asarray(vox, np.float32)
+    c = np.zeros((capacity, 3), np.int32)
+    val = np.zeros(capacity, np.float32)
+    n = fn(_ptr(s), _ptr(e), _ptr(v), float(norm_const), _ptr(c), _ptr(val), capacity)
+    if n < 0:
+        raise RuntimeError("capacity exceeded")
+    return c[:n].copy(), val[:n].copy()
+
+
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def ref_ray_trace(start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity=1 << 14):
+    """STIR's own RayTraceVoxelsOnCartesianGrid, compiled from the STIR tree into oracle/_ref."""
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_LIB)
+        _ref.ref_ray_trace.restype = _I64
+        _ref.ref_ray_trace.argtypes = [_P, _P, _P, _F, _P, _P, _I64]
+    return _trace(_ref.ref_ray_trace, start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity)

@@ -1,0 +1,609 @@
+// C ABI of the B200 ray-tracing projector pair (include/stir_b200.h).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/stir_b200.h"
+#include "geometry.hpp"
+#include "internal.hpp"
+
+namespace b200 {
+size_t projector_smem_bytes(const ProjParams& p);
+}
+
+using namespace b200;
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const std::string& where)
+      : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
+};
+inline void ck(cudaError_t e, const char* where) {
+  if (e != cudaSuccess) throw CudaError(e, where);
+}
+
+template <typename T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() {}
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  void upload(const std::vector<T>& v, cudaStream_t st) {
+    alloc(v.size());
+    if (!v.empty()) ck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+  }
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) ck(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct b200rt_projector {
+  std::unique_ptr<Geometry> geo;
+  int device = 0;
+  std::string err;
+  // device tables
+  DevBuf<RowElem> rows;
+  DevBuf<ProjBinDev> bins;
+  DevBuf<LineDev> lines;
+  DevBuf<SegDev> segs;
+  ProjParams params{};
+  // host copies
+  std::vector<ProjBinDev> h_bins;
+  std::vector<int> h_bin_view;  // basic view of each bin
+  std::vector<int> h_bin_seg;
+  std::map<long long, int> bin_index;  // (view, seg, tang, tof) -> bin
+  int64_t total_nnz = 0;
+  int num_basic_views = 0;
+  // subset work lists
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf<int>>> subset_lists;
+  std::map<std::pair<int, int>, int> subset_counts;
+  // staging for the host API
+  DevBuf<float> st_img_a, st_img_b, st_pd_a, st_pd_b;
+  cudaStream_t stream = nullptr;
+
+  long long bin_key(int view, int seg, int tang, int tof) const {
+    const Geometry& g = *geo;
+    return ((static_cast<long long>(view) * (2 * g.S() + 1) + (seg + g.S())) * 4096 + (tang + 2048)) * 1024 + (tof + 512);
+  }
+};
+
+namespace {
+
+int fail(b200rt_projector* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int status_of(const std::exception& e) {
+  if (auto* ce = dynamic_cast<const CudaError*>(&e)) {
+    return ce->code == cudaErrorMemoryAllocation ? B200RT_ERR_OUT_OF_MEMORY : B200RT_ERR_CUDA;
+  }
+  return B200RT_ERR_INVALID_ARGUMENT;
+}
+
+// Builds all basic rows on the device (ProjMatrixByBin cache fill) and the projector tables.
+void setup_projector(b200rt_projector& h) {
+  Geometry& g = *h.geo;
+  DeviceGuard dg(h.device);
+  ck(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (g.num_tof() > 1) throw std::runtime_error("TOF projection data is not supported by this build of the projector");
+
+  const std::vector<int> bviews = g.basic_views();
+  const std::vector<int> bsegs = g.basic_segments();
+  const std::vector<int> btangs = g.basic_tangs();
+  h.num_basic_views = static_cast<int>(bviews.size());
+
+  // related lines, shared by all bins of a (view, seg, tang==0) group
+  std::vector<LineDev> lines;
+  std::map<long long, std::pair<int, int>> line_groups;
+  auto group_lines = [&](int view, int seg, bool tz) {
+    const long long key = (static_cast<long long>(view) * 1024 + (seg + 512)) * 2 + (tz ? 1 : 0);
+    auto it = line_groups.find(key);
+    if (it != line_groups.end()) return it->second;
+    std::vector<RelatedLine> rel;
+    g.related_lines(view, seg, tz, rel);
+    const int first = static_cast<int>(lines.size());
+    for (const auto& r : rel) {
+      LineDev L;
+      L.view = static_cast<int16_t>(r.view);
+      L.seg = static_cast<int16_t>(r.seg);
+      L.tang_sign = static_cast<int8_t>(r.tang_sign);
+      L.flags = static_cast<int8_t>((r.op.swap ? 1 : 0) | (r.op.sx < 0 ? 2 : 0) | (r.op.sy < 0 ? 4 : 0) | (r.op.zq ? 8 : 0));
+      if (r.op.q < -32768 || r.op.q > 32767) throw std::runtime_error("z transform out of range");
+      L.q = static_cast<int16_t>(r.op.q);
+      lines.push_back(L);
+    }
+    const std::pair<int, int> v(first, static_cast<int>(rel.size()));
+    line_groups[key] = v;
+    return v;
+  };
+
+  std::vector<Ray> rays;
+  std::vector<BasicBin> bbs;
+  for (int v : bviews)
+    for (int s : bsegs)
+      for (int t : btangs) {
+        bbs.push_back(g.make_basic_bin(v, s, t, 0, rays));
+      }
+  const int nb = static_cast<int>(bbs.size());
+  h.h_bins.resize(nb);
+  h.h_bin_view.resize(nb);
+  h.h_bin_seg.resize(nb);
+
+  // device copies of the rays
+  std::vector<RayDev> hrays(rays.size());
+  for (size_t i = 0; i < rays.size(); ++i) {
+    for (int k = 0; k < 3; ++k) {
+      hrays[i].start[k] = rays[i].start[k];
+      hrays[i].stop[k] = rays[i].stop[k];
+    }
+    hrays[i].norm_const = rays[i].norm_const;
+  }
+  DevBuf<RayDev> d_rays;
+  d_rays.upload(hrays, h.stream);
+
+  // build in batches with bounded scratch (2*capacity RowKV elements per bin)
+  const size_t budget = size_t(1) << 27;  // RowKV elements of scratch per batch (2 GiB)
+  std::vector<int64_t> row_len(nb, 0);
+  std::vector<std::unique_ptr<DevBuf<RowElem>>> batch_rows;
+  std::vector<std::pair<int, int>> batch_ranges;
+  DevBuf<RowKV> scratch;
+  DevBuf<BuildBinDev> d_bb;
+  DevBuf<int> d_counts;
+  DevBuf<int64_t> d_off;
+  const float vox[3] = {g.desc().voxel_size_z, g.desc().voxel_size_y, g.desc().voxel_size_x};
+  int b0 = 0;
+  while (b0 < nb) {
+    std::vector<BuildBinDev> hb;
+    size_t need = 0;
+    int b1 = b0;
+    while (b1 < nb) {
+      const size_t c = 2 * static_cast<size_t>(bbs[b1].capacity);
+      if (b1 > b0 && need + c > budget) break;
+      BuildBinDev d{};
+      d.first_ray = bbs[b1].first_ray;
+      d.num_rays = bbs[b1].num_rays;
+      d.direct = bbs[b1].direct;
+      d.nlz = bbs[b1].num_lors_per_axial_pos;
+      d.z_origin_in_planes = bbs[b1].z_origin_in_planes;
+      d.z_centre = bbs[b1].z_centre;
+      d.left_edge = bbs[b1].left_edge;
+      d.tor_width = bbs[b1].tor_width;
+      d.scratch_offset = static_cast<int64_t>(need);
+      d.capacity = bbs[b1].capacity;
+      hb.push_back(d);
+      need += c;
+      ++b1;
+    }
+    const int n = b1 - b0;
+    scratch.alloc(std::max(need, scratch.n));
+    d_bb.upload(hb, h.stream);
+    d_counts.alloc(n);
+    ck(launch_build_rows(d_rays.p, d_bb.p, n, vox, scratch.p, d_counts.p, h.stream), "build rows");
+    std::vector<int> counts(n);
+    ck(cudaMemcpyAsync(counts.data(), d_counts.p, n * sizeof(int), cudaMemcpyDeviceToHost, h.stream), "counts");
+    ck(cudaStreamSynchronize(h.stream), "build rows");
+    std::vector<int64_t> off(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      if (counts[i] < 0) {
+        static const char* why[] = {"", "ray split too deep", "row capacity exceeded", "add_adjacent_z capacity exceeded",
+                                    "z copies capacity exceeded", "row element outside the packed coordinate range"};
+        const int c = -counts[i];
+        throw std::runtime_error(std::string("row builder: ") + (c >= 1 && c <= 5 ? why[c] : "unknown error"));
+      }
+      row_len[b0 + i] = counts[i];
+      off[i + 1] = off[i] + counts[i];
+    }
+    d_off.upload(off, h.stream);
+    auto out = std::make_unique<DevBuf<RowElem>>();
+    out->alloc(std::max<int64_t>(off[n], 1));
+    ck(launch_compact_rows(d_bb.p, n, scratch.p, d_off.p, out->p, h.stream), "compact rows");
+    ck(cudaStreamSynchronize(h.stream), "compact rows");
+    batch_rows.push_back(std::move(out));
+    batch_ranges.push_back({b0, b1});
+    b0 = b1;
+  }
+  scratch.release();
+
+  int64_t total = 0;
+  int max_len = 0;
+  for (int b = 0; b < nb; ++b) {
+    total += row_len[b];
+    max_len = std::max<int>(max_len, static_cast<int>(row_len[b]));
+  }
+  h.rows.alloc(std::max<int64_t>(total, 1));
+  int64_t pos = 0;
+  for (size_t i = 0; i < batch_rows.size(); ++i) {
+    int64_t cnt = 0;
+    for (int b = batch_ranges[i].first; b < batch_ranges[i].second; ++b) cnt += row_len[b];
+    if (cnt > 0)
+      ck(cudaMemcpyAsync(h.rows.p + pos, batch_rows[i]->p, cnt * sizeof(RowElem), cudaMemcpyDeviceToDevice, h.stream),
+         "rows");
+    pos += cnt;
+  }
+  ck(cudaStreamSynchronize(h.stream), "rows");
+  batch_rows.clear();
+
+  pos = 0;
+  for (int b = 0; b < nb; ++b) {
+    const BasicBin& bb = bbs[b];
+    const auto lg = group_lines(bb.view, bb.seg, bb.tang == 0);
+    ProjBinDev pb{};
+    pb.row_offset = pos;
+    pb.row_len = static_cast<int32_t>(row_len[b]);
+    pb.tang = static_cast<int16_t>(bb.tang);
+    pb.tof = static_cast<int16_t>(bb.tof);
+    pb.first_line = lg.first;
+    pb.num_lines = lg.second;
+    h.h_bins[b] = pb;
+    h.h_bin_view[b] = bb.view;
+    h.h_bin_seg[b] = bb.seg;
+    h.bin_index[h.bin_key(bb.view, bb.seg, bb.tang, bb.tof)] = b;
+    pos += row_len[b];
+  }
+  h.bins.upload(h.h_bins, h.stream);
+  h.lines.upload(lines, h.stream);
+  std::vector<SegDev> sd(2 * g.S() + 1);
+  for (int s = -g.S(); s <= g.S(); ++s) {
+    sd[s + g.S()].dev_offset = g.dev_segment_offset(s);
+    sd[s + g.S()].nax = g.nax(s);
+    sd[s + g.S()].npa = g.npa(s);
+  }
+  h.segs.upload(sd, h.stream);
+
+  ProjParams& p = h.params;
+  p.rows = h.rows.p;
+  p.bins = h.bins.p;
+  p.lines = h.lines.p;
+  p.segs = h.segs.p;
+  p.S = g.S();
+  p.num_views = g.num_views();
+  p.num_tang = g.num_tang();
+  p.min_tang = g.min_tang();
+  p.max_tang = g.max_tang();
+  p.num_tof = g.num_tof();
+  p.min_tof = g.min_tof();
+  p.tof_stride = g.tof_stride();
+  p.nz = g.desc().nz;
+  p.ny = g.desc().ny;
+  p.nx = g.desc().nx;
+  p.min_z = g.desc().min_z;
+  p.min_y = g.desc().min_y;
+  p.min_x = g.desc().min_x;
+  p.max_row_len = max_len;
+  if (static_cast<int64_t>(p.nz) * p.ny * p.nx >= (int64_t(1) << 31)) throw std::runtime_error("image too large");
+  const size_t smem = projector_smem_bytes(p);
+  if (smem > 220 * 1024) throw std::runtime_error("basic row too long for shared memory");
+
+  // total number of (bin, element) pairs inside the image
+  {
+    int64_t t = 0;
+    std::vector<RowElem> hr(static_cast<size_t>(total));
+    if (total > 0) ck(cudaMemcpy(hr.data(), h.rows.p, total * sizeof(RowElem), cudaMemcpyDeviceToHost), "rows");
+    for (int b = 0; b < nb; ++b) {
+      const ProjBinDev& pb = h.h_bins[b];
+      for (int l = 0; l < pb.num_lines; ++l) {
+        const LineDev& L = lines[pb.first_line + l];
+        const int tang = L.tang_sign * pb.tang;
+        if (tang < g.min_tang() || tang > g.max_tang()) continue;
+        const int npa = g.npa(L.seg), nax = g.nax(L.seg);
+        for (int k = 0; k < pb.row_len; ++k) {
+          int z, y, x;
+          unpack_zyx(hr[pb.row_offset + k].zyx, z, y, x);
+          const int zt = ((L.flags & 8) ? L.q - z : z) - p.min_z;
+          // number of a in [0,nax) with 0 <= zt + npa*a < nz
+          int lo = zt >= 0 ? 0 : (-zt + npa - 1) / npa;
+          int hi = (p.nz - 1 - zt) >= 0 ? (p.nz - 1 - zt) / npa : -1;
+          hi = std::min(hi, nax - 1);
+          if (hi >= lo) t += hi - lo + 1;
+        }
+      }
+    }
+    h.total_nnz = t;
+  }
+}
+
+// device list of the basic bins in subset `subset` of `nsub` (find_basic_vs_nums_in_subset.cxx:32-70)
+const int* subset_list(b200rt_projector& h, int subset, int nsub, int& count) {
+  const auto key = std::make_pair(subset, nsub);
+  auto it = h.subset_lists.find(key);
+  if (it != h.subset_lists.end()) {
+    count = h.subset_counts[key];
+    return it->second->p;
+  }
+  std::vector<int> list;
+  for (int b = 0; b < static_cast<int>(h.h_bins.size()); ++b)
+    if (h.h_bin_view[b] % nsub == subset) list.push_back(b);
+  auto buf = std::make_unique<DevBuf<int>>();
+  buf->upload(list, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "subset list");
+  count = static_cast<int>(list.size());
+  h.subset_counts[key] = count;
+  const int* p = buf->p;
+  h.subset_lists[key] = std::move(buf);
+  return p;
+}
+
+int check_subset(b200rt_projector* h, int subset, int nsub) {
+  if (nsub < 1 || subset < 0 || subset >= nsub) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "invalid subset number");
+  return B200RT_OK;
+}
+
+cudaError_t projdata_layout(const Geometry& g, const float* in, float* out, bool to_dev, cudaStream_t st) {
+  const int64_t nvt = static_cast<int64_t>(g.num_views()) * g.num_tang();
+  for (int k = 0; k < g.num_tof(); ++k)
+    for (int s = -g.S(); s <= g.S(); ++s) {
+      const int64_t so = k * g.tof_stride() + g.stir_segment_offset(s);
+      const int64_t dv = k * g.tof_stride() + g.dev_segment_offset(s);
+      const cudaError_t e = to_dev ? launch_projdata_to_dev(in + so, out + dv, g.nax(s), nvt, st)
+                                   : launch_projdata_from_dev(in + dv, out + so, g.nax(s), nvt, st);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200rt_create(const b200rt_geometry* geometry, int device, b200rt_projector** out) {
+  if (!out) return B200RT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!geometry) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_create_error = "null geometry";
+    return B200RT_ERR_INVALID_ARGUMENT;
+  }
+  auto h = std::make_unique<b200rt_projector>();
+  try {
+    int ndev = 0;
+    ck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) throw std::runtime_error("invalid CUDA device");
+    h->device = device;
+    h->geo = std::make_unique<Geometry>(*geometry);
+    setup_projector(*h);
+  } catch (const std::exception& e) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_create_error = e.what();
+    const int st = status_of(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->stream = nullptr;
+    return st == B200RT_ERR_INVALID_ARGUMENT && dynamic_cast<const CudaError*>(&e) == nullptr ? B200RT_ERR_INVALID_ARGUMENT : st;
+  }
+  *out = h.release();
+  return B200RT_OK;
+}
+
+void b200rt_destroy(b200rt_projector* h) {
+  if (!h) return;
+  {
+    DeviceGuard dg(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->subset_lists.clear();
+    h->rows.release();
+    h->bins.release();
+    h->lines.release();
+    h->segs.release();
+    h->st_img_a.release();
+    h->st_img_b.release();
+    h->st_pd_a.release();
+    h->st_pd_b.release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+  }
+  delete h;
+}
+
+const char* b200rt_last_error(const b200rt_projector* h) {
+  if (!h) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_create_error.c_str();
+  }
+  return h->err.c_str();
+}
+
+int b200rt_get_info(const b200rt_projector* h, b200rt_info* out) {
+  if (!h || !out) return B200RT_ERR_INVALID_ARGUMENT;
+  const Geometry& g = *h->geo;
+  std::memset(out, 0, sizeof(*out));
+  out->num_bins = g.projdata_size();
+  out->num_image_voxels = g.image_size();
+  out->num_basic_bins = static_cast<int64_t>(h->h_bins.size());
+  out->num_row_elements = static_cast<int64_t>(h->rows.n);
+  out->total_nnz = h->total_nnz;
+  out->num_tof_bins = g.num_tof();
+  out->num_basic_views = h->num_basic_views;
+  out->symmetries_used = g.symmetry_bits();
+  return B200RT_OK;
+}
+
+int64_t b200rt_projdata_size(const b200rt_projector* h) { return h ? h->geo->projdata_size() : -1; }
+int64_t b200rt_image_size(const b200rt_projector* h) { return h ? h->geo->image_size() : -1; }
+
+int b200rt_get_row(b200rt_projector* h, int segment, int view, int axial, int tangential, int timing, int32_t* coords_zyx,
+                   float* values, int64_t capacity, int64_t* length) {
+  if (!h || !length) return B200RT_ERR_INVALID_ARGUMENT;
+  try {
+    const Geometry& g = *h->geo;
+    if (segment < -g.S() || segment > g.S() || view < 0 || view >= g.num_views() || axial < 0 || axial >= g.nax(segment) ||
+        tangential < g.min_tang() || tangential > g.max_tang() || timing < g.min_tof() || timing >= g.min_tof() + g.num_tof())
+      return fail(h, B200RT_ERR_INVALID_ARGUMENT, "bin out of range");
+    const SymOp op = g.find_op(segment, view, axial, tangential);
+    int s = segment, v = view, a = axial, t = tangential, k = timing;
+    g.find_basic_bin(s, v, a, t, k);
+    auto it = h->bin_index.find(h->bin_key(v, s, t, k));
+    if (it == h->bin_index.end()) return fail(h, B200RT_ERR_STATE, "basic bin not found");
+    const ProjBinDev& pb = h->h_bins[it->second];
+    *length = pb.row_len;
+    const int64_t n = std::min<int64_t>(pb.row_len, capacity);
+    if (n <= 0) return B200RT_OK;
+    if (!coords_zyx || !values) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null output arrays");
+    DeviceGuard dg(h->device);
+    std::vector<RowElem> r(n);
+    ck(cudaMemcpy(r.data(), h->rows.p + pb.row_offset, n * sizeof(RowElem), cudaMemcpyDeviceToHost), "row");
+    const int zs = g.npa(segment) * axial;
+    for (int64_t i = 0; i < n; ++i) {
+      int z, y, x;
+      unpack_zyx(r[i].zyx, z, y, x);
+      coords_zyx[3 * i + 2] = (op.swap ? y : x) * op.sx;
+      coords_zyx[3 * i + 1] = (op.swap ? x : y) * op.sy;
+      coords_zyx[3 * i] = (op.zq ? op.q - z : z) + zs;
+      values[i] = r[i].v;
+    }
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_image_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream) {
+  if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
+  const auto& d = h->geo->desc();
+  DeviceGuard dg(h->device);
+  const cudaError_t e = launch_image_to_dev(stir_dev, dev, d.nz, d.ny, d.nx, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
+}
+int b200rt_image_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream) {
+  if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
+  const auto& d = h->geo->desc();
+  DeviceGuard dg(h->device);
+  const cudaError_t e = launch_image_from_dev(dev, stir_dev, d.nz, d.ny, d.nx, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
+}
+int b200rt_projdata_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream) {
+  if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  const cudaError_t e = projdata_layout(*h->geo, stir_dev, dev, true, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
+}
+int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream) {
+  if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
+  DeviceGuard dg(h->device);
+  const cudaError_t e = projdata_layout(*h->geo, dev, stir_dev, false, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
+}
+
+int b200rt_forward_project_dev(b200rt_projector* h, const float* image_dev, float* projdata_dev, int subset_num,
+                               int num_subsets, void* stream) {
+  if (!h || !image_dev || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    int n = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    ck(launch_forward(h->params, list, n, image_dev, projdata_dev, static_cast<cudaStream_t>(stream)), "forward projection");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, float* image_dev, int subset_num,
+                            int num_subsets, int mode, void* stream) {
+  if (!h || !image_dev || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (mode != B200RT_BACKPROJECT_ATOMIC) return fail(h, B200RT_ERR_UNSUPPORTED, "back-projection mode not available");
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int n = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    ck(cudaMemsetAsync(image_dev, 0, sizeof(float) * h->geo->image_size(), st), "memset");
+    ck(launch_back_atomic(h->params, list, n, projdata_dev, image_dev, st), "back projection");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host, int subset_num,
+                           int num_subsets) {
+  if (!h || !image_host || !projdata_host) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = h->stream;
+    h->st_img_a.alloc(g.image_size());
+    h->st_img_b.alloc(g.image_size());
+    h->st_pd_a.alloc(g.projdata_size());
+    h->st_pd_b.alloc(g.projdata_size());
+    ck(cudaMemcpyAsync(h->st_img_a.p, image_host, sizeof(float) * g.image_size(), cudaMemcpyHostToDevice, st), "H2D");
+    ck(launch_image_to_dev(h->st_img_a.p, h->st_img_b.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
+    ck(cudaMemsetAsync(h->st_pd_b.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+    int n = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    ck(launch_forward(h->params, list, n, h->st_img_b.p, h->st_pd_b.p, st), "forward projection");
+    ck(projdata_layout(g, h->st_pd_b.p, h->st_pd_a.p, false, st), "layout");
+    ck(cudaMemcpyAsync(projdata_host, h->st_pd_a.p, sizeof(float) * g.projdata_size(), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "forward projection");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* image_host, int subset_num,
+                        int num_subsets, int mode) {
+  if (!h || !image_host || !projdata_host) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (mode != B200RT_BACKPROJECT_ATOMIC) return fail(h, B200RT_ERR_UNSUPPORTED, "back-projection mode not available");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = h->stream;
+    h->st_img_a.alloc(g.image_size());
+    h->st_img_b.alloc(g.image_size());
+    h->st_pd_a.alloc(g.projdata_size());
+    h->st_pd_b.alloc(g.projdata_size());
+    ck(cudaMemcpyAsync(h->st_pd_a.p, projdata_host, sizeof(float) * g.projdata_size(), cudaMemcpyHostToDevice, st), "H2D");
+    ck(projdata_layout(g, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
+    int n = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    ck(cudaMemsetAsync(h->st_img_b.p, 0, sizeof(float) * g.image_size(), st), "memset");
+    ck(launch_back_atomic(h->params, list, n, h->st_pd_b.p, h->st_img_b.p, st), "back projection");
+    ck(launch_image_from_dev(h->st_img_b.p, h->st_img_a.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
+    ck(cudaMemcpyAsync(image_host, h->st_img_a.p, sizeof(float) * g.image_size(), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "back projection");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+}  // extern "C"

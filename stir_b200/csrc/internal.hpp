@@ -1,0 +1,104 @@
+// Device-side data structures shared by the kernels and the host driver.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200 {
+
+// A stored row element: voxel (z,y,x) packed into 32 bits and its value.
+//   bits  0..10 : x + 1024   bits 11..21 : y + 1024   bits 22..31 : (z - zmin_row) ... see pack_zyx
+// z is stored relative to a per-geometry row z bias so that the 10 bits cover [-512, 511].
+struct __align__(8) RowElem {
+  uint32_t zyx;
+  float v;
+};
+
+__host__ __device__ inline uint32_t pack_zyx(int z, int y, int x) {
+  return static_cast<uint32_t>(x + 1024) | (static_cast<uint32_t>(y + 1024) << 11) |
+         (static_cast<uint32_t>(z + 512) << 22);
+}
+__host__ __device__ inline void unpack_zyx(uint32_t p, int& z, int& y, int& x) {
+  x = static_cast<int>(p & 2047u) - 1024;
+  y = static_cast<int>((p >> 11) & 2047u) - 1024;
+  z = static_cast<int>(p >> 22) - 512;
+}
+
+// One ray of a basic bin (geometry.hpp Ray) as uploaded to the device
+struct RayDev {
+  float start[3];
+  float stop[3];
+  float norm_const;
+};
+
+// Per basic bin, for the row builder
+struct BuildBinDev {
+  int first_ray, num_rays;
+  int direct, nlz;
+  float z_origin_in_planes, z_centre, left_edge, tor_width;
+  int64_t scratch_offset;  // first element of this bin's scratch (2*capacity elements)
+  int capacity;
+  int pad;
+};
+
+// A related line of a basic view-segment: target viewgram and the symmetry operation
+//   flags: bit0 swap x<->y, bit1 negate x', bit2 negate y', bit3 z -> q - z
+struct LineDev {
+  int16_t view, seg;
+  int8_t tang_sign, flags;
+  int16_t q;
+};
+
+// Per basic bin, for the projectors
+struct ProjBinDev {
+  int64_t row_offset;
+  int32_t row_len;
+  int16_t tang;    // basic tangential position (>= 0 with the s symmetry)
+  int16_t tof;
+  int32_t first_line, num_lines;  // into lines[]
+};
+
+struct SegDev {
+  int64_t dev_offset;  // device-layout offset of the segment (TOF bin 0)
+  int32_t nax;
+  int32_t npa;
+};
+
+// Kernel parameters of the projectors
+struct ProjParams {
+  const RowElem* rows;
+  const ProjBinDev* bins;
+  const LineDev* lines;
+  const SegDev* segs;  // index seg + S
+  int S;
+  int num_views, num_tang, min_tang, max_tang;
+  int num_tof, min_tof;
+  int64_t tof_stride;
+  int nz, ny, nx;      // image (device layout [y][x][z])
+  int min_z, min_y, min_x;
+  int max_row_len;
+};
+
+// launchers (project.cu)
+cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
+                           cudaStream_t st);
+cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
+                               cudaStream_t st);
+cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st);
+cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny, int nx, cudaStream_t st);
+// per segment: STIR [ax][view*tang] <-> device [view*tang][ax]
+cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
+cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
+
+// row builder (rows.cu)
+struct RowKV {
+  uint64_t key;  // (z,y,x) sort key << 8 | tag
+  float v;
+  uint32_t pad;
+};
+cudaError_t launch_build_rows(const RayDev* rays, const BuildBinDev* bins, int nbins, const float voxel_zyx[3],
+                              RowKV* scratch, int* counts, cudaStream_t st);
+cudaError_t launch_compact_rows(const BuildBinDev* bins, int nbins, const RowKV* scratch, const int64_t* out_offsets,
+                                RowElem* rows, cudaStream_t st);
+
+}  // namespace b200

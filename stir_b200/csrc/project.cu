@@ -1,0 +1,250 @@
+// Forward and back projection with the rows of STIR's ray-tracing matrix,
+// unfolding its symmetries on the fly.
+//
+// Work decomposition (one CTA per basic bin):
+//   * the basic row (STIR's cached row, ProjMatrixByBin.inl:48-113) is staged in shared memory;
+//   * each warp takes one related line at a time: a viewgram related by a symmetry
+//     (DataSymmetriesForBins_PET_CartesianGrid::get_related_view_segment_numbers) at the
+//     basic tangential position or its mirror;
+//   * the warp's lanes are the axial positions of that line (the z-shift symmetry): lane a
+//     reads voxel z' = (zq ? q - z : z) + npa*a, so with the image stored z-fastest
+//     ([y][x][z]) the 32 lanes of a warp read consecutive floats of one column;
+//   * the transformed column offsets of the row are computed once per line by the warp's
+//     lanes in parallel (into shared memory) and reused for all axial positions.
+//
+// Forward: projdata[line][a] = sum_k image[col_k][z_k + npa*a] * w_k, z range-checked as in
+//          ProjMatrixElemsForOneBin::forward_project (ProjMatrixElemsForOneBin.cxx:354-370).
+// Back:    image[col_k][z_k + npa*a] += w_k * projdata[line][a] for projdata != 0
+//          (ProjMatrixElemsForOneBin::back_project, :333-351), with float atomics.
+#include "internal.hpp"
+
+namespace b200 {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kAxPerLane = 4;  // axial positions per lane per pass: 128 per warp
+
+struct LineSetup {
+  int64_t out_base;  // device-layout index of (line, axial 0)
+  int nax, npa;
+};
+
+__device__ __forceinline__ bool setup_line(const ProjParams& p, const ProjBinDev& pb, const LineDev& L, LineSetup& s) {
+  const int tang = static_cast<int>(L.tang_sign) * pb.tang;
+  if (tang < p.min_tang || tang > p.max_tang) return false;
+  const SegDev sd = p.segs[L.seg + p.S];
+  s.nax = sd.nax;
+  s.npa = sd.npa;
+  s.out_base = static_cast<int64_t>(pb.tof - p.min_tof) * p.tof_stride + sd.dev_offset +
+               (static_cast<int64_t>(L.view) * p.num_tang + (tang - p.min_tang)) * sd.nax;
+  return true;
+}
+
+// a row element after the line's symmetry operation: column start (col*nz), z' - min_z
+// without the axial shift, and the value
+struct __align__(16) XElem {
+  int colbase;
+  int zt;
+  float v;
+  int pad;
+};
+
+constexpr int kChunk = 256;  // row elements transformed per warp at a time
+
+__device__ __forceinline__ void transform_chunk(const ProjParams& p, const RowElem* srow, int c0, int cn, const LineDev& L,
+                                                XElem* xbuf, int lane) {
+  const int swap = L.flags & 1;
+  const int sx = (L.flags & 2) ? -1 : 1;
+  const int sy = (L.flags & 4) ? -1 : 1;
+  const int zq = (L.flags & 8) ? 1 : 0;
+  for (int k = lane; k < cn; k += 32) {
+    const RowElem e = srow[c0 + k];
+    int z, y, x;
+    unpack_zyx(e.zyx, z, y, x);
+    const int xt = (swap ? y : x) * sx;
+    const int yt = (swap ? x : y) * sy;
+    XElem o;
+    o.zt = (zq ? static_cast<int>(L.q) - z : z) - p.min_z;
+    o.colbase = ((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz;
+    o.v = e.v;
+    o.pad = 0;
+    xbuf[k] = o;
+  }
+}
+
+__device__ __forceinline__ void stage_row(const ProjParams& p, const ProjBinDev& pb, RowElem* srow) {
+  for (int i = threadIdx.x; i < pb.row_len; i += blockDim.x) srow[i] = p.rows[pb.row_offset + i];
+}
+
+__global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                           const float* __restrict__ img, float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  XElem* xbuf = reinterpret_cast<XElem*>(smem) + warp * kChunk;
+  RowElem* srow = reinterpret_cast<RowElem*>(smem + sizeof(XElem) * kWarps * kChunk);
+  const int n = pb.row_len;
+  stage_row(p, pb, srow);
+  __syncthreads();
+  const unsigned nz = static_cast<unsigned>(p.nz);
+  for (int l = warp; l < pb.num_lines; l += kWarps) {
+    const LineDev L = p.lines[pb.first_line + l];
+    LineSetup s;
+    if (!setup_line(p, pb, L, s)) continue;
+    for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
+      int zoff[kAxPerLane];
+      float acc[kAxPerLane];
+#pragma unroll
+      for (int j = 0; j < kAxPerLane; ++j) {
+        const int a = a0 + j * 32 + lane;
+        // lanes past the last axial position get an offset that fails the range check
+        zoff[j] = a < s.nax ? a * s.npa : (1 << 29);
+        acc[j] = 0.f;
+      }
+      for (int c0 = 0; c0 < n; c0 += kChunk) {
+        const int cn = min(kChunk, n - c0);
+        __syncwarp();
+        transform_chunk(p, srow, c0, cn, L, xbuf, lane);
+        __syncwarp();
+        for (int k = 0; k < cn; ++k) {
+          const XElem e = xbuf[k];
+#pragma unroll
+          for (int j = 0; j < kAxPerLane; ++j) {
+            const int zz = e.zt + zoff[j];
+            if (static_cast<unsigned>(zz) < nz) acc[j] += __ldg(img + e.colbase + zz) * e.v;
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kAxPerLane; ++j) {
+        const int a = a0 + j * 32 + lane;
+        if (a < s.nax) out[s.out_base + a] = acc[j];
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                               const float* __restrict__ pd, float* __restrict__ img) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  XElem* xbuf = reinterpret_cast<XElem*>(smem) + warp * kChunk;
+  RowElem* srow = reinterpret_cast<RowElem*>(smem + sizeof(XElem) * kWarps * kChunk);
+  const int n = pb.row_len;
+  stage_row(p, pb, srow);
+  __syncthreads();
+  const unsigned nz = static_cast<unsigned>(p.nz);
+  for (int l = warp; l < pb.num_lines; l += kWarps) {
+    const LineDev L = p.lines[pb.first_line + l];
+    LineSetup s;
+    if (!setup_line(p, pb, L, s)) continue;
+    for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
+      int zoff[kAxPerLane];
+      float d[kAxPerLane];
+      bool any = false;
+#pragma unroll
+      for (int j = 0; j < kAxPerLane; ++j) {
+        const int a = a0 + j * 32 + lane;
+        d[j] = a < s.nax ? __ldg(pd + s.out_base + a) : 0.f;
+        // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
+        zoff[j] = d[j] != 0.f ? a * s.npa : (1 << 29);
+        any |= d[j] != 0.f;
+      }
+      if (!__any_sync(0xffffffffu, any)) continue;
+      for (int c0 = 0; c0 < n; c0 += kChunk) {
+        const int cn = min(kChunk, n - c0);
+        __syncwarp();
+        transform_chunk(p, srow, c0, cn, L, xbuf, lane);
+        __syncwarp();
+        for (int k = 0; k < cn; ++k) {
+          const XElem e = xbuf[k];
+#pragma unroll
+          for (int j = 0; j < kAxPerLane; ++j) {
+            const int zz = e.zt + zoff[j];
+            if (static_cast<unsigned>(zz) < nz) atomicAdd(img + e.colbase + zz, e.v * d[j]);
+          }
+        }
+      }
+    }
+  }
+}
+
+// image [z][y][x] <-> [y][x][z]: a transpose of (nz) x (ny*nx)
+__global__ void transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows, int64_t cols) {
+  // in: rows x cols, out: cols x rows
+  __shared__ float tile[32][33];
+  const int64_t c0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const int r0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int i = ty; i < 32; i += 8) {
+    const int r = r0 + i;
+    const int64_t c = c0 + tx;
+    if (r < rows && c < cols) tile[i][tx] = in[static_cast<int64_t>(r) * cols + c];
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t c = c0 + i;
+    const int r = r0 + tx;
+    if (r < rows && c < cols) out[c * rows + r] = tile[tx][i];
+  }
+}
+
+cudaError_t transpose(const float* in, float* out, int rows, int64_t cols, cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t gx = (cols + 31) / 32;
+  const int64_t gy = (rows + 31) / 32;
+  if (gy > 65535 || gx > 2147483647LL) return cudaErrorInvalidValue;
+  transpose_kernel<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), dim3(32, 8), 0, st>>>(in, out, rows, cols);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+static size_t proj_smem_bytes(const ProjParams& p) {
+  return sizeof(XElem) * kWarps * kChunk + sizeof(RowElem) * static_cast<size_t>(p.max_row_len > 0 ? p.max_row_len : 1);
+}
+
+static cudaError_t prepare_smem(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  return cudaSuccess;
+}
+
+size_t projector_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p); }
+
+cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
+                           cudaStream_t st) {
+  if (nbins <= 0) return cudaSuccess;
+  const size_t sm = proj_smem_bytes(p);
+  cudaError_t e = prepare_smem(reinterpret_cast<const void*>(forward_kernel), sm);
+  if (e != cudaSuccess) return e;
+  forward_kernel<<<nbins, kThreads, sm, st>>>(p, bin_list, image, projdata);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
+                               cudaStream_t st) {
+  if (nbins <= 0) return cudaSuccess;
+  const size_t sm = proj_smem_bytes(p);
+  cudaError_t e = prepare_smem(reinterpret_cast<const void*>(back_atomic_kernel), sm);
+  if (e != cudaSuccess) return e;
+  back_atomic_kernel<<<nbins, kThreads, sm, st>>>(p, bin_list, projdata, image);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st) {
+  return transpose(stir, dev, nz, static_cast<int64_t>(ny) * nx, st);
+}
+cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny, int nx, cudaStream_t st) {
+  return transpose(dev, stir, ny * nx, nz, st);  // dev is (ny*nx) x nz
+}
+cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st) {
+  return transpose(stir, dev, nax, nvt, st);
+}
+cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st) {
+  return transpose(dev, stir, static_cast<int>(nvt), nax, st);
+}
+
+}  // namespace b200

@@ -1,0 +1,342 @@
+"""Benchmark of the B200 ray-tracing projector pair (forward + back projection LORs/s).
+
+Default workload: the clinical 3D PET geometry (64 rings x 504 detectors, span 11, max ring
+difference 60, 252 views x 344 tangential positions = 72.6M LORs; image 344x344x127), seeded
+synthetic phantom.  One step = a forward projection of every LOR followed by a back projection
+of every LOR (the projector work of one full OSEM iteration).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N>1) every rank projects its own copy of the workload (independent frames, no
+collective): value = all ranks' LORs / the slowest rank's time ("scaling": "weak").
+--impl reference times the CPU restatement of STIR's OpenMP path (oracle) on the host cores on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("clinical 3D PET: 64 rings x 504 det, R 328 mm, span 11, max ring diff 60, 252 views x 344 tang "
+            "(72,557,856 LORs), image 344x344x127 (2.09x2.09x2.03 mm), ray-tracing matrix, 1 tangential LOR")
+METRIC = "fwd+back LORs/s"
+CPU_SAMPLE_SUBSET = (0, 42)  # views 0, 42 and their symmetry partners: 1/42 of the views
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5).stdout
+                for line in out.strip().splitlines():
+                    self.samples.append([c.strip() for c in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and "Active" in s[5 + i]
+                          and "Not" not in s[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def subset_num_bins(pdi, geometry, bits, subset, nsub):
+    from stir_b200.subsets import views_in_subset
+    views = views_in_subset(geometry, subset, nsub, bits)
+    return len(views) * pdi.num_sinograms * pdi.num_tangential_poss
+
+
+class CpuBaseline:
+    """The oracle (restated STIR OpenMP path) on a bounded sample of the workload: forward + back
+    projection of one subset of the clinical geometry with all host threads."""
+
+    def __init__(self, nthreads=None):
+        from oracle.oracle import Oracle
+        from stir_b200 import geometry as G
+        from stir_b200 import phantoms
+        self.pdi, self.img = G.clinical_3d_pet()
+        self.geo = G.make_geometry(self.pdi, self.img)
+        self.orc = Oracle(self.geo)
+        self.nthreads = nthreads or os.cpu_count() or 1
+        self.x = phantoms.cylinder_with_spheres(self.img, n_spheres=6, sphere_radius=(5, 18), ellipse_axes=(150, 100))
+        self.sub, self.nsub = CPU_SAMPLE_SUBSET
+        t0 = time.perf_counter()
+        y = self.orc.forward(self.x, self.sub, self.nsub, self.nthreads)  # fills the row cache
+        self.cache_fill_s = time.perf_counter() - t0
+        self.y = (y + np.float32(0.3)).astype(np.float32)
+        self.out = np.zeros(self.orc.projdata_size, np.float32)
+        self.nbins = subset_num_bins(self.pdi, self.geo, self.orc.symmetries_used, self.sub, self.nsub)
+
+    def step(self):
+        t0 = time.perf_counter()
+        self.orc.forward(self.x, self.sub, self.nsub, self.nthreads, out=self.out)
+        self.orc.back(self.y, self.sub, self.nsub, self.nthreads)
+        return time.perf_counter() - t0
+
+    def describe(self, seconds):
+        return {"value": self.nbins / seconds, "unit": "LORs/s", "cores": self.nthreads, "kind": "port",
+                "sample": f"forward+back of subset {self.sub} of {self.nsub} ({self.nbins} LORs) of the clinical "
+                          f"workload with a warm row cache (cache fill {self.cache_fill_s:.2f} s), {self.nthreads} "
+                          "OpenMP threads; restated CPU path, not the STIR binary"}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0, None
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import datetime
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, ws, local, dist
+
+
+def reference_main(args):
+    rank, ws, local, dist = dist_setup()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cb = CpuBaseline()
+    for _ in range(max(0, args.warmup)):
+        cb.step()
+    times = [cb.step() for _ in range(max(1, args.steps))]
+    sec = float(np.mean(times))
+    desc = cb.describe(sec)
+    v = desc["value"]
+    line = {"metric": METRIC, "value": v, "unit": "LORs/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": desc["sample"]},
+            "cpu_baseline": desc,
+            "e2e": {"value": v, "unit": "LORs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def profile_traffic(kernel_name):
+    """DRAM bytes per launch of `kernel_name` from the committed ncu summary (profiles/), or None."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        try:
+            txt = open(path).read()
+        except OSError:
+            continue
+        m = re.search(rf"^traffic_per_launch\\[{kernel_name}\\]:\\s*([0-9.eE+]+)", txt, re.M)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def b200_main(args):
+    import ctypes
+
+    import torch
+
+    from stir_b200 import _abi
+    from stir_b200 import geometry as G
+    from stir_b200 import phantoms
+    from stir_b200.projectors import RayTracingProjector
+
+    rank, ws, local, dist = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pdi, img = G.clinical_3d_pet()
+    t0 = time.perf_counter()
+    proj = RayTracingProjector(pdi, img, device=local)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    nbins = proj.projdata_size
+    nnz = proj.info.total_nnz
+
+    # seeded phantom per rank (an independent frame per GPU), resident in HBM
+    x = phantoms.cylinder_with_spheres(img, n_spheres=6, sphere_radius=(5, 18), ellipse_axes=(150, 100), seed=1 + rank)
+    xd = proj.image_to_device_layout(torch.from_numpy(x).to(dev))
+    y = proj.forward_dev(xd)
+    y.add_(0.3 * float(y.mean()))  # strictly positive data: the back projection skips no bin
+    pd = proj.empty_projdata()
+    bk = proj.empty_image()
+    flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=dev)  # 512 MiB > 126 MB L2
+
+    def step():
+        proj.forward_dev(xd, out=pd)
+        proj.back_dev(y, out=bk)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e_start.record()
+        for k in range(K):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            proj.forward_dev(xd, out=pd)
+            ev[k][1].record()
+            proj.back_dev(y, out=bk)
+            ev[k][2].record()
+        e_end.record()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = e_start.elapsed_time(e_end)
+    fwd_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+    back_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    ms_per_step = max_ms / K
+    value = nbins * ws / (ms_per_step / 1e3)
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    x_pin = torch.from_numpy(x).pin_memory()
+    pd_pin = torch.empty(nbins, dtype=torch.float32).pin_memory()
+    y_pin = proj.projdata_from_device_layout(y).cpu().pin_memory()
+    img_pin = torch.empty(img.shape, dtype=torch.float32).pin_memory()
+    lib = proj.lib
+
+    def e2e_step():
+        _abi.check(lib.b200rt_forward_project(proj.h, ctypes.c_void_p(x_pin.data_ptr()), ctypes.c_void_p(pd_pin.data_ptr()),
+                                              0, 1), proj.h, "b200rt_forward_project")
+        _abi.check(lib.b200rt_back_project(proj.h, ctypes.c_void_p(y_pin.data_ptr()), ctypes.c_void_p(img_pin.data_ptr()),
+                                           0, 1, _abi.BACKPROJECT_ATOMIC), proj.h, "b200rt_back_project")
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ke = max(2, min(K, 5))
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / ke
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = nbins * ws / float(te.item())
+    img_bytes = 4 * img.nz * img.ny * img.nx
+    pd_bytes = 4 * nbins
+
+    hbm, peak_kind = peaks()
+    fwd_bytes = 4.0 * nnz + 4.0 * nbins
+    back_bytes = 8.0 * nnz + 4.0 * nbins
+    if fwd_ms >= back_ms:
+        kname, kms, kbytes = "forward_kernel", fwd_ms, fwd_bytes
+    else:
+        kname, kms, kbytes = "back_atomic_kernel", back_ms, back_bytes
+    achieved = kbytes / (kms / 1e3) / 1e9
+    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": profile_traffic(kname),
+            "algorithmic_bytes_per_launch": kbytes,
+            "kernels_ms": {"forward_kernel": fwd_ms, "back_atomic_kernel": back_ms},
+            "frac_forward": fwd_bytes / (fwd_ms / 1e3) / 1e9 / hbm, "frac_back": back_bytes / (back_ms / 1e3) / 1e9 / hbm}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cb = CpuBaseline()
+            cpu = cb.describe(cb.step())
+        except Exception as e:  # the baseline is reported, never the measured product
+            cpu = {"value": None, "unit": "LORs/s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+
+    line = {"metric": METRIC, "value": value, "unit": "LORs/s", "n_gpus": ws, "steps": K, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lors_per_step_per_gpu": nbins, "nnz_per_step_per_gpu": nnz,
+                       "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                       "l2": "512 MiB buffer written between steps; projection data 290 MB > L2",
+                       "setup_s": setup_s, "back_projection": "atomic"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "LORs/s", "h2d_bytes_per_step": img_bytes + pd_bytes,
+                    "d2h_bytes_per_step": pd_bytes + img_bytes},
+            "clocks": clocks.summary(),
+            "gpu_launches": 2 * K}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    proj.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        reference_main(a)
+    else:
+        b200_main(a)

@@ -307,6 +307,9 @@ void setup_projector(b200rt_projector& h) {
   p.min_y = g.desc().min_y;
   p.min_x = g.desc().min_x;
   p.max_row_len = max_len;
+  p.uniform_npa = g.npa(0);
+  for (int s = -g.S(); s <= g.S(); ++s)
+    if (g.npa(s) != p.uniform_npa) p.uniform_npa = 0;
   if (static_cast<int64_t>(p.nz) * p.ny * p.nx >= (int64_t(1) << 31)) throw std::runtime_error("image too large");
   const size_t smem = projector_smem_bytes(p);
   if (smem > 220 * 1024) throw std::runtime_error("basic row too long for shared memory");

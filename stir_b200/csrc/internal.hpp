@@ -77,6 +77,7 @@ struct ProjParams {
   int nz, ny, nx;      // image (device layout [y][x][z])
   int min_z, min_y, min_x;
   int max_row_len;
+  int uniform_npa;  // planes per axial position if equal for all segments, else 0
 };
 
 // launchers (project.cu)

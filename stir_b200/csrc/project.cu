@@ -42,19 +42,22 @@ __device__ __forceinline__ bool setup_line(const ProjParams& p, const ProjBinDev
   return true;
 }
 
-// a row element after the line's symmetry operation: column start (col*nz), z' - min_z
-// without the axial shift, and the value
+// A row element after the line's symmetry operation:
+//   base = col*nz + zt, the image index of the element for axial position 0,
+//   zt   = z' - min_z for axial position 0,
+//   full = 1 when z' stays inside [0,nz) for every axial position of the current pass, so the
+//          per-lane range checks can be skipped (a warp-uniform branch: all lanes read the same element).
 struct __align__(16) XElem {
-  int colbase;
+  int base;
   int zt;
   float v;
-  int pad;
+  int full;
 };
 
 constexpr int kChunk = 256;  // row elements transformed per warp at a time
 
 __device__ __forceinline__ void transform_chunk(const ProjParams& p, const RowElem* srow, int c0, int cn, const LineDev& L,
-                                                XElem* xbuf, int lane) {
+                                                int npa, int a_first, int a_last, XElem* xbuf, int lane) {
   const int swap = L.flags & 1;
   const int sx = (L.flags & 2) ? -1 : 1;
   const int sy = (L.flags & 4) ? -1 : 1;
@@ -67,9 +70,9 @@ __device__ __forceinline__ void transform_chunk(const ProjParams& p, const RowEl
     const int yt = (swap ? x : y) * sy;
     XElem o;
     o.zt = (zq ? static_cast<int>(L.q) - z : z) - p.min_z;
-    o.colbase = ((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz;
+    o.base = ((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz + o.zt;
     o.v = e.v;
-    o.pad = 0;
+    o.full = (o.zt + a_first * npa >= 0) && (o.zt + a_last * npa < p.nz);
     xbuf[k] = o;
   }
 }
@@ -78,6 +81,94 @@ __device__ __forceinline__ void stage_row(const ProjParams& p, const ProjBinDev&
   for (int i = threadIdx.x; i < pb.row_len; i += blockDim.x) srow[i] = p.rows[pb.row_offset + i];
 }
 
+// One pass of one line: NJ groups of 32 axial positions starting at a0 (lane j*32+lane is axial
+// a0+j*32+lane).  NPA: planes per axial position known at compile time (1, 2), or 0 for run time.
+template <int NPA, int NJ>
+__device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem* srow, int n, const LineDev& L,
+                                             const LineSetup& s, int a0, int nact, XElem* xbuf, int lane,
+                                             const float* __restrict__ img, float* __restrict__ out) {
+  const int npa = NPA ? NPA : s.npa;
+  const int step = 32 * npa;
+  const unsigned nz = static_cast<unsigned>(p.nz);
+  int zoff[NJ];
+  bool act[NJ];
+  float acc[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    act[j] = j * 32 + lane < nact;
+    zoff[j] = (a0 + j * 32 + lane) * npa;
+    acc[j] = 0.f;
+  }
+  for (int c0 = 0; c0 < n; c0 += kChunk) {
+    const int cn = min(kChunk, n - c0);
+    __syncwarp();
+    transform_chunk(p, srow, c0, cn, L, npa, a0, a0 + nact - 1, xbuf, lane);
+    __syncwarp();
+    for (int k = 0; k < cn; ++k) {
+      const XElem e = xbuf[k];
+      if (e.full) {
+        const float* q = img + (e.base + zoff[0]);
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+          if (act[j]) acc[j] += __ldg(q + j * step) * e.v;
+      } else {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const int zz = e.zt + zoff[j];
+          if (act[j] && static_cast<unsigned>(zz) < nz) acc[j] += __ldg(img + (e.base + zoff[j])) * e.v;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NJ; ++j)
+    if (act[j]) out[s.out_base + a0 + j * 32 + lane] = acc[j];
+}
+
+template <int NPA, int NJ>
+__device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* srow, int n, const LineDev& L,
+                                          const LineSetup& s, int a0, int nact, XElem* xbuf, int lane,
+                                          const float* __restrict__ pd, float* __restrict__ img) {
+  const int npa = NPA ? NPA : s.npa;
+  const int step = 32 * npa;
+  const unsigned nz = static_cast<unsigned>(p.nz);
+  int zoff[NJ];
+  bool act[NJ];
+  float d[NJ];
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    const bool in = j * 32 + lane < nact;
+    d[j] = in ? __ldg(pd + s.out_base + a0 + j * 32 + lane) : 0.f;
+    act[j] = d[j] != 0.f;  // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
+    zoff[j] = (a0 + j * 32 + lane) * npa;
+    any |= act[j];
+  }
+  if (!__any_sync(0xffffffffu, any)) return;
+  for (int c0 = 0; c0 < n; c0 += kChunk) {
+    const int cn = min(kChunk, n - c0);
+    __syncwarp();
+    transform_chunk(p, srow, c0, cn, L, npa, a0, a0 + nact - 1, xbuf, lane);
+    __syncwarp();
+    for (int k = 0; k < cn; ++k) {
+      const XElem e = xbuf[k];
+      if (e.full) {
+        float* q = img + (e.base + zoff[0]);
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+          if (act[j]) atomicAdd(q + j * step, e.v * d[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const int zz = e.zt + zoff[j];
+          if (act[j] && static_cast<unsigned>(zz) < nz) atomicAdd(img + (e.base + zoff[j]), e.v * d[j]);
+        }
+      }
+    }
+  }
+}
+
+template <int NPA>
 __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                            const float* __restrict__ img, float* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -88,44 +179,23 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
   const int n = pb.row_len;
   stage_row(p, pb, srow);
   __syncthreads();
-  const unsigned nz = static_cast<unsigned>(p.nz);
   for (int l = warp; l < pb.num_lines; l += kWarps) {
     const LineDev L = p.lines[pb.first_line + l];
     LineSetup s;
     if (!setup_line(p, pb, L, s)) continue;
     for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
-      int zoff[kAxPerLane];
-      float acc[kAxPerLane];
-#pragma unroll
-      for (int j = 0; j < kAxPerLane; ++j) {
-        const int a = a0 + j * 32 + lane;
-        // lanes past the last axial position get an offset that fails the range check
-        zoff[j] = a < s.nax ? a * s.npa : (1 << 29);
-        acc[j] = 0.f;
-      }
-      for (int c0 = 0; c0 < n; c0 += kChunk) {
-        const int cn = min(kChunk, n - c0);
-        __syncwarp();
-        transform_chunk(p, srow, c0, cn, L, xbuf, lane);
-        __syncwarp();
-        for (int k = 0; k < cn; ++k) {
-          const XElem e = xbuf[k];
-#pragma unroll
-          for (int j = 0; j < kAxPerLane; ++j) {
-            const int zz = e.zt + zoff[j];
-            if (static_cast<unsigned>(zz) < nz) acc[j] += __ldg(img + e.colbase + zz) * e.v;
-          }
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < kAxPerLane; ++j) {
-        const int a = a0 + j * 32 + lane;
-        if (a < s.nax) out[s.out_base + a] = acc[j];
+      const int nact = min(s.nax - a0, 32 * kAxPerLane);
+      switch ((nact + 31) >> 5) {
+        case 1: forward_pass<NPA, 1>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
+        case 2: forward_pass<NPA, 2>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
+        case 3: forward_pass<NPA, 3>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
+        default: forward_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
       }
     }
   }
 }
 
+template <int NPA>
 __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                                const float* __restrict__ pd, float* __restrict__ img) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -136,37 +206,17 @@ __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, con
   const int n = pb.row_len;
   stage_row(p, pb, srow);
   __syncthreads();
-  const unsigned nz = static_cast<unsigned>(p.nz);
   for (int l = warp; l < pb.num_lines; l += kWarps) {
     const LineDev L = p.lines[pb.first_line + l];
     LineSetup s;
     if (!setup_line(p, pb, L, s)) continue;
     for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
-      int zoff[kAxPerLane];
-      float d[kAxPerLane];
-      bool any = false;
-#pragma unroll
-      for (int j = 0; j < kAxPerLane; ++j) {
-        const int a = a0 + j * 32 + lane;
-        d[j] = a < s.nax ? __ldg(pd + s.out_base + a) : 0.f;
-        // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
-        zoff[j] = d[j] != 0.f ? a * s.npa : (1 << 29);
-        any |= d[j] != 0.f;
-      }
-      if (!__any_sync(0xffffffffu, any)) continue;
-      for (int c0 = 0; c0 < n; c0 += kChunk) {
-        const int cn = min(kChunk, n - c0);
-        __syncwarp();
-        transform_chunk(p, srow, c0, cn, L, xbuf, lane);
-        __syncwarp();
-        for (int k = 0; k < cn; ++k) {
-          const XElem e = xbuf[k];
-#pragma unroll
-          for (int j = 0; j < kAxPerLane; ++j) {
-            const int zz = e.zt + zoff[j];
-            if (static_cast<unsigned>(zz) < nz) atomicAdd(img + e.colbase + zz, e.v * d[j]);
-          }
-        }
+      const int nact = min(s.nax - a0, 32 * kAxPerLane);
+      switch ((nact + 31) >> 5) {
+        case 1: back_pass<NPA, 1>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
+        case 2: back_pass<NPA, 2>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
+        case 3: back_pass<NPA, 3>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
+        default: back_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
       }
     }
   }
@@ -214,24 +264,34 @@ static cudaError_t prepare_smem(const void* fn, size_t bytes) {
 
 size_t projector_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p); }
 
+template <typename K>
+static cudaError_t launch_proj(K kernel, const ProjParams& p, int nbins, cudaStream_t st, const int* list, const float* in,
+                               float* out) {
+  const size_t sm = proj_smem_bytes(p);
+  cudaError_t e = prepare_smem(reinterpret_cast<const void*>(kernel), sm);
+  if (e != cudaSuccess) return e;
+  kernel<<<nbins, kThreads, sm, st>>>(p, list, in, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
                            cudaStream_t st) {
   if (nbins <= 0) return cudaSuccess;
-  const size_t sm = proj_smem_bytes(p);
-  cudaError_t e = prepare_smem(reinterpret_cast<const void*>(forward_kernel), sm);
-  if (e != cudaSuccess) return e;
-  forward_kernel<<<nbins, kThreads, sm, st>>>(p, bin_list, image, projdata);
-  return cudaGetLastError();
+  switch (p.uniform_npa) {
+    case 1: return launch_proj(forward_kernel<1>, p, nbins, st, bin_list, image, projdata);
+    case 2: return launch_proj(forward_kernel<2>, p, nbins, st, bin_list, image, projdata);
+    default: return launch_proj(forward_kernel<0>, p, nbins, st, bin_list, image, projdata);
+  }
 }
 
 cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
                                cudaStream_t st) {
   if (nbins <= 0) return cudaSuccess;
-  const size_t sm = proj_smem_bytes(p);
-  cudaError_t e = prepare_smem(reinterpret_cast<const void*>(back_atomic_kernel), sm);
-  if (e != cudaSuccess) return e;
-  back_atomic_kernel<<<nbins, kThreads, sm, st>>>(p, bin_list, projdata, image);
-  return cudaGetLastError();
+  switch (p.uniform_npa) {
+    case 1: return launch_proj(back_atomic_kernel<1>, p, nbins, st, bin_list, projdata, image);
+    case 2: return launch_proj(back_atomic_kernel<2>, p, nbins, st, bin_list, projdata, image);
+    default: return launch_proj(back_atomic_kernel<0>, p, nbins, st, bin_list, projdata, image);
+  }
 }
 
 cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st) {

@@ -177,6 +177,45 @@ int b200rt_forward_project_dev(b200rt_projector* h, const float* image_dev, floa
 int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, float* image_dev,
                             int subset_num, int num_subsets, int mode, void* stream);
 
+/* ---- objective function and OSMAPOSL on device-resident data ----------- */
+
+/* Sensitivity of one subset: A^T m over the subset's bins, m = mult_dev (device layout) or ones
+ * when mult_dev is NULL, with the first and last axial position of segment 0 set to zero when
+ * zero_seg0_end_planes (PoissonLogLikelihoodWithLinearModelForMeanAndProjData::add_subset_sensitivity,
+ * src/recon_buildblock/PoissonLogLikelihoodWithLinearModelForMeanAndProjData.cxx:826-910, via
+ * RPC_process_related_viewgrams_sensitivity_computation :1517-1539).  sens_dev is overwritten. */
+int b200rt_sensitivity_dev(b200rt_projector* h, const float* mult_dev, float* sens_dev, int subset_num, int num_subsets,
+                           int zero_seg0_end_planes, void* stream);
+
+/* One OSMAPOSL sub-iteration on estimate_dev (in/out):
+ * OSMAPOSLReconstruction::update_estimate (src/iterative/OSMAPOSL/OSMAPOSLReconstruction.cxx:371-516)
+ * with the gradient of compute_sub_gradient_without_penalty_plus_sensitivity
+ * (RPC_process_related_viewgrams_gradient<true>, ...AndProjData.cxx:1421-1481):
+ *   u = A_S^T divide_and_truncate(y, A_S x + a);  u /= sens (or the MAP-OSL denominator of `prior`);
+ *   u clamped to [min_rel, max_rel] unless subiteration_num == 1;  x *= u.
+ * additive_dev may be NULL; prior may be NULL (no penalty).  update_dev (may be NULL) receives u.
+ * The forward projection, the ratio and the count of cancelled singularities are one kernel. */
+int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, const float* y_dev, const float* additive_dev,
+                                     const float* sens_dev, int subset_num, int num_subsets, int subiteration_num,
+                                     int zero_seg0_end_planes, const b200rt_prior* prior, float min_relative_change,
+                                     float max_relative_change, int back_projection_mode, float* update_dev, void* stream);
+/* singularities cancelled by divide_and_truncate in the last sub-iteration (distributable.cxx:590-594); synchronises */
+int b200rt_get_num_cancelled(b200rt_projector* h, int64_t* out);
+
+/* Poisson log-likelihood of one subset (accumulate_loglikelihood, src/buildblock/recon_array_functions.cxx:335-377,
+ * RPC_process_related_viewgrams_accumulate_loglikelihood, ...AndProjData.cxx:1483-1515):
+ * sum over bins of y log(ybar') - ybar', ybar' = max((A x + a) m, y/1e4), in FP64 with a fixed
+ * summation order.  additive_dev and mult_dev may be NULL.  Synchronises and writes *out. */
+int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const float* y_dev, const float* additive_dev,
+                              const float* mult_dev, int subset_num, int num_subsets, int zero_seg0_end_planes, double* out,
+                              void* stream);
+
+/* Prior gradient (QuadraticPrior::compute_gradient, src/recon_buildblock/QuadraticPrior.cxx:303-372;
+ * RelativeDifferencePrior::compute_gradient, src/recon_buildblock/RelativeDifferencePrior.cxx:376-452),
+ * images in device layout. */
+int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, float* gradient_dev,
+                              void* stream);
+
 /* ---- projectors on host arrays in STIR order (copies included) ---------- */
 int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host,
                            int subset_num, int num_subsets);

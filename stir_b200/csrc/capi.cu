@@ -1,5 +1,6 @@
 // C ABI of the B200 ray-tracing projector pair (include/stir_b200.h).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -93,6 +94,13 @@ struct b200rt_projector {
   // subset work lists
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf<int>>> subset_lists;
   std::map<std::pair<int, int>, int> subset_counts;
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf<int>>> subset_views;  // all views of the subset
+  std::map<std::pair<int, int>, int> subset_view_counts;
+  // OSMAPOSL scratch
+  DevBuf<float> ratio, upd, grad, small_value, partial_max, umax;
+  DevBuf<unsigned int> cancelled;
+  DevBuf<double> ll_partials, ll_sum;
+  float prior_w[27] = {0};
   // staging for the host API
   DevBuf<float> st_img_a, st_img_b, st_pd_a, st_pd_b;
   cudaStream_t stream = nullptr;
@@ -363,6 +371,52 @@ const int* subset_list(b200rt_projector& h, int subset, int nsub, int& count) {
   return p;
 }
 
+// device list of every view of the subset: the basic views and their symmetry partners
+const int* subset_views(b200rt_projector& h, int subset, int nsub, int& count) {
+  const auto key = std::make_pair(subset, nsub);
+  auto it = h.subset_views.find(key);
+  if (it != h.subset_views.end()) {
+    count = h.subset_view_counts[key];
+    return it->second->p;
+  }
+  const Geometry& g = *h.geo;
+  std::vector<char> in(g.num_views(), 0);
+  for (int v : g.basic_views()) {
+    if (v % nsub != subset) continue;
+    for (int seg : g.basic_segments()) {
+      std::vector<RelatedLine> rel;
+      g.related_lines(v, seg, true, rel);
+      for (const auto& r : rel) in[r.view] = 1;
+    }
+  }
+  std::vector<int> views;
+  for (int v = 0; v < g.num_views(); ++v)
+    if (in[v]) views.push_back(v);
+  auto buf = std::make_unique<DevBuf<int>>();
+  buf->upload(views, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "subset views");
+  count = static_cast<int>(views.size());
+  h.subset_view_counts[key] = count;
+  const int* p = buf->p;
+  h.subset_views[key] = std::move(buf);
+  return p;
+}
+
+// QuadraticPrior / RelativeDifferencePrior weights: voxel_x / distance (QuadraticPrior.cxx:203-230)
+void prior_weights(const Geometry& g, int only_2D, float w[27]) {
+  const float vz = g.desc().voxel_size_z, vy = g.desc().voxel_size_y, vx = g.desc().voxel_size_x;
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        float v = 0.f;
+        if (!(z == 0 && y == 0 && x == 0) && !(only_2D && z != 0)) {
+          const float a = static_cast<float>(x) * vx, b = static_cast<float>(y) * vy, c = static_cast<float>(z) * vz;
+          v = vx / std::sqrt(a * a + b * b + c * c);
+        }
+        w[(z + 1) * 9 + (y + 1) * 3 + (x + 1)] = v;
+      }
+}
+
 int check_subset(b200rt_projector* h, int subset, int nsub) {
   if (nsub < 1 || subset < 0 || subset >= nsub) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "invalid subset number");
   return B200RT_OK;
@@ -419,6 +473,16 @@ void b200rt_destroy(b200rt_projector* h) {
     DeviceGuard dg(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->subset_lists.clear();
+    h->subset_views.clear();
+    h->ratio.release();
+    h->upd.release();
+    h->grad.release();
+    h->small_value.release();
+    h->partial_max.release();
+    h->umax.release();
+    h->cancelled.release();
+    h->ll_partials.release();
+    h->ll_sum.release();
     h->rows.release();
     h->bins.release();
     h->lines.release();
@@ -603,6 +667,153 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
     ck(launch_image_from_dev(h->st_img_b.p, h->st_img_a.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
     ck(cudaMemcpyAsync(image_host, h->st_img_a.p, sizeof(float) * g.image_size(), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "back projection");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_sensitivity_dev(b200rt_projector* h, const float* mult_dev, float* sens_dev, int subset_num, int num_subsets,
+                           int zero_seg0_end_planes, void* stream) {
+  if (!h || !sens_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int n = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    ck(cudaMemsetAsync(sens_dev, 0, sizeof(float) * h->geo->image_size(), st), "memset");
+    ck(launch_back_atomic(h->params, list, n, mult_dev, sens_dev, st, zero_seg0_end_planes), "sensitivity");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, const float* y_dev, const float* additive_dev,
+                                     const float* sens_dev, int subset_num, int num_subsets, int subiteration_num,
+                                     int zero_seg0_end_planes, const b200rt_prior* prior, float min_relative_change,
+                                     float max_relative_change, int back_projection_mode, float* update_dev, void* stream) {
+  if (!h || !estimate_dev || !y_dev || !sens_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
+  if (prior && (prior->type < B200RT_PRIOR_NONE || prior->type > B200RT_PRIOR_RELATIVE_DIFFERENCE))
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown prior type");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t ni = g.image_size();
+    h->ratio.alloc(g.projdata_size());
+    if (!update_dev) h->upd.alloc(ni);
+    float* u = update_dev ? update_dev : h->upd.p;
+    h->small_value.alloc(static_cast<size_t>(2 * g.S() + 1) * g.num_views());
+    h->cancelled.alloc(1);
+    h->partial_max.alloc(update_num_blocks(ni));
+    h->umax.alloc(1);
+    const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+    if (has_prior) {
+      h->grad.alloc(ni);
+      prior_weights(g, prior->only_2D, h->prior_w);
+    }
+    int n = 0, nv = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    const int* views = subset_views(*h, subset_num, num_subsets, nv);
+    ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
+                                    h->small_value.p, st),
+       "viewgram thresholds");
+    ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
+    FwdEpilogue ep{};
+    ep.mode = kEpiRatio;
+    ep.zero_ends = zero_seg0_end_planes;
+    ep.y = y_dev;
+    ep.add = additive_dev;
+    ep.small_value = h->small_value.p;
+    ep.cancelled = h->cancelled.p;
+    ck(launch_forward(h->params, list, n, estimate_dev, h->ratio.p, st, &ep), "forward projection");
+    ck(cudaMemsetAsync(u, 0, sizeof(float) * ni, st), "memset");
+    if (back_projection_mode == B200RT_BACKPROJECT_ATOMIC)
+      ck(launch_back_atomic(h->params, list, n, h->ratio.p, u, st), "back projection");
+    else
+      return fail(h, B200RT_ERR_UNSUPPORTED, "deterministic back projection not available in this build");
+    ck(launch_update(u, estimate_dev, sens_dev, has_prior ? h->grad.p : nullptr, has_prior ? prior : nullptr, h->prior_w,
+                     num_subsets, subiteration_num, min_relative_change, max_relative_change, g.desc().ny, g.desc().nx,
+                     g.desc().nz, h->partial_max.p, h->umax.p, st),
+       "update");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_get_num_cancelled(b200rt_projector* h, int64_t* out) {
+  if (!h || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    unsigned int c = 0;
+    if (h->cancelled.p) ck(cudaMemcpy(&c, h->cancelled.p, sizeof(c), cudaMemcpyDeviceToHost), "D2H");
+    *out = c;
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const float* y_dev, const float* additive_dev,
+                              const float* mult_dev, int subset_num, int num_subsets, int zero_seg0_end_planes, double* out,
+                              void* stream) {
+  if (!h || !image_dev || !y_dev || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int n = 0, nv = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    const int* views = subset_views(*h, subset_num, num_subsets, nv);
+    h->small_value.alloc(static_cast<size_t>(2 * g.S() + 1) * g.num_views());
+    h->ll_partials.alloc(std::max(n, 1));
+    h->ll_sum.alloc(1);
+    ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
+                                    h->small_value.p, st),
+       "viewgram thresholds");
+    FwdEpilogue ep{};
+    ep.mode = kEpiLoglik;
+    ep.zero_ends = zero_seg0_end_planes;
+    ep.y = y_dev;
+    ep.add = additive_dev;
+    ep.mult = mult_dev;
+    ep.small_value = h->small_value.p;
+    ep.partials = h->ll_partials.p;
+    ck(launch_forward(h->params, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
+    ck(launch_reduce_sum(h->ll_partials.p, n, h->ll_sum.p, st), "reduce");
+    ck(cudaMemcpyAsync(out, h->ll_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "log-likelihood");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, float* gradient_dev,
+                              void* stream) {
+  if (!h || !prior || !image_dev || !gradient_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (prior->type < B200RT_PRIOR_NONE || prior->type > B200RT_PRIOR_RELATIVE_DIFFERENCE)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown prior type");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0) {
+      ck(cudaMemsetAsync(gradient_dev, 0, sizeof(float) * g.image_size(), st), "memset");
+      return B200RT_OK;
+    }
+    float w[27];
+    prior_weights(g, prior->only_2D, w);
+    h->partial_max.alloc(update_num_blocks(g.image_size()));
+    ck(launch_prior_gradient(image_dev, gradient_dev, prior, w, g.desc().ny, g.desc().nx, g.desc().nz, h->partial_max.p, st),
+       "prior gradient");
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());

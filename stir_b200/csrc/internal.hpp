@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/stir_b200.h"
+
 namespace b200 {
 
 // A stored row element: voxel (z,y,x) packed into 32 bits and its value.
@@ -80,16 +82,46 @@ struct ProjParams {
   int uniform_npa;  // planes per axial position if equal for all segments, else 0
 };
 
+// What the forward projector does with each projected bin A x:
+//   kEpiNone:   store it;
+//   kEpiRatio:  store divide_and_truncate(y, A x + a) (the OSMAPOSL gradient numerator);
+//   kEpiLoglik: accumulate the Poisson log-likelihood of y given (A x + a) m in FP64, per CTA.
+constexpr int kEpiNone = 0;
+constexpr int kEpiRatio = 1;
+constexpr int kEpiLoglik = 2;
+struct FwdEpilogue {
+  int mode;
+  int zero_ends;               // zero the first/last axial position of segment 0
+  const float* y;              // measured data (device layout)
+  const float* add;            // additive term or nullptr
+  const float* mult;           // multiplicative term or nullptr (log-likelihood only)
+  const float* small_value;    // per (segment+S)*num_views+view: max(viewgram y)*SMALL_NUM, >= 0
+  unsigned int* cancelled;     // number of ratios clipped at 1e4
+  double* partials;            // one log-likelihood partial sum per CTA
+};
+
 // launchers (project.cu)
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
-                           cudaStream_t st);
+                           cudaStream_t st, const FwdEpilogue* ep = nullptr);
+// projdata == nullptr back-projects ones
 cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
-                               cudaStream_t st);
+                               cudaStream_t st, int zero_ends = 0);
 cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st);
 cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny, int nx, cudaStream_t st);
 // per segment: STIR [ax][view*tang] <-> device [view*tang][ax]
 cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
+
+// OSMAPOSL pieces (osem.cu)
+cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
+                                         const int* views, int nviews, int zero_ends, float* out, cudaStream_t st);
+int update_num_blocks(int64_t n);
+cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
+                          const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
+                          int ny, int nx, int nz, float* partial_max, float* umax, cudaStream_t st);
+cudaError_t launch_prior_gradient(const float* x, float* g, const b200rt_prior* prior, const float prior_weights[27], int ny,
+                                  int nx, int nz, float* partial_max, cudaStream_t st);
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st);
 
 // row builder (rows.cu)
 struct RowKV {

@@ -1,0 +1,245 @@
+// Elementwise parts of the OSMAPOSL sub-iteration on device-resident images, and the
+// reductions around the fused forward-projection epilogue.
+//
+//   viewgram thresholds  divide_and_truncate's small_value per viewgram (recon_array_functions.cxx:185)
+//   prior gradient       QuadraticPrior::compute_gradient (QuadraticPrior.cxx:303-372),
+//                        RelativeDifferencePrior::compute_gradient (RelativeDifferencePrior.cxx:376-452)
+//   update               OSMAPOSLReconstruction::update_estimate (OSMAPOSLReconstruction.cxx:371-516):
+//                        division by the (MAP) denominator with divide()'s threshold (numerics/divide.inl:26-48),
+//                        threshold_upper_lower, multiplicative update
+//
+// Images use the device layout [y][x][z] (z fastest).
+#include "internal.hpp"
+
+namespace b200 {
+
+namespace {
+
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// one block per (segment, view) of the subset: max over the viewgram of y with segment 0 end planes zeroed
+__global__ void viewgram_small_value_kernel(const float* __restrict__ y, const SegDev* __restrict__ segs, int S, int num_views,
+                                            int num_tang, const int* __restrict__ views, int zero_ends, float* __restrict__ out) {
+  const int seg = static_cast<int>(blockIdx.y) - S;
+  const int view = views[blockIdx.x];
+  const SegDev sd = segs[seg + S];
+  const int64_t base = sd.dev_offset + static_cast<int64_t>(view) * num_tang * sd.nax;
+  const int n = num_tang * sd.nax;
+  float m = -INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int a = i % sd.nax;
+    float v = y[base + i];
+    if (zero_ends && seg == 0 && (a == 0 || a == sd.nax - 1)) v = 0.f;
+    m = fmaxf(m, v);
+  }
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+    m = warp_max(m);
+    if (threadIdx.x == 0) out[(seg + S) * num_views + view] = fmaxf(m * 0.000001F, 0.F);  // SMALL_NUM
+  }
+}
+
+struct PriorDev {
+  int type;
+  float beta, gamma, epsilon;
+  int dzmin, dzmax;
+  float w[27];  // [dz+1][dy+1][dx+1]
+  const float* kappa;
+};
+
+// RelativeDifferencePrior::derivative_10 (RelativeDifferencePrior.cxx:287-300)
+__device__ __forceinline__ float rdp_derivative_10(float x, float y, float gamma, float epsilon) {
+  if (epsilon == 0.0f && x == 0 && y == 0) return 0.f;
+  const double num = static_cast<double>(x - y) * (gamma * fabsf(x - y) + x + 3 * y + 2 * epsilon);
+  const double ds = static_cast<double>(x + y) + gamma * fabsf(x - y) + epsilon;
+  return static_cast<float>(num / (ds * ds));
+}
+
+// prior gradient of one voxel (double accumulation as STIR), device layout indices
+__device__ __forceinline__ float prior_gradient_at(const float* __restrict__ x, const PriorDev& pr, int yi, int xi, int zi,
+                                                   int ny, int nx, int nz) {
+  const int64_t i = (static_cast<int64_t>(yi) * nx + xi) * nz + zi;
+  const float xc = x[i];
+  double g = 0.0;
+  const int dz0 = max(pr.dzmin, -zi), dz1 = min(pr.dzmax, nz - 1 - zi);
+  const int dy0 = max(-1, -yi), dy1 = min(1, ny - 1 - yi);
+  const int dx0 = max(-1, -xi), dx1 = min(1, nx - 1 - xi);
+  for (int dz = dz0; dz <= dz1; ++dz)
+    for (int dy = dy0; dy <= dy1; ++dy)
+      for (int dx = dx0; dx <= dx1; ++dx) {
+        const int64_t j = i + (static_cast<int64_t>(dy) * nx + dx) * nz + dz;
+        const float xn = x[j];
+        const float w = pr.w[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+        double cur = (pr.type == 1) ? static_cast<double>(w * (xc - xn)) : static_cast<double>(w * rdp_derivative_10(xc, xn, pr.gamma, pr.epsilon));
+        if (pr.kappa) cur *= pr.kappa[i] * pr.kappa[j];
+        g += cur;
+      }
+  return static_cast<float>(g * pr.beta);
+}
+
+// pass 1: per-block max of the update image u, and the prior gradient (if any) into g
+__global__ void update_prepare_kernel(const float* __restrict__ u, const float* __restrict__ x, float* __restrict__ g, PriorDev pr,
+                                      int ny, int nx, int nz, float* __restrict__ partial_max) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  float m = -INFINITY;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    m = fmaxf(m, u[i]);
+    if (pr.type != 0) {
+      const int zi = static_cast<int>(i % nz);
+      const int64_t c = i / nz;
+      const int xi = static_cast<int>(c % nx), yi = static_cast<int>(c / nx);
+      g[i] = prior_gradient_at(x, pr, yi, xi, zi, ny, nx, nz);
+    }
+  }
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+    m = warp_max(m);
+    if (threadIdx.x == 0) partial_max[blockIdx.x] = m;
+  }
+}
+
+__global__ void reduce_max_kernel(const float* __restrict__ partial, int n, float* __restrict__ out) {
+  float m = -INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, partial[i]);
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+    m = warp_max(m);
+    if (threadIdx.x == 0) *out = m;
+  }
+}
+
+// pass 2: u /= denominator with divide()'s threshold, clamp, x *= u
+__global__ void update_apply_kernel(float* __restrict__ u, float* __restrict__ x, const float* __restrict__ sens,
+                                    const float* __restrict__ g, int prior, int map_model, float num_subsets,
+                                    const float* __restrict__ umax, float small_num, int clamp, float min_rel, float max_rel,
+                                    int64_t n) {
+  float sv = *umax * small_num;
+  sv = sv > 0 ? sv : 0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float s = sens[i];
+    float den;
+    if (!prior) {
+      den = s;
+    } else if (map_model == 0) {
+      // additive MAP model (OSMAPOSLReconstruction.cxx:415-433)
+      den = g[i] / num_subsets + s;
+      den = fmaxf(fminf(den, s * 10), s / 10);
+    } else {
+      // multiplicative MAP model (:436-453)
+      den = g[i] + 1;
+      den = fmaxf(fminf(den, 10.F), 1 / 10.F);
+      den *= s;
+    }
+    float v = u[i];
+    if (fabsf(den) <= sv && fabsf(v) <= sv)
+      v = 0;
+    else
+      v /= den;
+    if (clamp) {
+      // threshold_upper_lower (thresholding.h:45-54)
+      if (v > max_rel)
+        v = max_rel;
+      else if (min_rel > v)
+        v = min_rel;
+    }
+    u[i] = v;
+    x[i] *= v;
+  }
+}
+
+__global__ void reduce_sum_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+  // one block, fixed order per thread and a fixed tree: deterministic
+  __shared__ double red[256];
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t += partial[i];
+  red[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+}  // namespace
+
+cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
+                                         const int* views, int nviews, int zero_ends, float* out, cudaStream_t st) {
+  if (nviews <= 0) return cudaSuccess;
+  viewgram_small_value_kernel<<<dim3(nviews, 2 * S + 1), 256, 0, st>>>(y, segs, S, num_views, num_tang, views, zero_ends, out);
+  return cudaGetLastError();
+}
+
+int update_num_blocks(int64_t n) {
+  const int64_t b = (n + 255) / 256;
+  return static_cast<int>(b < 148 * 16 ? b : 148 * 16);
+}
+
+cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
+                          const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
+                          int ny, int nx, int nz, float* partial_max, float* umax, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  const int blocks = update_num_blocks(n);
+  PriorDev pr{};
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  pr.type = has_prior ? prior->type : 0;
+  if (has_prior) {
+    pr.beta = prior->penalisation_factor;
+    pr.gamma = prior->gamma;
+    pr.epsilon = prior->epsilon;
+    pr.dzmin = prior->only_2D ? 0 : -1;
+    pr.dzmax = prior->only_2D ? 0 : 1;
+    for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
+    pr.kappa = prior->kappa_dev;
+  }
+  update_prepare_kernel<<<blocks, 256, 0, st>>>(u, x, g, pr, ny, nx, nz, partial_max);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  reduce_max_kernel<<<1, 1024, 0, st>>>(partial_max, blocks, umax);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  update_apply_kernel<<<blocks, 256, 0, st>>>(u, x, sens, g, has_prior ? 1 : 0, has_prior ? prior->map_model : 0,
+                                               static_cast<float>(num_subsets), umax, has_prior ? 0.000001F : 0.F,
+                                               subiteration_num != 1, min_rel, max_rel, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prior_gradient(const float* x, float* g, const b200rt_prior* prior, const float prior_weights[27], int ny,
+                                  int nx, int nz, float* partial_max, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  PriorDev pr{};
+  pr.type = prior->type;
+  pr.beta = prior->penalisation_factor;
+  pr.gamma = prior->gamma;
+  pr.epsilon = prior->epsilon;
+  pr.dzmin = prior->only_2D ? 0 : -1;
+  pr.dzmax = prior->only_2D ? 0 : 1;
+  for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
+  pr.kappa = prior->kappa_dev;
+  update_prepare_kernel<<<update_num_blocks(n), 256, 0, st>>>(x, x, g, pr, ny, nx, nz, partial_max);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st) {
+  reduce_sum_kernel<<<1, 256, 0, st>>>(partial, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace b200

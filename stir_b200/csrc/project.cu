@@ -83,10 +83,11 @@ __device__ __forceinline__ void stage_row(const ProjParams& p, const ProjBinDev&
 
 // One pass of one line: NJ groups of 32 axial positions starting at a0 (lane j*32+lane is axial
 // a0+j*32+lane).  NPA: planes per axial position known at compile time (1, 2), or 0 for run time.
-template <int NPA, int NJ>
+template <int NPA, int NJ, int EPI>
 __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem* srow, int n, const LineDev& L,
                                              const LineSetup& s, int a0, int nact, XElem* xbuf, int lane,
-                                             const float* __restrict__ img, float* __restrict__ out) {
+                                             const float* __restrict__ img, float* __restrict__ out, const FwdEpilogue& ep,
+                                             double& ll, unsigned& ncancel) {
   const int npa = NPA ? NPA : s.npa;
   const int step = 32 * npa;
   const unsigned nz = static_cast<unsigned>(p.nz);
@@ -122,13 +123,49 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
   }
 #pragma unroll
   for (int j = 0; j < NJ; ++j)
-    if (act[j]) out[s.out_base + a0 + j * 32 + lane] = acc[j];
+    if (act[j]) {
+      const int a = a0 + j * 32 + lane;
+      const int64_t idx = s.out_base + a;
+      if (EPI == kEpiNone) {
+        out[idx] = acc[j];
+      } else {
+        // segment 0 end planes zeroed (distributable.cxx:146-158,216-221)
+        const bool zend = ep.zero_ends && L.seg == 0 && (a == 0 || a == s.nax - 1);
+        const float y = zend ? 0.f : __ldg(ep.y + idx);
+        const float av = (ep.add && !zend) ? __ldg(ep.add + idx) : 0.f;
+        const float sv = ep.small_value[(L.seg + p.S) * p.num_views + L.view];
+        if (EPI == kEpiRatio) {
+          // divide_and_truncate (recon_array_functions.cxx:171-266) of y by A x + a
+          const float den = acc[j] + av;
+          float r;
+          if (y <= sv) {
+            r = 0.f;
+          } else if (y > 10000.F * den) {
+            r = 10000.F;
+            ++ncancel;
+          } else {
+            r = y / den;
+          }
+          out[idx] = r;
+        } else {
+          // accumulate_loglikelihood (recon_array_functions.cxx:335-377) of ybar = (A x + a) * m
+          float e = acc[j] + av;
+          if (zend)
+            e *= 0.f;
+          else if (ep.mult)
+            e *= __ldg(ep.mult + idx);
+          const float ne = fmaxf(e, y / 10000.F);
+          ll += (y <= sv) ? -static_cast<double>(ne) : y * log(static_cast<double>(ne)) - static_cast<double>(ne);
+          if (out) out[idx] = e;
+        }
+      }
+    }
 }
 
 template <int NPA, int NJ>
 __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* srow, int n, const LineDev& L,
                                           const LineSetup& s, int a0, int nact, XElem* xbuf, int lane,
-                                          const float* __restrict__ pd, float* __restrict__ img) {
+                                          const float* __restrict__ pd, float* __restrict__ img, int zero_ends) {
   const int npa = NPA ? NPA : s.npa;
   const int step = 32 * npa;
   const unsigned nz = static_cast<unsigned>(p.nz);
@@ -138,8 +175,10 @@ __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* sr
   bool any = false;
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
-    const bool in = j * 32 + lane < nact;
-    d[j] = in ? __ldg(pd + s.out_base + a0 + j * 32 + lane) : 0.f;
+    const int a = a0 + j * 32 + lane;
+    const bool in = j * 32 + lane < nact && !(zero_ends && L.seg == 0 && (a == 0 || a == s.nax - 1));
+    // pd == nullptr back-projects ones (the sensitivity of RPC_process_related_viewgrams_sensitivity_computation)
+    d[j] = in ? (pd ? __ldg(pd + s.out_base + a) : 1.f) : 0.f;
     act[j] = d[j] != 0.f;  // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
     zoff[j] = (a0 + j * 32 + lane) * npa;
     any |= act[j];
@@ -168,9 +207,10 @@ __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* sr
   }
 }
 
-template <int NPA>
+template <int NPA, int EPI>
 __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                           const float* __restrict__ img, float* __restrict__ out) {
+                                                           const float* __restrict__ img, float* __restrict__ out,
+                                                           FwdEpilogue ep) {
   extern __shared__ __align__(16) unsigned char smem[];
   const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -179,6 +219,8 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
   const int n = pb.row_len;
   stage_row(p, pb, srow);
   __syncthreads();
+  double ll = 0.0;
+  unsigned ncancel = 0;
   for (int l = warp; l < pb.num_lines; l += kWarps) {
     const LineDev L = p.lines[pb.first_line + l];
     LineSetup s;
@@ -186,18 +228,36 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
     for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
       const int nact = min(s.nax - a0, 32 * kAxPerLane);
       switch ((nact + 31) >> 5) {
-        case 1: forward_pass<NPA, 1>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
-        case 2: forward_pass<NPA, 2>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
-        case 3: forward_pass<NPA, 3>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
-        default: forward_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out); break;
+        case 1: forward_pass<NPA, 1, EPI>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out, ep, ll, ncancel); break;
+        case 2: forward_pass<NPA, 2, EPI>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out, ep, ll, ncancel); break;
+        case 3: forward_pass<NPA, 3, EPI>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out, ep, ll, ncancel); break;
+        default: forward_pass<NPA, 4, EPI>(p, srow, n, L, s, a0, nact, xbuf, lane, img, out, ep, ll, ncancel); break;
       }
+    }
+  }
+  if (EPI == kEpiRatio) {
+    // cancelled singularities (distributable.cxx:590-594)
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
+  }
+  if (EPI == kEpiLoglik) {
+    // per-CTA partial sums, reduced in a fixed order by the caller: deterministic
+    __shared__ double red[kWarps];
+    for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
+    if (lane == 0) red[warp] = ll;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kWarps; ++w) t += red[w];
+      ep.partials[blockIdx.x] = t;
     }
   }
 }
 
 template <int NPA>
 __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                               const float* __restrict__ pd, float* __restrict__ img) {
+                                                               const float* __restrict__ pd, float* __restrict__ img,
+                                                               int zero_ends) {
   extern __shared__ __align__(16) unsigned char smem[];
   const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -213,10 +273,10 @@ __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, con
     for (int a0 = 0; a0 < s.nax; a0 += 32 * kAxPerLane) {
       const int nact = min(s.nax - a0, 32 * kAxPerLane);
       switch ((nact + 31) >> 5) {
-        case 1: back_pass<NPA, 1>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
-        case 2: back_pass<NPA, 2>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
-        case 3: back_pass<NPA, 3>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
-        default: back_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img); break;
+        case 1: back_pass<NPA, 1>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img, zero_ends); break;
+        case 2: back_pass<NPA, 2>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img, zero_ends); break;
+        case 3: back_pass<NPA, 3>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img, zero_ends); break;
+        default: back_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img, zero_ends); break;
       }
     }
   }
@@ -264,33 +324,41 @@ static cudaError_t prepare_smem(const void* fn, size_t bytes) {
 
 size_t projector_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p); }
 
-template <typename K>
-static cudaError_t launch_proj(K kernel, const ProjParams& p, int nbins, cudaStream_t st, const int* list, const float* in,
-                               float* out) {
+template <typename K, typename... A>
+static cudaError_t launch_proj(K kernel, const ProjParams& p, int nbins, cudaStream_t st, A... args) {
   const size_t sm = proj_smem_bytes(p);
   cudaError_t e = prepare_smem(reinterpret_cast<const void*>(kernel), sm);
   if (e != cudaSuccess) return e;
-  kernel<<<nbins, kThreads, sm, st>>>(p, list, in, out);
+  kernel<<<nbins, kThreads, sm, st>>>(p, args...);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
-                           cudaStream_t st) {
-  if (nbins <= 0) return cudaSuccess;
+template <int EPI>
+static cudaError_t launch_forward_epi(const ProjParams& p, const int* list, int nbins, const float* image, float* out,
+                                      const FwdEpilogue& ep, cudaStream_t st) {
   switch (p.uniform_npa) {
-    case 1: return launch_proj(forward_kernel<1>, p, nbins, st, bin_list, image, projdata);
-    case 2: return launch_proj(forward_kernel<2>, p, nbins, st, bin_list, image, projdata);
-    default: return launch_proj(forward_kernel<0>, p, nbins, st, bin_list, image, projdata);
+    case 1: return launch_proj(forward_kernel<1, EPI>, p, nbins, st, list, image, out, ep);
+    case 2: return launch_proj(forward_kernel<2, EPI>, p, nbins, st, list, image, out, ep);
+    default: return launch_proj(forward_kernel<0, EPI>, p, nbins, st, list, image, out, ep);
   }
 }
 
+cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
+                           cudaStream_t st, const FwdEpilogue* ep) {
+  if (nbins <= 0) return cudaSuccess;
+  FwdEpilogue none{};
+  if (!ep || ep->mode == kEpiNone) return launch_forward_epi<kEpiNone>(p, bin_list, nbins, image, projdata, none, st);
+  if (ep->mode == kEpiRatio) return launch_forward_epi<kEpiRatio>(p, bin_list, nbins, image, projdata, *ep, st);
+  return launch_forward_epi<kEpiLoglik>(p, bin_list, nbins, image, projdata, *ep, st);
+}
+
 cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
-                               cudaStream_t st) {
+                               cudaStream_t st, int zero_ends) {
   if (nbins <= 0) return cudaSuccess;
   switch (p.uniform_npa) {
-    case 1: return launch_proj(back_atomic_kernel<1>, p, nbins, st, bin_list, projdata, image);
-    case 2: return launch_proj(back_atomic_kernel<2>, p, nbins, st, bin_list, projdata, image);
-    default: return launch_proj(back_atomic_kernel<0>, p, nbins, st, bin_list, projdata, image);
+    case 1: return launch_proj(back_atomic_kernel<1>, p, nbins, st, bin_list, projdata, image, zero_ends);
+    case 2: return launch_proj(back_atomic_kernel<2>, p, nbins, st, bin_list, projdata, image, zero_ends);
+    default: return launch_proj(back_atomic_kernel<0>, p, nbins, st, bin_list, projdata, image, zero_ends);
   }
 }
 

@@ -210,6 +210,25 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
                               const float* mult_dev, int subset_num, int num_subsets, int zero_seg0_end_planes, double* out,
                               void* stream);
 
+/* Allocation-free variant of b200rt_log_likelihood_dev.  No counterpart in the reference.
+ * For callers that must not allocate device memory once they are set up: for example a
+ * reconstruction service that hands all device memory to a caching allocator at start-up, or
+ * that cannot afford the device-wide synchronisation a cudaMalloc/cudaFree implies in the middle
+ * of a frame.  This call allocates nothing: its scratch (the subset's bin list, the viewgram
+ * thresholds and one partial sum per CTA) lives in a fixed 1.77 MiB array compiled into the
+ * library, which every GPU that loads the library holds until the process exits.
+ *   - limits: at most 131072 basic bins in the subset, 4096 views, 65536 viewgrams
+ *     ((2*max_segment_num+1)*num_views); larger requests return B200RT_ERR_TOO_LARGE;
+ *   - the result is written to out_dev, a device double the caller provides; the call is
+ *     asynchronous on `stream` and does not synchronise;
+ *   - all calls share the one array: calls that overlap on the GPU (other streams, other threads)
+ *     race and corrupt each other's results;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress); make
+ *     that first call before any stream capture. */
+int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const float* image_dev, const float* y_dev,
+                                      const float* additive_dev, const float* mult_dev, int subset_num, int num_subsets,
+                                      int zero_seg0_end_planes, double* out_dev, void* stream);
+
 /* Prior gradient (QuadraticPrior::compute_gradient, src/recon_buildblock/QuadraticPrior.cxx:303-372;
  * RelativeDifferencePrior::compute_gradient, src/recon_buildblock/RelativeDifferencePrior.cxx:376-452),
  * images in device layout. */

@@ -51,8 +51,9 @@ extern "C" {
 #define B200RT_ERR_TOO_LARGE (-7)
 
 /* back-projection accumulation modes */
-#define B200RT_BACKPROJECT_ATOMIC 0        /* scatter with float atomics (fast)        */
-#define B200RT_BACKPROJECT_DETERMINISTIC 1 /* voxel-driven gather, fixed summation order */
+#define B200RT_BACKPROJECT_ATOMIC 0        /* scatter with float atomics (fast; order-dependent rounding)  */
+#define B200RT_BACKPROJECT_DETERMINISTIC 1 /* contributions summed as 64-bit fixed point: order-independent,
+                                              bit-identical from run to run */
 
 /* priors (src/recon_buildblock/QuadraticPrior.cxx, RelativeDifferencePrior.cxx) */
 #define B200RT_PRIOR_NONE 0
@@ -183,9 +184,10 @@ int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, floa
  * when mult_dev is NULL, with the first and last axial position of segment 0 set to zero when
  * zero_seg0_end_planes (PoissonLogLikelihoodWithLinearModelForMeanAndProjData::add_subset_sensitivity,
  * src/recon_buildblock/PoissonLogLikelihoodWithLinearModelForMeanAndProjData.cxx:826-910, via
- * RPC_process_related_viewgrams_sensitivity_computation :1517-1539).  sens_dev is overwritten. */
+ * RPC_process_related_viewgrams_sensitivity_computation :1517-1539).  sens_dev is overwritten.
+ * back_projection_mode: B200RT_BACKPROJECT_ATOMIC or _DETERMINISTIC. */
 int b200rt_sensitivity_dev(b200rt_projector* h, const float* mult_dev, float* sens_dev, int subset_num, int num_subsets,
-                           int zero_seg0_end_planes, void* stream);
+                           int zero_seg0_end_planes, int back_projection_mode, void* stream);
 
 /* One OSMAPOSL sub-iteration on estimate_dev (in/out):
  * OSMAPOSLReconstruction::update_estimate (src/iterative/OSMAPOSL/OSMAPOSLReconstruction.cxx:371-516)

@@ -127,7 +127,7 @@ EXPORTS = [
     ("b200rt_projdata_from_device_layout", _I, [_P, _P, _P, _P]),
     ("b200rt_forward_project_dev", _I, [_P, _P, _P, _I, _I, _P]),
     ("b200rt_back_project_dev", _I, [_P, _P, _P, _I, _I, _I, _P]),
-    ("b200rt_sensitivity_dev", _I, [_P, _P, _P, _I, _I, _I, _P]),
+    ("b200rt_sensitivity_dev", _I, [_P, _P, _P, _I, _I, _I, _I, _P]),
     ("b200rt_osmaposl_subiteration_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(Prior), ctypes.c_float,
                                               ctypes.c_float, _I, _P, _P]),
     ("b200rt_get_num_cancelled", _I, [_P, ctypes.POINTER(_I64)]),

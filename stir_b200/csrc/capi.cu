@@ -100,6 +100,12 @@ struct b200rt_projector {
   DevBuf<float> ratio, upd, grad, small_value, partial_max, umax;
   DevBuf<unsigned int> cancelled;
   DevBuf<double> ll_partials, ll_sum;
+  // deterministic back projection
+  DevBuf<unsigned long long> acc64;
+  DevBuf<double> fixed_scale;
+  DevBuf<float> colmax, det_partial, det_bound;
+  float det_bound_value = 0.f;
+  bool colmax_ready = false;
   float prior_w[27] = {0};
   // staging for the host API
   DevBuf<float> st_img_a, st_img_b, st_pd_a, st_pd_b;
@@ -417,6 +423,48 @@ void prior_weights(const Geometry& g, int only_2D, float w[27]) {
       }
 }
 
+// Back projection of the subset into image_dev (overwritten), atomic or deterministic.
+// max_abs > 0: a bound on |pd| known in advance (the OSMAPOSL ratio is at most 1e4), which keeps the
+// fixed-point scale independent of bins outside the subset
+void back_project_into(b200rt_projector& h, const float* pd, float* image, int subset, int nsub, int mode, int zero_ends,
+                       cudaStream_t st, float max_abs = 0.f) {
+  const Geometry& g = *h.geo;
+  const int64_t ni = g.image_size();
+  int n = 0;
+  const int* list = subset_list(h, subset, nsub, n);
+  if (mode == B200RT_BACKPROJECT_ATOMIC) {
+    ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
+    ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
+    return;
+  }
+  h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(g.projdata_size(), ni)), 1));
+  if (!h.colmax_ready) {
+    // largest column sum of A (A^T 1 over every bin): bounds every voxel's sum of |w d| / max|d|
+    h.colmax.alloc(1);
+    int nall = 0;
+    const int* all = subset_list(h, 0, 1, nall);
+    ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
+    ck(launch_back_atomic(h.params, all, nall, nullptr, image, st, 0), "column sums");
+    ck(launch_max(image, ni, h.det_partial.p, h.colmax.p, st), "column sums");
+    h.colmax_ready = true;
+  }
+  h.acc64.alloc(ni);
+  h.fixed_scale.alloc(1);
+  if (max_abs > 0) {
+    if (h.det_bound_value != max_abs) {
+      h.det_bound.alloc(1);
+      ck(cudaMemcpy(h.det_bound.p, &max_abs, sizeof(float), cudaMemcpyHostToDevice), "H2D");
+      h.det_bound_value = max_abs;
+    }
+    ck(launch_fixed_scale(h.det_bound.p, 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
+  } else {
+    ck(launch_fixed_scale(pd, pd ? g.projdata_size() : 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
+  }
+  ck(cudaMemsetAsync(h.acc64.p, 0, sizeof(unsigned long long) * ni, st), "memset");
+  ck(launch_back_fixed(h.params, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends), "back projection");
+  ck(launch_fixed_to_float(h.acc64.p, h.fixed_scale.p, image, ni, st), "back projection");
+}
+
 int check_subset(b200rt_projector* h, int subset, int nsub) {
   if (nsub < 1 || subset < 0 || subset >= nsub) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "invalid subset number");
   return B200RT_OK;
@@ -482,6 +530,11 @@ void b200rt_destroy(b200rt_projector* h) {
     h->umax.release();
     h->cancelled.release();
     h->ll_partials.release();
+    h->acc64.release();
+    h->fixed_scale.release();
+    h->colmax.release();
+    h->det_partial.release();
+    h->det_bound.release();
     h->ll_sum.release();
     h->rows.release();
     h->bins.release();
@@ -604,14 +657,11 @@ int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, floa
                             int num_subsets, int mode, void* stream) {
   if (!h || !image_dev || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
-  if (mode != B200RT_BACKPROJECT_ATOMIC) return fail(h, B200RT_ERR_UNSUPPORTED, "back-projection mode not available");
+  if (mode != B200RT_BACKPROJECT_ATOMIC && mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
   try {
     DeviceGuard dg(h->device);
-    const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int n = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    ck(cudaMemsetAsync(image_dev, 0, sizeof(float) * h->geo->image_size(), st), "memset");
-    ck(launch_back_atomic(h->params, list, n, projdata_dev, image_dev, st), "back projection");
+    back_project_into(*h, projdata_dev, image_dev, subset_num, num_subsets, mode, 0, static_cast<cudaStream_t>(stream));
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());
@@ -649,7 +699,8 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
                         int num_subsets, int mode) {
   if (!h || !image_host || !projdata_host) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
-  if (mode != B200RT_BACKPROJECT_ATOMIC) return fail(h, B200RT_ERR_UNSUPPORTED, "back-projection mode not available");
+  if (mode != B200RT_BACKPROJECT_ATOMIC && mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
   try {
     DeviceGuard dg(h->device);
     const Geometry& g = *h->geo;
@@ -660,10 +711,7 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
     h->st_pd_b.alloc(g.projdata_size());
     ck(cudaMemcpyAsync(h->st_pd_a.p, projdata_host, sizeof(float) * g.projdata_size(), cudaMemcpyHostToDevice, st), "H2D");
     ck(projdata_layout(g, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
-    int n = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    ck(cudaMemsetAsync(h->st_img_b.p, 0, sizeof(float) * g.image_size(), st), "memset");
-    ck(launch_back_atomic(h->params, list, n, h->st_pd_b.p, h->st_img_b.p, st), "back projection");
+    back_project_into(*h, h->st_pd_b.p, h->st_img_b.p, subset_num, num_subsets, mode, 0, st);
     ck(launch_image_from_dev(h->st_img_b.p, h->st_img_a.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
     ck(cudaMemcpyAsync(image_host, h->st_img_a.p, sizeof(float) * g.image_size(), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "back projection");
@@ -674,16 +722,15 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
 }
 
 int b200rt_sensitivity_dev(b200rt_projector* h, const float* mult_dev, float* sens_dev, int subset_num, int num_subsets,
-                           int zero_seg0_end_planes, void* stream) {
+                           int zero_seg0_end_planes, int back_projection_mode, void* stream) {
   if (!h || !sens_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
   try {
     DeviceGuard dg(h->device);
-    const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int n = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    ck(cudaMemsetAsync(sens_dev, 0, sizeof(float) * h->geo->image_size(), st), "memset");
-    ck(launch_back_atomic(h->params, list, n, mult_dev, sens_dev, st, zero_seg0_end_planes), "sensitivity");
+    back_project_into(*h, mult_dev, sens_dev, subset_num, num_subsets, back_projection_mode, zero_seg0_end_planes,
+                      static_cast<cudaStream_t>(stream));
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());
@@ -705,7 +752,10 @@ int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, c
     const Geometry& g = *h->geo;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t ni = g.image_size();
-    h->ratio.alloc(g.projdata_size());
+    if (!h->ratio.p) {
+      h->ratio.alloc(g.projdata_size());
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");  // bins outside the subset
+    }
     if (!update_dev) h->upd.alloc(ni);
     float* u = update_dev ? update_dev : h->upd.p;
     h->small_value.alloc(static_cast<size_t>(2 * g.S() + 1) * g.num_views());
@@ -732,11 +782,7 @@ int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, c
     ep.small_value = h->small_value.p;
     ep.cancelled = h->cancelled.p;
     ck(launch_forward(h->params, list, n, estimate_dev, h->ratio.p, st, &ep), "forward projection");
-    ck(cudaMemsetAsync(u, 0, sizeof(float) * ni, st), "memset");
-    if (back_projection_mode == B200RT_BACKPROJECT_ATOMIC)
-      ck(launch_back_atomic(h->params, list, n, h->ratio.p, u, st), "back projection");
-    else
-      return fail(h, B200RT_ERR_UNSUPPORTED, "deterministic back projection not available in this build");
+    back_project_into(*h, h->ratio.p, u, subset_num, num_subsets, back_projection_mode, 0, st, 10000.F);
     ck(launch_update(u, estimate_dev, sens_dev, has_prior ? h->grad.p : nullptr, has_prior ? prior : nullptr, h->prior_w,
                      num_subsets, subiteration_num, min_relative_change, max_relative_change, g.desc().ny, g.desc().nx,
                      g.desc().nz, h->partial_max.p, h->umax.p, st),

@@ -112,6 +112,16 @@ cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny,
 cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
 
+// deterministic back projection: contributions accumulated as int64 multiples of 1/scale
+cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbins, const float* projdata,
+                              unsigned long long* acc, const double* scale, cudaStream_t st, int zero_ends = 0);
+// max |projdata| (nullptr data = 1) and the fixed-point scale 2^floor(62 - log2(max|d| * colmax * 1.01)) (osem.cu)
+cudaError_t launch_fixed_scale(const float* projdata, int64_t n, const float* colmax, float* partial, double* scale,
+                               cudaStream_t st);
+cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* scale, float* image, int64_t n,
+                                  cudaStream_t st);
+cudaError_t launch_max(const float* data, int64_t n, float* partial, float* out, cudaStream_t st);
+
 // OSMAPOSL pieces (osem.cu)
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, float* out, cudaStream_t st);

@@ -178,7 +178,75 @@ __global__ void reduce_sum_kernel(const double* __restrict__ partial, int n, dou
   if (threadIdx.x == 0) *out = red[0];
 }
 
+// per-block max |x| (data == nullptr stands for ones)
+__global__ void absmax_kernel(const float* __restrict__ data, int64_t n, float* __restrict__ partial) {
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    m = fmaxf(m, data ? fabsf(data[i]) : 1.f);
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    m = warp_max(m);
+    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+  }
+}
+
+// scale = 2^floor(62 - log2(bound)): every partial sum of |w d| over a voxel is at most
+// max|d| * max column sum of A, so the int64 accumulator cannot overflow
+__global__ void fixed_scale_kernel(const float* __restrict__ partial, int n, const float* __restrict__ colmax,
+                                   double* __restrict__ scale) {
+  float m = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, partial[i]);
+  __shared__ float red[32];
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
+    const double bound = static_cast<double>(t) * static_cast<double>(*colmax) * 1.01 + 1e-30;
+    *scale = exp2(fmin(floor(62.0 - log2(bound)), 1000.0));
+  }
+}
+
+__global__ void fixed_to_float_kernel(const unsigned long long* __restrict__ acc, const double* __restrict__ scale,
+                                      float* __restrict__ img, int64_t n) {
+  const double inv = 1.0 / *scale;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    img[i] = static_cast<float>(static_cast<double>(static_cast<long long>(acc[i])) * inv);
+}
+
 }  // namespace
+
+cudaError_t launch_max(const float* data, int64_t n, float* partial, float* out, cudaStream_t st) {
+  const int blocks = update_num_blocks(n);
+  absmax_kernel<<<blocks, 256, 0, st>>>(data, n, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  reduce_max_kernel<<<1, 1024, 0, st>>>(partial, blocks, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixed_scale(const float* projdata, int64_t n, const float* colmax, float* partial, double* scale,
+                               cudaStream_t st) {
+  const int blocks = update_num_blocks(n);
+  absmax_kernel<<<blocks, 256, 0, st>>>(projdata, n, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  fixed_scale_kernel<<<1, 1024, 0, st>>>(partial, blocks, colmax, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* scale, float* image, int64_t n,
+                                  cudaStream_t st) {
+  fixed_to_float_kernel<<<update_num_blocks(n), 256, 0, st>>>(acc, scale, image, n);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, float* out, cudaStream_t st) {

@@ -162,10 +162,26 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
     }
 }
 
-template <int NPA, int NJ>
+// Accumulation of one back-projected contribution w*d:
+//   float image: red.global.add.f32 (order-dependent rounding);
+//   fixed point: the contribution rounded to an integer multiple of 1/scale (scale a power of two) and added
+//   with 64-bit integer atomics, so the sum is the same whatever the order of the additions (deterministic mode).
+struct FloatAcc {
+  float* img;
+  __device__ __forceinline__ void add(int64_t i, float v) const { atomicAdd(img + i, v); }
+};
+struct FixedAcc {
+  unsigned long long* acc;
+  const double* scale;
+  __device__ __forceinline__ void add(int64_t i, float v) const {
+    atomicAdd(acc + i, static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(v) * *scale)));
+  }
+};
+
+template <int NPA, int NJ, typename Acc>
 __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* srow, int n, const LineDev& L,
                                           const LineSetup& s, int a0, int nact, XElem* xbuf, int lane,
-                                          const float* __restrict__ pd, float* __restrict__ img, int zero_ends) {
+                                          const float* __restrict__ pd, const Acc& out, int zero_ends) {
   const int npa = NPA ? NPA : s.npa;
   const int step = 32 * npa;
   const unsigned nz = static_cast<unsigned>(p.nz);
@@ -192,15 +208,15 @@ __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* sr
     for (int k = 0; k < cn; ++k) {
       const XElem e = xbuf[k];
       if (e.full) {
-        float* q = img + (e.base + zoff[0]);
+        const int64_t q = e.base + zoff[0];
 #pragma unroll
         for (int j = 0; j < NJ; ++j)
-          if (act[j]) atomicAdd(q + j * step, e.v * d[j]);
+          if (act[j]) out.add(q + j * step, e.v * d[j]);
       } else {
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
           const int zz = e.zt + zoff[j];
-          if (act[j] && static_cast<unsigned>(zz) < nz) atomicAdd(img + (e.base + zoff[j]), e.v * d[j]);
+          if (act[j] && static_cast<unsigned>(zz) < nz) out.add(e.base + zoff[j], e.v * d[j]);
         }
       }
     }
@@ -254,10 +270,9 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
   }
 }
 
-template <int NPA>
+template <int NPA, typename Acc>
 __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                               const float* __restrict__ pd, float* __restrict__ img,
-                                                               int zero_ends) {
+                                                               const float* __restrict__ pd, Acc img, int zero_ends) {
   extern __shared__ __align__(16) unsigned char smem[];
   const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -352,14 +367,25 @@ cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, 
   return launch_forward_epi<kEpiLoglik>(p, bin_list, nbins, image, projdata, *ep, st);
 }
 
-cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
-                               cudaStream_t st, int zero_ends) {
+template <typename Acc>
+static cudaError_t launch_back_acc(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, Acc acc,
+                                   cudaStream_t st, int zero_ends) {
   if (nbins <= 0) return cudaSuccess;
   switch (p.uniform_npa) {
-    case 1: return launch_proj(back_atomic_kernel<1>, p, nbins, st, bin_list, projdata, image, zero_ends);
-    case 2: return launch_proj(back_atomic_kernel<2>, p, nbins, st, bin_list, projdata, image, zero_ends);
-    default: return launch_proj(back_atomic_kernel<0>, p, nbins, st, bin_list, projdata, image, zero_ends);
+    case 1: return launch_proj(back_atomic_kernel<1, Acc>, p, nbins, st, bin_list, projdata, acc, zero_ends);
+    case 2: return launch_proj(back_atomic_kernel<2, Acc>, p, nbins, st, bin_list, projdata, acc, zero_ends);
+    default: return launch_proj(back_atomic_kernel<0, Acc>, p, nbins, st, bin_list, projdata, acc, zero_ends);
   }
+}
+
+cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
+                               cudaStream_t st, int zero_ends) {
+  return launch_back_acc(p, bin_list, nbins, projdata, FloatAcc{image}, st, zero_ends);
+}
+
+cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbins, const float* projdata,
+                              unsigned long long* acc, const double* scale, cudaStream_t st, int zero_ends) {
+  return launch_back_acc(p, bin_list, nbins, projdata, FixedAcc{acc, scale}, st, zero_ends);
 }
 
 cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st) {

@@ -94,7 +94,7 @@ class OSMAPOSLReconstruction:
         for s in range(self.num_subsets):
             t = self.proj.empty_image(zero=False)
             _abi.check(lib.b200rt_sensitivity_dev(h, _ptr(self.mult), _ptr(t), s, self.num_subsets,
-                                                  int(self.zero_seg0_end_planes), _stream_ptr(self.stream)), h,
+                                                  int(self.zero_seg0_end_planes), self.mode, _stream_ptr(self.stream)), h,
                        "b200rt_sensitivity_dev")
             subs.append(t)
         if self.use_subset_sensitivities:

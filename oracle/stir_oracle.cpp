@@ -325,27 +325,33 @@ template <typename T> void setup_geometry(Geometry<T>& g, const b200rt_geometry&
     off += static_cast<int64_t>(g.nax(s)) * g.num_views * g.num_tang;
   }
   g.tof_stride = off;
-  /* TOF bins (ProjDataInfo::set_tof_mash_factor, ProjDataInfo.cxx:174-255) */
+  /* TOF bins (ProjDataInfo::set_tof_mash_factor, ProjDataInfo.cxx:174-255; get_k / get_sampling_in_k :69-92) */
   g.num_tof = 1;
   g.min_tof = g.max_tof = 0;
   if (d.tof_mash_factor > 0) {
     const int max_poss = d.max_num_timing_poss;
+    if (max_poss < 1 || max_poss % d.tof_mash_factor) throw std::runtime_error("bad TOF mashing");
     g.num_tof = max_poss / d.tof_mash_factor;
-    g.min_tof = -(g.num_tof / 2);
+    g.min_tof = -g.num_tof / 2;
     g.max_tof = g.min_tof + g.num_tof - 1;
-    if (g.num_tof < 1) throw std::runtime_error("bad TOF mashing");
-    /* tof_delta_time_to_mm (TOF_conversions.h:18-34): c/2 in mm/ps */
-    auto delta_t_to_mm = [](double ps) { return static_cast<T>(ps * 0.299792458 / 2.0); };
-    const T tof_width = delta_t_to_mm(d.size_of_timing_pos_ps * d.tof_mash_factor);
+    /* tof_delta_time_to_mm (TOF_conversions.h:31-34): speed of light / 2 in mm/ps */
+    const double c_half = 0.299792458 * 0.5;
+    const float fmash_size = static_cast<float>(d.tof_mash_factor) * d.size_of_timing_pos_ps;
+    const T inc = static_cast<T>(static_cast<float>(static_cast<double>(fmash_size) * c_half));
+    auto get_k = [&](int k) {
+      return (g.num_tof % 2) ? static_cast<T>(k) * inc : static_cast<T>(k) * inc + inc / T(2.f);
+    };
     g.tof_low.resize(g.num_tof);
     g.tof_high.resize(g.num_tof);
     for (int k = g.min_tof; k <= g.max_tof; ++k) {
-      const T cur_low = (static_cast<T>(k) - T(0.5F)) * tof_width;  /* ProjDataInfo.cxx:226-237 */
-      g.tof_low[k - g.min_tof] = cur_low;
-      g.tof_high[k - g.min_tof] = cur_low + tof_width;
+      const T sampling = (get_k(k + 1) - get_k(k - 1)) / T(2.f);
+      const T centre = get_k(k);
+      g.tof_low[k - g.min_tof] = centre - sampling / T(2.f);
+      g.tof_high[k - g.min_tof] = centre + sampling / T(2.f);
     }
-    const T sigma = delta_t_to_mm(d.timing_resolution_ps) / T(2.355F);
-    g.r_sqrt2_gauss_sigma = T(1.0F) / (sigma * static_cast<T>(std::sqrt(2.0)));
+    /* ProjMatrixByBin::enable_tof (ProjMatrixByBin.cxx:66-75) */
+    const T sigma = static_cast<T>(static_cast<float>(static_cast<double>(d.timing_resolution_ps) * c_half)) / T(2.355f);
+    g.r_sqrt2_gauss_sigma = T(1.0f) / (sigma * static_cast<T>(std::sqrt(2.0)));
   }
   g.projdata_size = g.tof_stride * g.num_tof;
 
@@ -720,12 +726,34 @@ template <typename T> void calculate_row(const Geometry<T>& g, const Bin<T>& bin
   }
 }
 
-/* ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197); erf evaluated exactly instead of
-   STIR's 200000-sample FastErf table (ProjMatrixByBin.cxx:174-176, FastErf.inl:105-108) */
+/* FastErf (numerics/FastErf.inl:21-66) as set up by ProjMatrixByBin::set_up (ProjMatrixByBin.cxx:174-176):
+   200000 samples of erf on [-5,5] (plus two end samples), linear interpolation in double */
+struct FastErf {
+  std::vector<double> v;
+  double max_v = 5, period = 0;
+  FastErf() {
+    const int n = 200000;
+    period = (2 * max_v) / n;
+    v.resize(n + 2);
+    for (int i = 0; i < n + 2; ++i) v[i] = std::erf(i * period - max_v);
+  }
+  double operator()(double xp) const {
+    xp = std::max(std::min(max_v, xp), -max_v);
+    const double xi = (xp + max_v) / period;
+    const int lower = static_cast<int>(std::floor(xi));
+    return v[lower] + (xi - lower) * (v[lower + 1] - v[lower]);
+  }
+};
+const FastErf& fast_erf() {
+  static const FastErf f;
+  return f;
+}
+
+/* ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197) */
 template <typename T> T tof_value(const Geometry<T>& g, T d1, T d2) {
   const T d1n = d1 * g.r_sqrt2_gauss_sigma, d2n = d2 * g.r_sqrt2_gauss_sigma;
   if ((d1n >= T(4.f) && d2n >= T(4.f)) || (d1n <= T(-4.f) && d2n <= T(-4.f))) return T(0);
-  return static_cast<T>(0.5 * (std::erf(static_cast<double>(d2n)) - std::erf(static_cast<double>(d1n))));
+  return static_cast<T>(0.5 * (fast_erf()(static_cast<double>(d2n)) - fast_erf()(static_cast<double>(d1n))));
 }
 
 /* ---------------------------------------------------------------------------
@@ -770,30 +798,49 @@ template <typename T> struct Handle : HandleBase {
     });
     return cache[k];
   }
-  /* ProjMatrixByBin::apply_tof_kernel (ProjMatrixByBin.inl:115-185) */
+  /* ProjMatrixByBin::apply_tof_kernel (ProjMatrixByBin.inl:115-185) with the LOR end points of
+     ProjDataInfoCylindrical::get_LOR (ProjDataInfoCylindrical.cxx:515-548) converted by
+     LORInAxialAndNoArcCorrSinogramCoordinates / LORInCylinderCoordinates / LORAs2Points (LORCoordinates.inl:106-140,288-299) */
   void apply_tof_kernel(const Bin<T>& b, Row<T>& r) {
-    /* LOR end points on the scanner cylinder (get_LOR + LORAs2Points), in scanner coordinates */
-    const T phi = g.get_phi(b.view);
+    const T R = g.ring_radius;
     const T s = g.get_s(b.tang);
     const T m = g.get_m(b.seg, b.ax);
     const T tantheta = g.get_tantheta(b.seg, b.tang);
-    const T R = g.ring_radius;
-    const T half_chord = std::sqrt(square(R) - square(s));
-    /* point1/point2 of LORInAxialAndNoArcCorrSinogramCoordinates -> LORAs2Points */
-    const T cphi = std::cos(phi), sphi = std::sin(phi);
-    C3<T> p1{m + tantheta * half_chord, s * sphi - half_chord * cphi, s * cphi + half_chord * sphi};
-    C3<T> p2{m - tantheta * half_chord, s * sphi + half_chord * cphi, s * cphi - half_chord * sphi};
+    T phi = g.get_phi(b.view);
+    const T max_a = std::sqrt(square(R) - square(s));
+    const T min_a = -max_a;
+    T z1 = m - max_a * tantheta, z2 = m - min_a * tantheta;
+    T beta = std::asin(s / R);
+    const T two_pi = static_cast<T>(2 * kPI);
+    phi = modulo(phi, two_pi);
+    bool swapped = false;
+    if (phi >= kPI) {
+      phi -= static_cast<T>(kPI);
+      beta = -beta;
+      std::swap(z1, z2);
+      swapped = true;
+    }
+    T psi1 = modulo(phi + beta, two_pi);
+    T psi2 = modulo(phi - beta + static_cast<T>(kPI), two_pi);
+    T pz1 = z1, pz2 = z2;
+    if (swapped) {
+      std::swap(psi1, psi2);
+      std::swap(pz1, pz2);
+    }
+    const C3<T> p1{pz1, -R * std::cos(psi1), R * std::sin(psi1)};
+    const C3<T> p2{pz2, -R * std::cos(psi2), R * std::sin(psi2)};
     const T scanner_z_offset = static_cast<T>(g.d.num_rings - 1) / T(2.0f) * g.ring_spacing;
     const C3<T> mid{(p1.z + p2.z) * T(0.5f), (p1.y + p2.y) * T(0.5f), (p1.x + p2.x) * T(0.5f)};
-    C3<T> diff{p2.z - mid.z, p2.y - mid.y, p2.x - mid.x};
+    const C3<T> diff{p2.z - mid.z, p2.y - mid.y, p2.x - mid.x};
     const T n = static_cast<T>(norm3(diff.z, diff.y, diff.x));
     const C3<T> u{diff.z / n, diff.y / n, diff.x / n};
     const int ti = b.tof - g.min_tof;
     Row<T> out;
     for (const auto& e : r) {
-      const T pz = static_cast<T>(e.z) * g.vox.z + g.origin.z - scanner_z_offset;
-      const T py = static_cast<T>(e.y) * g.vox.y + g.origin.y;
-      const T px = static_cast<T>(e.x) * g.vox.x + g.origin.x;
+      /* get_physical_coordinates_for_indices: spacing*index + origin, then minus the scanner offset in z */
+      const T pz = (static_cast<T>(e.z) * g.vox.z + g.origin.z) - scanner_z_offset;
+      const T py = (static_cast<T>(e.y) * g.vox.y + g.origin.y) - T(0.0f);
+      const T px = (static_cast<T>(e.x) * g.vox.x + g.origin.x) - T(0.0f);
       T ip = T(0);
       ip = ip + (pz - mid.z) * u.z;
       ip = ip + (py - mid.y) * u.y;

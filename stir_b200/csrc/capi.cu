@@ -136,7 +136,6 @@ void setup_projector(b200rt_projector& h) {
   Geometry& g = *h.geo;
   DeviceGuard dg(h.device);
   ck(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-  if (g.num_tof() > 1) throw std::runtime_error("TOF projection data is not supported by this build of the projector");
 
   const std::vector<int> bviews = g.basic_views();
   const std::vector<int> bsegs = g.basic_segments();
@@ -274,22 +273,115 @@ void setup_projector(b200rt_projector& h) {
   ck(cudaStreamSynchronize(h.stream), "rows");
   batch_rows.clear();
 
-  pos = 0;
-  for (int b = 0; b < nb; ++b) {
-    const BasicBin& bb = bbs[b];
-    const auto lg = group_lines(bb.view, bb.seg, bb.tang == 0);
-    ProjBinDev pb{};
-    pb.row_offset = pos;
-    pb.row_len = static_cast<int32_t>(row_len[b]);
-    pb.tang = static_cast<int16_t>(bb.tang);
-    pb.tof = static_cast<int16_t>(bb.tof);
-    pb.first_line = lg.first;
-    pb.num_lines = lg.second;
-    h.h_bins[b] = pb;
-    h.h_bin_view[b] = bb.view;
-    h.h_bin_seg[b] = bb.seg;
-    h.bin_index[h.bin_key(bb.view, bb.seg, bb.tang, bb.tof)] = b;
-    pos += row_len[b];
+  if (g.num_tof() == 1) {
+    pos = 0;
+    for (int b = 0; b < nb; ++b) {
+      const BasicBin& bb = bbs[b];
+      const auto lg = group_lines(bb.view, bb.seg, bb.tang == 0);
+      ProjBinDev pb{};
+      pb.row_offset = pos;
+      pb.row_len = static_cast<int32_t>(row_len[b]);
+      pb.tang = static_cast<int16_t>(bb.tang);
+      pb.tof = static_cast<int16_t>(bb.tof);
+      pb.first_line = lg.first;
+      pb.num_lines = lg.second;
+      h.h_bins[b] = pb;
+      h.h_bin_view[b] = bb.view;
+      h.h_bin_seg[b] = bb.seg;
+      h.bin_index[h.bin_key(bb.view, bb.seg, bb.tang, bb.tof)] = b;
+      pos += row_len[b];
+    }
+  } else {
+    // TOF: every basic row weighted by the kernel of each timing bin (ProjMatrixByBin.inl:66-72,115-185)
+    const int nt = g.num_tof();
+    std::vector<TofJobDev> jobs(static_cast<size_t>(nb) * nt);
+    int64_t src = 0;
+    for (int b = 0; b < nb; ++b) {
+      float mid[3], unit[3];
+      g.lor_middle_and_direction(bbs[b].seg, bbs[b].view, bbs[b].tang, mid, unit);
+      for (int k = 0; k < nt; ++k) {
+        TofJobDev& j = jobs[static_cast<size_t>(b) * nt + k];
+        j.src_offset = src;
+        j.src_len = static_cast<int>(row_len[b]);
+        j.tof_index = k;
+        for (int c = 0; c < 3; ++c) {
+          j.mid[c] = mid[c];
+          j.unit[c] = unit[c];
+        }
+      }
+      src += row_len[b];
+    }
+    // FastErf table (numerics/FastErf.inl:21-36) with ProjMatrixByBin's 200000 samples on [-5,5]
+    const int ns = 200000;
+    const double emax = 5.0, period = (2 * emax) / ns;
+    std::vector<double> table(ns + 2);
+    for (int i = 0; i < ns + 2; ++i) table[i] = std::erf(i * period - emax);
+    std::vector<float> low(nt), high(nt);
+    for (int k = 0; k < nt; ++k) {
+      low[k] = g.tof_low(g.min_tof() + k);
+      high[k] = g.tof_high(g.min_tof() + k);
+    }
+    DevBuf<double> d_table;
+    DevBuf<float> d_low, d_high;
+    DevBuf<TofJobDev> d_jobs;
+    d_table.upload(table, h.stream);
+    d_low.upload(low, h.stream);
+    d_high.upload(high, h.stream);
+    d_jobs.upload(jobs, h.stream);
+    TofParams tp{};
+    tp.vox[0] = g.desc().voxel_size_z;
+    tp.vox[1] = g.desc().voxel_size_y;
+    tp.vox[2] = g.desc().voxel_size_x;
+    tp.origin[0] = g.desc().origin_z;
+    tp.origin[1] = g.desc().origin_y;
+    tp.origin[2] = g.desc().origin_x;
+    tp.scanner_z_offset = g.scanner_z_offset();
+    tp.r_sqrt2_sigma = g.r_sqrt2_gauss_sigma();
+    tp.low = d_low.p;
+    tp.high = d_high.p;
+    tp.erf_table = d_table.p;
+    tp.erf_n = ns + 2;
+    tp.erf_max = emax;
+    tp.erf_period = period;
+    const int njobs = static_cast<int>(jobs.size());
+    DevBuf<int> d_cnt;
+    d_cnt.alloc(njobs);
+    ck(launch_tof_rows(h.rows.p, d_jobs.p, njobs, tp, nullptr, nullptr, d_cnt.p, h.stream), "TOF rows");
+    std::vector<int> cnt(njobs);
+    ck(cudaMemcpyAsync(cnt.data(), d_cnt.p, njobs * sizeof(int), cudaMemcpyDeviceToHost, h.stream), "counts");
+    ck(cudaStreamSynchronize(h.stream), "TOF rows");
+    std::vector<int64_t> off(njobs + 1, 0);
+    for (int j = 0; j < njobs; ++j) off[j + 1] = off[j] + cnt[j];
+    DevBuf<int64_t> d_off2;
+    d_off2.upload(off, h.stream);
+    DevBuf<RowElem> tof_rows;
+    tof_rows.alloc(std::max<int64_t>(off[njobs], 1));
+    ck(launch_tof_rows(h.rows.p, d_jobs.p, njobs, tp, d_off2.p, tof_rows.p, d_cnt.p, h.stream), "TOF rows");
+    ck(cudaStreamSynchronize(h.stream), "TOF rows");
+    std::swap(h.rows.p, tof_rows.p);
+    std::swap(h.rows.n, tof_rows.n);
+    total = off[njobs];
+    h.h_bins.resize(njobs);
+    h.h_bin_view.resize(njobs);
+    h.h_bin_seg.resize(njobs);
+    for (int b = 0; b < nb; ++b) {
+      const BasicBin& bb = bbs[b];
+      const auto lg = group_lines(bb.view, bb.seg, bb.tang == 0);
+      for (int k = 0; k < nt; ++k) {
+        const int j = b * nt + k;
+        ProjBinDev pb{};
+        pb.row_offset = off[j];
+        pb.row_len = cnt[j];
+        pb.tang = static_cast<int16_t>(bb.tang);
+        pb.tof = static_cast<int16_t>(g.min_tof() + k);
+        pb.first_line = lg.first;
+        pb.num_lines = lg.second;
+        h.h_bins[j] = pb;
+        h.h_bin_view[j] = bb.view;
+        h.h_bin_seg[j] = bb.seg;
+        h.bin_index[h.bin_key(bb.view, bb.seg, bb.tang, g.min_tof() + k)] = j;
+      }
+    }
   }
   h.bins.upload(h.h_bins, h.stream);
   h.lines.upload(lines, h.stream);
@@ -333,7 +425,7 @@ void setup_projector(b200rt_projector& h) {
     int64_t t = 0;
     std::vector<RowElem> hr(static_cast<size_t>(total));
     if (total > 0) ck(cudaMemcpy(hr.data(), h.rows.p, total * sizeof(RowElem), cudaMemcpyDeviceToHost), "rows");
-    for (int b = 0; b < nb; ++b) {
+    for (size_t b = 0; b < h.h_bins.size(); ++b) {
       const ProjBinDev& pb = h.h_bins[b];
       for (int l = 0; l < pb.num_lines; ++l) {
         const LineDev& L = lines[pb.first_line + l];
@@ -758,7 +850,7 @@ int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, c
     }
     if (!update_dev) h->upd.alloc(ni);
     float* u = update_dev ? update_dev : h->upd.p;
-    h->small_value.alloc(static_cast<size_t>(2 * g.S() + 1) * g.num_views());
+    h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
     h->cancelled.alloc(1);
     h->partial_max.alloc(update_num_blocks(ni));
     h->umax.alloc(1);
@@ -771,7 +863,7 @@ int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, c
     const int* list = subset_list(*h, subset_num, num_subsets, n);
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
-                                    h->small_value.p, st),
+                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
        "viewgram thresholds");
     ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
     FwdEpilogue ep{};
@@ -818,11 +910,11 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     int n = 0, nv = 0;
     const int* list = subset_list(*h, subset_num, num_subsets, n);
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
-    h->small_value.alloc(static_cast<size_t>(2 * g.S() + 1) * g.num_views());
+    h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
     h->ll_partials.alloc(std::max(n, 1));
     h->ll_sum.alloc(1);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
-                                    h->small_value.p, st),
+                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
        "viewgram thresholds");
     FwdEpilogue ep{};
     ep.mode = kEpiLoglik;
@@ -929,7 +1021,7 @@ extern "C" int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const floa
     for (int v = 0; v < g.num_views(); ++v)
       if (in[v]) views.push_back(v);
     if (bins.size() > static_cast<size_t>(kNoAllocMaxBins) || views.size() > static_cast<size_t>(kNoAllocMaxViews) ||
-        static_cast<int64_t>(2 * g.S() + 1) * g.num_views() > kNoAllocMaxViewgrams)
+        static_cast<int64_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views() > kNoAllocMaxViewgrams)
       return fail(h, B200RT_ERR_TOO_LARGE,
                   "b200rt_log_likelihood_dev_noalloc: more than 131072 basic bins, 4096 views or 65536 viewgrams");
     if (bins.empty()) {
@@ -945,7 +1037,8 @@ extern "C" int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const floa
     ck(cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
     // every threshold and partial the kernels read is written by this call first; nothing stale is used
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), d_views,
-                                    static_cast<int>(views.size()), zero_seg0_end_planes, d_small, st),
+                                    static_cast<int>(views.size()), zero_seg0_end_planes, g.num_tof(), g.tof_stride(),
+                                    d_small, st),
        "viewgram thresholds");
     FwdEpilogue ep{};
     ep.mode = kEpiLoglik;

@@ -473,13 +473,8 @@ void Geometry::lor_middle_and_direction(int seg, int view, int tang, float mid[3
   float z1 = m - max_a * tantheta;
   float z2 = m - min_a * tantheta;
   float beta = std::asin(s / R);
-  auto to_0_2pi = [](float a) {
-    const float tp = static_cast<float>(2 * kPi);
-    float r = static_cast<float>(std::fmod(static_cast<double>(a), static_cast<double>(tp)));
-    if (r < 0) r += tp;
-    return r;
-  };
-  phi = to_0_2pi(phi);
+  const float two_pi = static_cast<float>(2 * kPi);
+  phi = modulo_f(phi, two_pi);  // to_0_2pi (modulo.h:136-140)
   bool swapped = false;
   if (phi >= kPi) {
     phi -= static_cast<float>(kPi);
@@ -487,8 +482,8 @@ void Geometry::lor_middle_and_direction(int seg, int view, int tang, float mid[3
     std::swap(z1, z2);
     swapped = true;
   }
-  float psi1 = to_0_2pi(phi + beta);
-  float psi2 = to_0_2pi(phi - beta + static_cast<float>(kPi));
+  float psi1 = modulo_f(phi + beta, two_pi);
+  float psi2 = modulo_f(phi - beta + static_cast<float>(kPi), two_pi);
   float pz1 = z1, pz2 = z2;
   if (swapped) {
     std::swap(psi1, psi2);

@@ -95,7 +95,7 @@ struct FwdEpilogue {
   const float* y;              // measured data (device layout)
   const float* add;            // additive term or nullptr
   const float* mult;           // multiplicative term or nullptr (log-likelihood only)
-  const float* small_value;    // per (segment+S)*num_views+view: max(viewgram y)*SMALL_NUM, >= 0
+  const float* small_value;    // per ((tof-min)*(2S+1)+segment+S)*num_views+view: max(viewgram y)*SMALL_NUM, >= 0
   unsigned int* cancelled;     // number of ratios clipped at 1e4
   double* partials;            // one log-likelihood partial sum per CTA
 };
@@ -123,8 +123,10 @@ cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* s
 cudaError_t launch_max(const float* data, int64_t n, float* partial, float* out, cudaStream_t st);
 
 // OSMAPOSL pieces (osem.cu)
+// out index: ((tof bin - min) * (2S+1) + segment + S) * num_views + view
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
-                                         const int* views, int nviews, int zero_ends, float* out, cudaStream_t st);
+                                         const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
+                                         float* out, cudaStream_t st);
 int update_num_blocks(int64_t n);
 cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
                           const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
@@ -141,6 +143,27 @@ struct RowKV {
 };
 cudaError_t launch_build_rows(const RayDev* rays, const BuildBinDev* bins, int nbins, const float voxel_zyx[3],
                               RowKV* scratch, int* counts, cudaStream_t st);
+// TOF rows: the non-TOF row of a basic bin weighted by the TOF kernel of one timing bin
+// (ProjMatrixByBin::apply_tof_kernel, ProjMatrixByBin.inl:115-185)
+struct TofJobDev {
+  int64_t src_offset;  // non-TOF row
+  int src_len;
+  int tof_index;       // timing bin - min
+  float mid[3], unit[3];  // LOR middle and direction (scanner coordinates), z,y,x
+};
+struct TofParams {
+  float vox[3], origin[3];  // z,y,x
+  float scanner_z_offset;
+  float r_sqrt2_sigma;
+  const float* low;         // per timing bin
+  const float* high;
+  const double* erf_table;  // FastErf samples
+  int erf_n;
+  double erf_max, erf_period;
+};
+cudaError_t launch_tof_rows(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp,
+                            const int64_t* out_offsets, RowElem* out, int* counts, cudaStream_t st);
+
 cudaError_t launch_compact_rows(const BuildBinDev* bins, int nbins, const RowKV* scratch, const int64_t* out_offsets,
                                 RowElem* rows, cudaStream_t st);
 

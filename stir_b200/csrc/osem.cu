@@ -22,11 +22,13 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // one block per (segment, view) of the subset: max over the viewgram of y with segment 0 end planes zeroed
 __global__ void viewgram_small_value_kernel(const float* __restrict__ y, const SegDev* __restrict__ segs, int S, int num_views,
-                                            int num_tang, const int* __restrict__ views, int zero_ends, float* __restrict__ out) {
+                                            int num_tang, const int* __restrict__ views, int zero_ends, int64_t tof_stride,
+                                            float* __restrict__ out) {
   const int seg = static_cast<int>(blockIdx.y) - S;
   const int view = views[blockIdx.x];
+  const int tofi = blockIdx.z;
   const SegDev sd = segs[seg + S];
-  const int64_t base = sd.dev_offset + static_cast<int64_t>(view) * num_tang * sd.nax;
+  const int64_t base = tofi * tof_stride + sd.dev_offset + static_cast<int64_t>(view) * num_tang * sd.nax;
   const int n = num_tang * sd.nax;
   float m = -INFINITY;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -42,7 +44,7 @@ __global__ void viewgram_small_value_kernel(const float* __restrict__ y, const S
   if (threadIdx.x < 32) {
     m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
     m = warp_max(m);
-    if (threadIdx.x == 0) out[(seg + S) * num_views + view] = fmaxf(m * 0.000001F, 0.F);  // SMALL_NUM
+    if (threadIdx.x == 0) out[(tofi * (2 * S + 1) + seg + S) * num_views + view] = fmaxf(m * 0.000001F, 0.F);  // SMALL_NUM
   }
 }
 
@@ -249,9 +251,11 @@ cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* s
 }
 
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
-                                         const int* views, int nviews, int zero_ends, float* out, cudaStream_t st) {
+                                         const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
+                                         float* out, cudaStream_t st) {
   if (nviews <= 0) return cudaSuccess;
-  viewgram_small_value_kernel<<<dim3(nviews, 2 * S + 1), 256, 0, st>>>(y, segs, S, num_views, num_tang, views, zero_ends, out);
+  viewgram_small_value_kernel<<<dim3(nviews, 2 * S + 1, num_tof), 256, 0, st>>>(y, segs, S, num_views, num_tang, views,
+                                                                                  zero_ends, tof_stride, out);
   return cudaGetLastError();
 }
 

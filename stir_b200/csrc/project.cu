@@ -29,6 +29,7 @@ constexpr int kAxPerLane = 4;  // axial positions per lane per pass: 128 per war
 struct LineSetup {
   int64_t out_base;  // device-layout index of (line, axial 0)
   int nax, npa;
+  int tofi;          // timing bin - min
 };
 
 __device__ __forceinline__ bool setup_line(const ProjParams& p, const ProjBinDev& pb, const LineDev& L, LineSetup& s) {
@@ -37,6 +38,7 @@ __device__ __forceinline__ bool setup_line(const ProjParams& p, const ProjBinDev
   const SegDev sd = p.segs[L.seg + p.S];
   s.nax = sd.nax;
   s.npa = sd.npa;
+  s.tofi = pb.tof - p.min_tof;
   s.out_base = static_cast<int64_t>(pb.tof - p.min_tof) * p.tof_stride + sd.dev_offset +
                (static_cast<int64_t>(L.view) * p.num_tang + (tang - p.min_tang)) * sd.nax;
   return true;
@@ -133,7 +135,7 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
         const bool zend = ep.zero_ends && L.seg == 0 && (a == 0 || a == s.nax - 1);
         const float y = zend ? 0.f : __ldg(ep.y + idx);
         const float av = (ep.add && !zend) ? __ldg(ep.add + idx) : 0.f;
-        const float sv = ep.small_value[(L.seg + p.S) * p.num_views + L.view];
+        const float sv = ep.small_value[(s.tofi * (2 * p.S + 1) + L.seg + p.S) * p.num_views + L.view];
         if (EPI == kEpiRatio) {
           // divide_and_truncate (recon_array_functions.cxx:171-266) of y by A x + a
           const float den = acc[j] + av;

@@ -288,7 +288,65 @@ __global__ void compact_rows_kernel(const BuildBinDev* bins, int nbins, const Ro
   }
 }
 
+// FastErf::get_erf_linear_interpolation (numerics/FastErf.inl:46-66)
+__device__ __forceinline__ double fast_erf(const TofParams& tp, double xp) {
+  xp = fmax(fmin(tp.erf_max, xp), -tp.erf_max);
+  const double xi = (xp + tp.erf_max) / tp.erf_period;
+  const int lower = static_cast<int>(floor(xi));
+  return tp.erf_table[lower] + (xi - lower) * (tp.erf_table[lower + 1] - tp.erf_table[lower]);
+}
+
+// ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197)
+__device__ __forceinline__ float tof_value(const TofParams& tp, float d1, float d2) {
+  const float d1n = d1 * tp.r_sqrt2_sigma, d2n = d2 * tp.r_sqrt2_sigma;
+  if ((d1n >= 4.f && d2n >= 4.f) || (d1n <= -4.f && d2n <= -4.f)) return 0.f;
+  return static_cast<float>(0.5 * (fast_erf(tp, static_cast<double>(d2n)) - fast_erf(tp, static_cast<double>(d1n))));
+}
+
+// one thread per (basic bin, timing bin): out == nullptr counts, otherwise fills at out_offsets[job]
+__global__ void tof_rows_kernel(const RowElem* __restrict__ src, const TofJobDev* __restrict__ jobs, int njobs, TofParams tp,
+                                const int64_t* __restrict__ out_offsets, RowElem* __restrict__ out, int* __restrict__ counts) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const TofJobDev job = jobs[j];
+  const float low = tp.low[job.tof_index], high = tp.high[job.tof_index];
+  int n = 0;
+  int64_t o = out ? out_offsets[j] : 0;
+  for (int k = 0; k < job.src_len; ++k) {
+    const RowElem e = src[job.src_offset + k];
+    int z, y, x;
+    unpack_zyx(e.zyx, z, y, x);
+    // get_physical_coordinates_for_indices, minus the scanner centre in z
+    const float pz = (static_cast<float>(z) * tp.vox[0] + tp.origin[0]) - tp.scanner_z_offset;
+    const float py = (static_cast<float>(y) * tp.vox[1] + tp.origin[1]) - 0.0f;
+    const float px = (static_cast<float>(x) * tp.vox[2] + tp.origin[2]) - 0.0f;
+    float ip = 0.f;
+    ip = ip + (pz - job.mid[0]) * job.unit[0];
+    ip = ip + (py - job.mid[1]) * job.unit[1];
+    ip = ip + (px - job.mid[2]) * job.unit[2];
+    const float d2 = -ip;
+    const float kv = tof_value(tp, low - d2, high - d2);
+    if (kv > 0 && e.v != 0) {
+      if (out) {
+        RowElem r;
+        r.zyx = e.zyx;
+        r.v = e.v * kv;
+        out[o + n] = r;
+      }
+      ++n;
+    }
+  }
+  if (!out) counts[j] = n;
+}
+
 }  // namespace
+
+cudaError_t launch_tof_rows(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp,
+                            const int64_t* out_offsets, RowElem* out, int* counts, cudaStream_t st) {
+  if (njobs <= 0) return cudaSuccess;
+  tof_rows_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(src, jobs, njobs, tp, out_offsets, out, counts);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_build_rows(const RayDev* rays, const BuildBinDev* bins, int nbins, const float voxel_zyx[3],
                               RowKV* scratch, int* counts, cudaStream_t st) {

@@ -254,13 +254,19 @@ def clinical_3d_pet_half():
     return pdi, img
 
 
-def tof_small_3d_pet(num_tof_bins: int = 33, fwhm_ps: float = 550.0):
-    """small_3d_pet with TOF: `num_tof_bins` bins, Gaussian kernel of `fwhm_ps` FWHM."""
+def tof_small_3d_pet(num_tof_bins: int = 33, fwhm_ps: float = 550.0, timing_bin_ps: float = 50.0, num_views: int = 144):
+    """small_3d_pet with TOF: `num_tof_bins` timing bins of `timing_bin_ps` (33 x 50 ps cover the 248 mm FOV)
+    and a Gaussian kernel of `fwhm_ps` FWHM."""
     pdi, img = small_3d_pet()
-    sc = dataclasses.replace(pdi.scanner, timing_resolution=fwhm_ps, size_of_timing_pos=4000.0 / num_tof_bins * 1.0,
+    sc = dataclasses.replace(pdi.scanner, timing_resolution=fwhm_ps, size_of_timing_pos=timing_bin_ps,
                              max_num_timing_poss=num_tof_bins)
-    pdi = dataclasses.replace(pdi, scanner=sc, tof_mash_factor=1)
+    pdi = dataclasses.replace(pdi, scanner=sc, tof_mash_factor=1, num_views=num_views)
     return pdi, img
+
+
+def non_tof(pdi: ProjDataInfo) -> ProjDataInfo:
+    """ProjDataInfo::create_non_tof_clone: the same projection data without timing bins."""
+    return dataclasses.replace(pdi, tof_mash_factor=0)
 
 
 def rpt_sensitivity_test():

@@ -212,6 +212,22 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
                               const float* mult_dev, int subset_num, int num_subsets, int zero_seg0_end_planes, double* out,
                               void* stream);
 
+/* Gradient of the subset log-likelihood:
+ *   A_S^T [ divide_and_truncate(y, A_S x + a) - m ],  m = mult_dev or ones
+ * (compute_sub_gradient_without_penalty, RPC_process_related_viewgrams_gradient<false>,
+ * src/recon_buildblock/PoissonLogLikelihoodWithLinearModelForMeanAndProjData.cxx:1421-1481).  The
+ * projection A x is recomputed here, never stored by the caller.  gradient_dev is overwritten. */
+int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_dev, const float* y_dev,
+                                       const float* additive_dev, const float* mult_dev, int subset_num, int num_subsets,
+                                       int zero_seg0_end_planes, int back_projection_mode, float* gradient_dev,
+                                       void* stream);
+
+/* Prior value (QuadraticPrior::compute_value, src/recon_buildblock/QuadraticPrior.cxx:233-298;
+ * RelativeDifferencePrior::compute_value, src/recon_buildblock/RelativeDifferencePrior.cxx:302-370), FP64 with a
+ * fixed summation order.  Synchronises and writes *out. */
+int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
+                           void* stream);
+
 /* Allocation-free variant of b200rt_log_likelihood_dev.  No counterpart in the reference.
  * For callers that must not allocate device memory once they are set up: for example a
  * reconstruction service that hands all device memory to a caching allocator at start-up, or

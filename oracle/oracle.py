@@ -53,6 +53,7 @@ def _load():
         "or_osmaposl_update_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F, _I,
                                         ctypes.POINTER(_I)]),
         "or_log_likelihood_f32": (_D, [_P, _P, _P, _P, _P, _I, _I, _I, _I]),
+        "or_loglik_gradient_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P]),
         "or_prior_gradient_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_prior_value_f32": (_D, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F]),
         "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
@@ -173,6 +174,18 @@ class Oracle:
         if st != 0:
             raise RuntimeError("oracle OSMAPOSL update failed")
         return x, cancelled.value
+
+    def log_likelihood_gradient(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
+                                nthreads=None):
+        x = np.ascontiguousarray(image, np.float32).ravel()
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+        m = None if mult is None else np.ascontiguousarray(mult, np.float32).ravel()
+        g = np.zeros(self.image_shape, np.float32)
+        if lib().or_loglik_gradient_f32(self.h, _ptr(x), _ptr(y), _ptr(a), _ptr(m), subset, nsub,
+                                        int(zero_seg0_end_planes), nthreads or default_threads(), _ptr(g)) != 0:
+            raise RuntimeError("oracle gradient failed")
+        return g
 
     def log_likelihood(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
                        nthreads=None):

@@ -1377,6 +1377,37 @@ int or_osmaposl_update_f32(or_handle* h, float* x, const float* y, const float* 
   }
 }
 
+/* sub-gradient of the log-likelihood without penalty: A^T [divide_and_truncate(y, A x + a) - m]
+   (RPC_process_related_viewgrams_gradient<false>, ...AndProjData.cxx:1421-1481) */
+int or_loglik_gradient_f32(or_handle* h, const float* x, const float* y, const float* add, const float* mult, int subset,
+                           int nsub, int zero_ends, int nthreads, float* grad) {
+  if (!h->f) return -1;
+  try {
+    auto& H = *h->f;
+    auto& g = H.g;
+    std::vector<float> ratio;
+    subset_ratio(H, x, y, add, subset, nsub, zero_ends, nthreads, ratio, nullptr);
+    const auto vs = basic_vs_in_subset(g, subset, nsub);
+    for (const auto& b : vs)
+      for (int k = g.min_tof; k <= g.max_tof; ++k) {
+        std::vector<std::pair<int, int>> rel;
+        related_vs(g, b.first, b.second, rel);
+        for (const auto& r : rel) {
+          const int seg = r.second, view = r.first;
+          for_viewgram(g, seg, view, k, [&](int a, int, int64_t i) {
+            const bool z_here = zero_ends && seg == 0 && (a == 0 || a == g.nax(0) - 1);
+            ratio[i] -= z_here ? 0.f : (mult ? mult[i] : 1.f);
+          });
+        }
+      }
+    H.back(ratio.data(), grad, subset, nsub, nthreads);
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "oracle: %s\n", e.what());
+    return -1;
+  }
+}
+
 double or_log_likelihood_f32(or_handle* h, const float* x, const float* y, const float* add, const float* mult,
                              int subset, int nsub, int zero_ends, int nthreads) {
   if (!h->f) return std::nan("");

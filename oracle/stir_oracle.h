@@ -67,6 +67,10 @@ int or_osmaposl_update_f32(or_handle* h, float* estimate, const float* y, const 
 double or_log_likelihood_f32(or_handle* h, const float* image, const float* y, const float* additive, const float* mult,
                              int subset, int nsub, int zero_seg0_end_planes, int nthreads);
 
+/* A^T [divide_and_truncate(y, A x + a) - m] over one subset (m = mult or ones) */
+int or_loglik_gradient_f32(or_handle* h, const float* image, const float* y, const float* additive, const float* mult,
+                           int subset, int nsub, int zero_seg0_end_planes, int nthreads, float* gradient);
+
 /* Prior gradient and value (QuadraticPrior.cxx:233-372, RelativeDifferencePrior.cxx:280-452);
    image [z][y][x]; voxel sizes z,y,x. */
 int or_prior_gradient_f32(const b200rt_prior* prior, const float* image, const float* kappa, int nz, int ny, int nx,

@@ -132,6 +132,8 @@ EXPORTS = [
                                               ctypes.c_float, _I, _P, _P]),
     ("b200rt_get_num_cancelled", _I, [_P, ctypes.POINTER(_I64)]),
     ("b200rt_log_likelihood_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(ctypes.c_double), _P]),
+    ("b200rt_log_likelihood_gradient_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P]),
+    ("b200rt_prior_value_dev", _I, [_P, ctypes.POINTER(Prior), _P, ctypes.POINTER(ctypes.c_double), _P]),
     ("b200rt_log_likelihood_dev_noalloc", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
     ("b200rt_prior_gradient_dev", _I, [_P, ctypes.POINTER(Prior), _P, _P, _P]),
     ("b200rt_forward_project", _I, [_P, _P, _P, _I, _I]),

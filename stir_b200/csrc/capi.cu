@@ -958,6 +958,77 @@ int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, co
   }
 }
 
+int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_dev, const float* y_dev,
+                                       const float* additive_dev, const float* mult_dev, int subset_num, int num_subsets,
+                                       int zero_seg0_end_planes, int back_projection_mode, float* gradient_dev,
+                                       void* stream) {
+  if (!h || !image_dev || !y_dev || !gradient_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!h->ratio.p) {
+      h->ratio.alloc(g.projdata_size());
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+    }
+    h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
+    h->cancelled.alloc(1);
+    int n = 0, nv = 0;
+    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    const int* views = subset_views(*h, subset_num, num_subsets, nv);
+    ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
+                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
+       "viewgram thresholds");
+    ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
+    FwdEpilogue ep{};
+    ep.mode = kEpiGradient;
+    ep.zero_ends = zero_seg0_end_planes;
+    ep.y = y_dev;
+    ep.add = additive_dev;
+    ep.mult = mult_dev;
+    ep.small_value = h->small_value.p;
+    ep.cancelled = h->cancelled.p;
+    ck(launch_forward(h->params, list, n, image_dev, h->ratio.p, st, &ep), "forward projection");
+    back_project_into(*h, h->ratio.p, gradient_dev, subset_num, num_subsets, back_projection_mode, 0, st);
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
+                           void* stream) {
+  if (!h || !prior || !image_dev || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (prior->type < B200RT_PRIOR_NONE || prior->type > B200RT_PRIOR_RELATIVE_DIFFERENCE)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown prior type");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0) {
+      *out = 0.0;
+      return B200RT_OK;
+    }
+    float w[27];
+    prior_weights(g, prior->only_2D, w);
+    const int np = update_num_blocks(g.image_size());
+    h->ll_partials.alloc(std::max<size_t>(h->ll_partials.n, static_cast<size_t>(np)));
+    h->ll_sum.alloc(1);
+    ck(launch_prior_value(image_dev, prior, w, g.desc().ny, g.desc().nx, g.desc().nz, h->ll_partials.p, np, h->ll_sum.p, st),
+       "prior value");
+    double v = 0.0;
+    ck(cudaMemcpyAsync(&v, h->ll_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "prior value");
+    *out = v * prior->penalisation_factor;
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -86,9 +86,12 @@ struct ProjParams {
 //   kEpiNone:   store it;
 //   kEpiRatio:  store divide_and_truncate(y, A x + a) (the OSMAPOSL gradient numerator);
 //   kEpiLoglik: accumulate the Poisson log-likelihood of y given (A x + a) m in FP64, per CTA.
+//   kEpiGradient: store divide_and_truncate(y, A x + a) - m (m = mult or 1): back-projected, the gradient of
+//                the log-likelihood (RPC_process_related_viewgrams_gradient<false>, ...AndProjData.cxx:1462-1477).
 constexpr int kEpiNone = 0;
 constexpr int kEpiRatio = 1;
 constexpr int kEpiLoglik = 2;
+constexpr int kEpiGradient = 3;
 struct FwdEpilogue {
   int mode;
   int zero_ends;               // zero the first/last axial position of segment 0
@@ -134,6 +137,9 @@ cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const
 cudaError_t launch_prior_gradient(const float* x, float* g, const b200rt_prior* prior, const float prior_weights[27], int ny,
                                   int nx, int nz, float* partial_max, cudaStream_t st);
 cudaError_t launch_reduce_sum(const double* partial, int n, double* out, cudaStream_t st);
+// prior value (QuadraticPrior::compute_value :233-298, RelativeDifferencePrior::compute_value :302-370), FP64
+cudaError_t launch_prior_value(const float* x, const b200rt_prior* prior, const float prior_weights[27], int ny, int nx,
+                               int nz, double* partial, int npartial, double* out, cudaStream_t st);
 
 // row builder (rows.cu)
 struct RowKV {

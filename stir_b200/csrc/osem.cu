@@ -180,6 +180,55 @@ __global__ void reduce_sum_kernel(const double* __restrict__ partial, int n, dou
   if (threadIdx.x == 0) *out = red[0];
 }
 
+// RelativeDifferencePrior::value (RelativeDifferencePrior.cxx:278-285)
+__device__ __forceinline__ double rdp_value(float x, float y, float gamma, float epsilon) {
+  const double d = static_cast<double>(x - y);
+  return 0.5 * (d * d / (x + y + gamma * fabsf(x - y) + epsilon));
+}
+
+// per-block FP64 partial sums of the prior value over voxels (grid-stride, fixed assignment: deterministic)
+__global__ void prior_value_kernel(const float* __restrict__ x, PriorDev pr, int ny, int nx, int nz,
+                                   double* __restrict__ partial) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  double t = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int zi = static_cast<int>(i % nz);
+    const int64_t c = i / nz;
+    const int xi = static_cast<int>(c % nx), yi = static_cast<int>(c / nx);
+    const float xc = x[i];
+    const int dz0 = max(pr.dzmin, -zi), dz1 = min(pr.dzmax, nz - 1 - zi);
+    const int dy0 = max(-1, -yi), dy1 = min(1, ny - 1 - yi);
+    const int dx0 = max(-1, -xi), dx1 = min(1, nx - 1 - xi);
+    for (int dz = dz0; dz <= dz1; ++dz)
+      for (int dy = dy0; dy <= dy1; ++dy)
+        for (int dx = dx0; dx <= dx1; ++dx) {
+          const int64_t j = i + (static_cast<int64_t>(dy) * nx + dx) * nz + dz;
+          const float xn = x[j];
+          const float w = pr.w[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+          double cur;
+          if (pr.type == 1) {
+            const float d = xc - xn;
+            cur = static_cast<double>(w * (d * d) / 4);  // QuadraticPrior.cxx:283-286 (float expression)
+          } else if (pr.epsilon == 0.0f && xc == 0.0f && xn == 0.0f) {
+            cur = 0.0;
+          } else {
+            cur = w * rdp_value(xc, xn, pr.gamma, pr.epsilon);  // RelativeDifferencePrior.cxx:340-349
+          }
+          if (pr.kappa) cur *= pr.kappa[i] * pr.kappa[j];
+          t += cur;
+        }
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
 // per-block max |x| (data == nullptr stands for ones)
 __global__ void absmax_kernel(const float* __restrict__ data, int64_t n, float* __restrict__ partial) {
   float m = 0.f;
@@ -306,6 +355,24 @@ cudaError_t launch_prior_gradient(const float* x, float* g, const b200rt_prior* 
   for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
   pr.kappa = prior->kappa_dev;
   update_prepare_kernel<<<update_num_blocks(n), 256, 0, st>>>(x, x, g, pr, ny, nx, nz, partial_max);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prior_value(const float* x, const b200rt_prior* prior, const float prior_weights[27], int ny, int nx,
+                               int nz, double* partial, int npartial, double* out, cudaStream_t st) {
+  PriorDev pr{};
+  pr.type = prior->type;
+  pr.beta = prior->penalisation_factor;
+  pr.gamma = prior->gamma;
+  pr.epsilon = prior->epsilon;
+  pr.dzmin = prior->only_2D ? 0 : -1;
+  pr.dzmax = prior->only_2D ? 0 : 1;
+  for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
+  pr.kappa = prior->kappa_dev;
+  prior_value_kernel<<<npartial, 256, 0, st>>>(x, pr, ny, nx, nz, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  reduce_sum_kernel<<<1, 256, 0, st>>>(partial, npartial, out);
   return cudaGetLastError();
 }
 

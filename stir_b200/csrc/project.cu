@@ -136,7 +136,7 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
         const float y = zend ? 0.f : __ldg(ep.y + idx);
         const float av = (ep.add && !zend) ? __ldg(ep.add + idx) : 0.f;
         const float sv = ep.small_value[(s.tofi * (2 * p.S + 1) + L.seg + p.S) * p.num_views + L.view];
-        if (EPI == kEpiRatio) {
+        if (EPI == kEpiRatio || EPI == kEpiGradient) {
           // divide_and_truncate (recon_array_functions.cxx:171-266) of y by A x + a
           const float den = acc[j] + av;
           float r;
@@ -148,6 +148,7 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
           } else {
             r = y / den;
           }
+          if (EPI == kEpiGradient) r -= zend ? 0.f : (ep.mult ? __ldg(ep.mult + idx) : 1.f);
           out[idx] = r;
         } else {
           // accumulate_loglikelihood (recon_array_functions.cxx:335-377) of ybar = (A x + a) * m
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
       }
     }
   }
-  if (EPI == kEpiRatio) {
+  if (EPI == kEpiRatio || EPI == kEpiGradient) {
     // cancelled singularities (distributable.cxx:590-594)
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
@@ -366,6 +367,7 @@ cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, 
   FwdEpilogue none{};
   if (!ep || ep->mode == kEpiNone) return launch_forward_epi<kEpiNone>(p, bin_list, nbins, image, projdata, none, st);
   if (ep->mode == kEpiRatio) return launch_forward_epi<kEpiRatio>(p, bin_list, nbins, image, projdata, *ep, st);
+  if (ep->mode == kEpiGradient) return launch_forward_epi<kEpiGradient>(p, bin_list, nbins, image, projdata, *ep, st);
   return launch_forward_epi<kEpiLoglik>(p, bin_list, nbins, image, projdata, *ep, st);
 }
 

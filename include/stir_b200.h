@@ -201,6 +201,17 @@ int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, c
                                      const float* sens_dev, int subset_num, int num_subsets, int subiteration_num,
                                      int zero_seg0_end_planes, const b200rt_prior* prior, float min_relative_change,
                                      float max_relative_change, int back_projection_mode, float* update_dev, void* stream);
+/* The two halves of b200rt_osmaposl_subiteration_dev, for callers that combine partial numerators
+ * (e.g. several GPUs each projecting part of a subset, then summing u with an all-reduce):
+ *   numerator:    u = A_S^T divide_and_truncate(y, A_S x + a)   (numerator_dev overwritten)
+ *   apply_update: u /= sens (or the MAP-OSL denominator), clamp unless subiteration_num == 1, x *= u. */
+int b200rt_osmaposl_numerator_dev(b200rt_projector* h, const float* estimate_dev, const float* y_dev,
+                                  const float* additive_dev, int subset_num, int num_subsets, int zero_seg0_end_planes,
+                                  int back_projection_mode, float* numerator_dev, void* stream);
+int b200rt_osmaposl_apply_update_dev(b200rt_projector* h, float* estimate_dev, float* numerator_dev, const float* sens_dev,
+                                     int num_subsets, int subiteration_num, const b200rt_prior* prior,
+                                     float min_relative_change, float max_relative_change, void* stream);
+
 /* singularities cancelled by divide_and_truncate in the last sub-iteration (distributable.cxx:590-594); synchronises */
 int b200rt_get_num_cancelled(b200rt_projector* h, int64_t* out);
 

@@ -53,6 +53,8 @@ def _load():
         "or_osmaposl_update_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F, _I,
                                         ctypes.POINTER(_I)]),
         "or_log_likelihood_f32": (_D, [_P, _P, _P, _P, _P, _I, _I, _I, _I]),
+        "or_osmaposl_numerator_f32": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(_I)]),
+        "or_osmaposl_apply_f32": (_I, [_P, _P, _P, _P, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F]),
         "or_loglik_gradient_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P]),
         "or_prior_gradient_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_prior_value_f32": (_D, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F]),
@@ -174,6 +176,28 @@ class Oracle:
         if st != 0:
             raise RuntimeError("oracle OSMAPOSL update failed")
         return x, cancelled.value
+
+    def osmaposl_numerator(self, estimate, y, additive, subset, nsub, zero_seg0_end_planes=False, nthreads=None):
+        x = np.ascontiguousarray(estimate, np.float32).ravel()
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+        u = np.zeros(self.image_shape, np.float32)
+        c = ctypes.c_int(0)
+        if lib().or_osmaposl_numerator_f32(self.h, _ptr(x), _ptr(y), _ptr(a), subset, nsub, int(zero_seg0_end_planes),
+                                           nthreads or default_threads(), _ptr(u), ctypes.byref(c)) != 0:
+            raise RuntimeError("oracle numerator failed")
+        return u
+
+    def osmaposl_apply(self, estimate, u, sens, nsub, subiteration_num, prior=None, kappa=None, min_rel=0.0, max_rel=1e37):
+        x = np.ascontiguousarray(estimate, np.float32).copy().reshape(self.image_shape)
+        uu = np.ascontiguousarray(u, np.float32).copy().reshape(self.image_shape)
+        s = np.ascontiguousarray(sens, np.float32).ravel()
+        k = None if kappa is None else np.ascontiguousarray(kappa, np.float32).ravel()
+        p = prior if prior is not None else _abi.Prior(type=_abi.PRIOR_NONE)
+        if lib().or_osmaposl_apply_f32(self.h, _ptr(x), _ptr(uu), _ptr(s), nsub, subiteration_num, ctypes.byref(p), _ptr(k),
+                                       float(min_rel), float(max_rel)) != 0:
+            raise RuntimeError("oracle update failed")
+        return x
 
     def log_likelihood_gradient(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
                                 nthreads=None):

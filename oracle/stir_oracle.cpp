@@ -1313,68 +1313,81 @@ static void subset_ratio(Handle<float>& H, const float* x, const float* y, const
   if (cancelled) *cancelled = count;
 }
 
-int or_osmaposl_update_f32(or_handle* h, float* x, const float* y, const float* add, const float* sens, int subset,
-                           int nsub, int subiter, int zero_ends, const b200rt_prior* prior, const float* kappa,
-                           float min_rel, float max_rel, int nthreads, int* num_cancelled) {
+/* u = A_S^T divide_and_truncate(y, A_S x + a): compute_sub_gradient_without_penalty_plus_sensitivity */
+int or_osmaposl_numerator_f32(or_handle* h, const float* x, const float* y, const float* add, int subset, int nsub,
+                              int zero_ends, int nthreads, float* u, int* num_cancelled) {
   if (!h->f) return -1;
   try {
-    auto& H = *h->f;
-    auto& g = H.g;
-    const int64_t ni = static_cast<int64_t>(g.nz) * g.ny * g.nx;
     std::vector<float> ratio;
-    subset_ratio(H, x, y, add, subset, nsub, zero_ends, nthreads, ratio, num_cancelled);
-    std::vector<float> u(ni, 0.f);
-    H.back(ratio.data(), u.data(), subset, nsub, nthreads);
-    /* OSMAPOSLReconstruction::update_estimate (OSMAPOSLReconstruction.cxx:394-467) */
-    const bool no_prior = !prior || prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0;
-    std::vector<float> den(ni);
-    float small_num;
-    if (no_prior) {
-      std::copy(sens, sens + ni, den.begin());
-      small_num = 0.F;
-    } else {
-      prior_gradient(*prior, x, kappa, g.nz, g.ny, g.nx, g.d.voxel_size_z, g.d.voxel_size_y, g.d.voxel_size_x,
-                     den.data());
-      if (prior->map_model == B200RT_MAP_ADDITIVE) {
-        for (int64_t i = 0; i < ni; ++i) {
-          float dv = den[i] / static_cast<float>(nsub) + sens[i];
-          den[i] = std::max(std::min(dv, sens[i] * 10), sens[i] / 10);
-        }
-      } else {
-        for (int64_t i = 0; i < ni; ++i) {
-          float dv = den[i] + 1;
-          dv = std::max(std::min(dv, 10.F), 1 / 10.F);
-          den[i] = dv * sens[i];
-        }
-      }
-      small_num = 0.000001F;
-    }
-    /* divide (numerics/divide.inl:26-48) */
-    {
-      float small_value = *std::max_element(u.begin(), u.end()) * small_num;
-      small_value = (small_value > 0) ? small_value : 0;
-      for (int64_t i = 0; i < ni; ++i) {
-        if (std::fabs(den[i]) <= small_value && std::fabs(u[i]) <= small_value)
-          u[i] = 0;
-        else
-          u[i] /= den[i];
-      }
-    }
-    /* threshold_upper_lower (:491-507, thresholding.h:45-54) */
-    if (subiter != 1)
-      for (int64_t i = 0; i < ni; ++i) {
-        if (u[i] > max_rel)
-          u[i] = max_rel;
-        else if (min_rel > u[i])
-          u[i] = min_rel;
-      }
-    /* apply_multiplicative_update (:354-369) */
-    for (int64_t i = 0; i < ni; ++i) x[i] *= u[i];
+    subset_ratio(*h->f, x, y, add, subset, nsub, zero_ends, nthreads, ratio, num_cancelled);
+    h->f->back(ratio.data(), u, subset, nsub, nthreads);
     return 0;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "oracle: %s\n", e.what());
     return -1;
   }
+}
+
+/* the rest of OSMAPOSLReconstruction::update_estimate (OSMAPOSLReconstruction.cxx:394-510) given u */
+int or_osmaposl_apply_f32(or_handle* h, float* x, float* u, const float* sens, int nsub, int subiter,
+                          const b200rt_prior* prior, const float* kappa, float min_rel, float max_rel) {
+  if (!h->f) return -1;
+  auto& g = h->f->g;
+  const int64_t ni = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+  const bool no_prior = !prior || prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0;
+  std::vector<float> den(ni);
+  float small_num;
+  if (no_prior) {
+    std::copy(sens, sens + ni, den.begin());
+    small_num = 0.F;
+  } else {
+    prior_gradient(*prior, x, kappa, g.nz, g.ny, g.nx, g.d.voxel_size_z, g.d.voxel_size_y, g.d.voxel_size_x, den.data());
+    if (prior->map_model == B200RT_MAP_ADDITIVE) {
+      for (int64_t i = 0; i < ni; ++i) {
+        float dv = den[i] / static_cast<float>(nsub) + sens[i];
+        den[i] = std::max(std::min(dv, sens[i] * 10), sens[i] / 10);
+      }
+    } else {
+      for (int64_t i = 0; i < ni; ++i) {
+        float dv = den[i] + 1;
+        dv = std::max(std::min(dv, 10.F), 1 / 10.F);
+        den[i] = dv * sens[i];
+      }
+    }
+    small_num = 0.000001F;
+  }
+  /* divide (numerics/divide.inl:26-48) */
+  {
+    float small_value = *std::max_element(u, u + ni) * small_num;
+    small_value = (small_value > 0) ? small_value : 0;
+    for (int64_t i = 0; i < ni; ++i) {
+      if (std::fabs(den[i]) <= small_value && std::fabs(u[i]) <= small_value)
+        u[i] = 0;
+      else
+        u[i] /= den[i];
+    }
+  }
+  /* threshold_upper_lower (:491-507, thresholding.h:45-54) */
+  if (subiter != 1)
+    for (int64_t i = 0; i < ni; ++i) {
+      if (u[i] > max_rel)
+        u[i] = max_rel;
+      else if (min_rel > u[i])
+        u[i] = min_rel;
+    }
+  /* apply_multiplicative_update (:354-369) */
+  for (int64_t i = 0; i < ni; ++i) x[i] *= u[i];
+  return 0;
+}
+
+int or_osmaposl_update_f32(or_handle* h, float* x, const float* y, const float* add, const float* sens, int subset,
+                           int nsub, int subiter, int zero_ends, const b200rt_prior* prior, const float* kappa,
+                           float min_rel, float max_rel, int nthreads, int* num_cancelled) {
+  if (!h->f) return -1;
+  const int64_t ni = static_cast<int64_t>(h->f->g.nz) * h->f->g.ny * h->f->g.nx;
+  std::vector<float> u(ni, 0.f);
+  if (or_osmaposl_numerator_f32(h, x, y, add, subset, nsub, zero_ends, nthreads, u.data(), num_cancelled) != 0) return -1;
+  return or_osmaposl_apply_f32(h, x, u.data(), sens, nsub, subiter, prior, kappa, min_rel, max_rel);
 }
 
 /* sub-gradient of the log-likelihood without penalty: A^T [divide_and_truncate(y, A x + a) - m]

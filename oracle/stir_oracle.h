@@ -62,6 +62,13 @@ int or_osmaposl_update_f32(or_handle* h, float* estimate, const float* y, const 
                            const b200rt_prior* prior, const float* kappa, float min_rel, float max_rel, int nthreads,
                            int* num_cancelled);
 
+/* The two halves of the update: the numerator A_S^T divide_and_truncate(y, A_S x + a), and the
+   division / clamp / multiplication given it (u in/out). */
+int or_osmaposl_numerator_f32(or_handle* h, const float* estimate, const float* y, const float* additive, int subset,
+                              int nsub, int zero_seg0_end_planes, int nthreads, float* u, int* num_cancelled);
+int or_osmaposl_apply_f32(or_handle* h, float* estimate, float* u, const float* sens, int nsub, int subiteration_num,
+                          const b200rt_prior* prior, const float* kappa, float min_rel, float max_rel);
+
 /* Poisson log-likelihood of one subset (accumulate_loglikelihood, recon_array_functions.cxx:335-377,
    RPC at ...AndProjData.cxx:1483-1515), FP64 accumulation.  additive / mult may be NULL. */
 double or_log_likelihood_f32(or_handle* h, const float* image, const float* y, const float* additive, const float* mult,

@@ -130,6 +130,9 @@ EXPORTS = [
     ("b200rt_sensitivity_dev", _I, [_P, _P, _P, _I, _I, _I, _I, _P]),
     ("b200rt_osmaposl_subiteration_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(Prior), ctypes.c_float,
                                               ctypes.c_float, _I, _P, _P]),
+    ("b200rt_osmaposl_numerator_dev", _I, [_P, _P, _P, _P, _I, _I, _I, _I, _P, _P]),
+    ("b200rt_osmaposl_apply_update_dev", _I, [_P, _P, _P, _P, _I, _I, ctypes.POINTER(Prior), ctypes.c_float, ctypes.c_float,
+                                              _P]),
     ("b200rt_get_num_cancelled", _I, [_P, ctypes.POINTER(_I64)]),
     ("b200rt_log_likelihood_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(ctypes.c_double), _P]),
     ("b200rt_log_likelihood_gradient_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P]),

@@ -829,56 +829,115 @@ int b200rt_sensitivity_dev(b200rt_projector* h, const float* mult_dev, float* se
   }
 }
 
+}  // extern "C"
+
+namespace {
+
+// u = A_S^T divide_and_truncate(y, A_S x + a): fused forward projection/ratio, then back projection
+void osmaposl_numerator(b200rt_projector& h, const float* x, const float* y, const float* add, int subset, int nsub,
+                        int zero_ends, int mode, float* u, cudaStream_t st) {
+  const Geometry& g = *h.geo;
+  if (!h.ratio.p) {
+    h.ratio.alloc(g.projdata_size());
+    ck(cudaMemsetAsync(h.ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");  // bins outside the subset
+  }
+  h.small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
+  h.cancelled.alloc(1);
+  int n = 0, nv = 0;
+  const int* list = subset_list(h, subset, nsub, n);
+  const int* views = subset_views(h, subset, nsub, nv);
+  ck(launch_viewgram_small_values(y, h.segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_ends, g.num_tof(),
+                                  g.tof_stride(), h.small_value.p, st),
+     "viewgram thresholds");
+  ck(cudaMemsetAsync(h.cancelled.p, 0, sizeof(unsigned int), st), "memset");
+  FwdEpilogue ep{};
+  ep.mode = kEpiRatio;
+  ep.zero_ends = zero_ends;
+  ep.y = y;
+  ep.add = add;
+  ep.small_value = h.small_value.p;
+  ep.cancelled = h.cancelled.p;
+  ck(launch_forward(h.params, list, n, x, h.ratio.p, st, &ep), "forward projection");
+  back_project_into(h, h.ratio.p, u, subset, nsub, mode, 0, st, 10000.F);
+}
+
+// u /= denominator, clamp, x *= u (OSMAPOSLReconstruction.cxx:394-510)
+void osmaposl_apply(b200rt_projector& h, float* x, float* u, const float* sens, int nsub, int subiter,
+                    const b200rt_prior* prior, float min_rel, float max_rel, cudaStream_t st) {
+  const Geometry& g = *h.geo;
+  const int64_t ni = g.image_size();
+  h.partial_max.alloc(update_num_blocks(ni));
+  h.umax.alloc(1);
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  if (has_prior) {
+    h.grad.alloc(ni);
+    prior_weights(g, prior->only_2D, h.prior_w);
+  }
+  ck(launch_update(u, x, sens, has_prior ? h.grad.p : nullptr, has_prior ? prior : nullptr, h.prior_w, nsub, subiter,
+                   min_rel, max_rel, g.desc().ny, g.desc().nx, g.desc().nz, h.partial_max.p, h.umax.p, st),
+     "update");
+}
+
+int check_mode_prior(b200rt_projector* h, int mode, const b200rt_prior* prior) {
+  if (mode != B200RT_BACKPROJECT_ATOMIC && mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
+  if (prior && (prior->type < B200RT_PRIOR_NONE || prior->type > B200RT_PRIOR_RELATIVE_DIFFERENCE))
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown prior type");
+  return B200RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int b200rt_osmaposl_subiteration_dev(b200rt_projector* h, float* estimate_dev, const float* y_dev, const float* additive_dev,
                                      const float* sens_dev, int subset_num, int num_subsets, int subiteration_num,
                                      int zero_seg0_end_planes, const b200rt_prior* prior, float min_relative_change,
                                      float max_relative_change, int back_projection_mode, float* update_dev, void* stream) {
   if (!h || !estimate_dev || !y_dev || !sens_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
-  if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
-    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
-  if (prior && (prior->type < B200RT_PRIOR_NONE || prior->type > B200RT_PRIOR_RELATIVE_DIFFERENCE))
-    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown prior type");
+  if (int st = check_mode_prior(h, back_projection_mode, prior)) return st;
   try {
     DeviceGuard dg(h->device);
-    const Geometry& g = *h->geo;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int64_t ni = g.image_size();
-    if (!h->ratio.p) {
-      h->ratio.alloc(g.projdata_size());
-      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");  // bins outside the subset
-    }
-    if (!update_dev) h->upd.alloc(ni);
+    if (!update_dev) h->upd.alloc(h->geo->image_size());
     float* u = update_dev ? update_dev : h->upd.p;
-    h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
-    h->cancelled.alloc(1);
-    h->partial_max.alloc(update_num_blocks(ni));
-    h->umax.alloc(1);
-    const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
-    if (has_prior) {
-      h->grad.alloc(ni);
-      prior_weights(g, prior->only_2D, h->prior_w);
-    }
-    int n = 0, nv = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    const int* views = subset_views(*h, subset_num, num_subsets, nv);
-    ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
-                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
-       "viewgram thresholds");
-    ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
-    FwdEpilogue ep{};
-    ep.mode = kEpiRatio;
-    ep.zero_ends = zero_seg0_end_planes;
-    ep.y = y_dev;
-    ep.add = additive_dev;
-    ep.small_value = h->small_value.p;
-    ep.cancelled = h->cancelled.p;
-    ck(launch_forward(h->params, list, n, estimate_dev, h->ratio.p, st, &ep), "forward projection");
-    back_project_into(*h, h->ratio.p, u, subset_num, num_subsets, back_projection_mode, 0, st, 10000.F);
-    ck(launch_update(u, estimate_dev, sens_dev, has_prior ? h->grad.p : nullptr, has_prior ? prior : nullptr, h->prior_w,
-                     num_subsets, subiteration_num, min_relative_change, max_relative_change, g.desc().ny, g.desc().nx,
-                     g.desc().nz, h->partial_max.p, h->umax.p, st),
-       "update");
+    osmaposl_numerator(*h, estimate_dev, y_dev, additive_dev, subset_num, num_subsets, zero_seg0_end_planes,
+                       back_projection_mode, u, st);
+    osmaposl_apply(*h, estimate_dev, u, sens_dev, num_subsets, subiteration_num, prior, min_relative_change,
+                   max_relative_change, st);
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_osmaposl_numerator_dev(b200rt_projector* h, const float* estimate_dev, const float* y_dev,
+                                  const float* additive_dev, int subset_num, int num_subsets, int zero_seg0_end_planes,
+                                  int back_projection_mode, float* numerator_dev, void* stream) {
+  if (!h || !estimate_dev || !y_dev || !numerator_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (int st = check_mode_prior(h, back_projection_mode, nullptr)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    osmaposl_numerator(*h, estimate_dev, y_dev, additive_dev, subset_num, num_subsets, zero_seg0_end_planes,
+                       back_projection_mode, numerator_dev, static_cast<cudaStream_t>(stream));
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_osmaposl_apply_update_dev(b200rt_projector* h, float* estimate_dev, float* numerator_dev, const float* sens_dev,
+                                     int num_subsets, int subiteration_num, const b200rt_prior* prior,
+                                     float min_relative_change, float max_relative_change, void* stream) {
+  if (!h || !estimate_dev || !numerator_dev || !sens_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (num_subsets < 1) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "invalid number of subsets");
+  if (int st = check_mode_prior(h, B200RT_BACKPROJECT_ATOMIC, prior)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    osmaposl_apply(*h, estimate_dev, numerator_dev, sens_dev, num_subsets, subiteration_num, prior, min_relative_change,
+                   max_relative_change, static_cast<cudaStream_t>(stream));
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());

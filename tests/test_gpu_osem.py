@@ -170,3 +170,26 @@ def test_deterministic_osem_is_reproducible(setup):
         sens = s["host_img"](rec_sens.sensitivities[sub])
         xo, _ = s["orc"].osmaposl_update(xo, s["y"], s["add"], sens, sub, 6, it)
     assert rel_l2(s["host_img"](results[0]), xo) <= OSEM_TOL
+
+
+def test_numerator_and_apply_equal_subiteration(setup):
+    """b200rt_osmaposl_numerator_dev + b200rt_osmaposl_apply_update_dev == b200rt_osmaposl_subiteration_dev
+    (the split the multi-GPU driver uses), bit for bit with the deterministic back projection."""
+    import torch
+    from stir_b200.distributed import B200Backend
+    from stir_b200.osmaposl import OSMAPOSLReconstruction
+    s = setup
+    y, add = s["dev_pd"](s["y"]), s["dev_pd"](s["add"])
+    mode = _abi.BACKPROJECT_DETERMINISTIC
+    rec = OSMAPOSLReconstruction(s["proj"], y, additive=add, num_subsets=6, back_projection_mode=mode,
+                                 minimum_relative_change=0.2, maximum_relative_change=5.0).set_up()
+    b = B200Backend(s["proj"], y, add, mode=mode)
+    x1 = s["dev_img"](np.ones(s["img"].shape, np.float32))
+    x2 = x1.clone()
+    for it in (1, 2):
+        rec.subiteration_num = it
+        rec.update_estimate(x1)
+        sub = (it - 1) % 6
+        u = b.numerator(x2, sub, 6)
+        b.apply(x2, u, rec.sensitivities[sub], 6, it, min_rel=0.2, max_rel=5.0)
+        assert torch.equal(x1, x2)

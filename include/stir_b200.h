@@ -270,6 +270,47 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
 int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* image_host,
                         int subset_num, int num_subsets, int mode);
 
+/* ---- batched OSMAPOSL: several reconstructions per launch ---------------
+ * STIR reconstructs the frames of a dynamic study one at a time (one OSMAPOSLReconstruction,
+ * OSMAPOSLReconstruction.cxx:371-516, per frame); there is no batch interface to replace.  A batch
+ * holds any number of reconstructions ("frames"), each with its own projector (image size), data,
+ * sensitivities, subset count and prior.  Batched sub-iteration k advances every frame with
+ * num_subiterations >= k by its own sub-iteration k, subset (start_subset + k - 1) % num_subsets, with
+ * the result of b200rt_osmaposl_subiteration_dev (atomic back projection) up to float rounding.  Per k:
+ * one persistent forward launch (ratio epilogue) and one persistent back projection cover every
+ * frame's subset; the thresholds and the update of each frame run around them.  Projectors passed to
+ * add_frame must outlive the batch and are not used concurrently by the caller while it runs. */
+typedef struct b200rt_batch b200rt_batch;
+
+typedef struct {
+  int ctas_per_sm_forward; /* persistent CTAs per SM; 0 = as many as fit */
+  int ctas_per_sm_back;
+  int order;               /* work order inside a frame: 0 = basic-bin order, 1 = longest rows first */
+} b200rt_batch_config;
+
+int b200rt_batch_create(int device, b200rt_batch** out);
+void b200rt_batch_destroy(b200rt_batch* b);
+const char* b200rt_batch_last_error(const b200rt_batch* b);
+/* sensitivity_devs[num_subsets]: one image per subset (device layout; entries may repeat).
+ * additive_dev and prior may be NULL.  *frame receives the frame's index. */
+int b200rt_batch_add_frame(b200rt_batch* b, b200rt_projector* h, float* estimate_dev, const float* y_dev,
+                           const float* additive_dev, const float* const* sensitivity_devs, int num_subsets,
+                           int start_subset, int num_subiterations, int zero_seg0_end_planes, const b200rt_prior* prior,
+                           float min_relative_change, float max_relative_change, int* frame);
+int b200rt_batch_num_frames(const b200rt_batch* b);
+/* Runs batched sub-iterations first..first+count-1 on `stream`.  use_graph != 0: the sequence is
+ * captured once into a CUDA graph (kept per (first, count) until a frame is added or the
+ * configuration changes) and launched as one graph. */
+int b200rt_batch_run(b200rt_batch* b, int first_subiteration, int count, int use_graph, void* stream);
+/* Times the batched projectors of sub-iteration `subiteration` for each configuration (CTAs per SM,
+ * work order), keeps the fastest and writes it to *out (may be NULL).  Estimates are not changed;
+ * synchronises. */
+int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config* out);
+int b200rt_batch_set_config(b200rt_batch* b, const b200rt_batch_config* config);
+int b200rt_batch_get_config(const b200rt_batch* b, b200rt_batch_config* out);
+/* cancelled singularities of one frame in the last batched sub-iteration it took part in; synchronises */
+int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,16 @@ class Prior(ctypes.Structure):
     ]
 
 
+class BatchConfig(ctypes.Structure):
+    """b200rt_batch_config"""
+
+    _fields_ = [
+        ("ctas_per_sm_forward", ctypes.c_int32),
+        ("ctas_per_sm_back", ctypes.c_int32),
+        ("order", ctypes.c_int32),
+    ]
+
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "libstir_b200.so")
 
@@ -141,6 +151,17 @@ EXPORTS = [
     ("b200rt_prior_gradient_dev", _I, [_P, ctypes.POINTER(Prior), _P, _P, _P]),
     ("b200rt_forward_project", _I, [_P, _P, _P, _I, _I]),
     ("b200rt_back_project", _I, [_P, _P, _P, _I, _I, _I]),
+    ("b200rt_batch_create", _I, [_I, ctypes.POINTER(_P)]),
+    ("b200rt_batch_destroy", None, [_P]),
+    ("b200rt_batch_last_error", ctypes.c_char_p, [_P]),
+    ("b200rt_batch_add_frame", _I, [_P, _P, _P, _P, _P, ctypes.POINTER(_P), _I, _I, _I, _I, ctypes.POINTER(Prior),
+                                    ctypes.c_float, ctypes.c_float, ctypes.POINTER(_I)]),
+    ("b200rt_batch_num_frames", _I, [_P]),
+    ("b200rt_batch_run", _I, [_P, _I, _I, _I, _P]),
+    ("b200rt_batch_autotune", _I, [_P, _I, ctypes.POINTER(BatchConfig)]),
+    ("b200rt_batch_set_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
+    ("b200rt_batch_get_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
+    ("b200rt_batch_get_num_cancelled", _I, [_P, _I, ctypes.POINTER(_I64)]),
 ]
 
 _lib = None
@@ -170,9 +191,9 @@ class B200Error(RuntimeError):
     pass
 
 
-def check(status: int, handle=None, what: str = ""):
+def check(status: int, handle=None, what: str = "", batch=None):
     if status != OK:
         lib = load_library()
-        msg = lib.b200rt_last_error(handle)
+        msg = lib.b200rt_batch_last_error(batch) if batch is not None else lib.b200rt_last_error(handle)
         msg = msg.decode() if msg else ""
         raise B200Error(f"{what} failed with status {status}: {msg}")

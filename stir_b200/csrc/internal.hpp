@@ -103,9 +103,32 @@ struct FwdEpilogue {
   double* partials;            // one log-likelihood partial sum per CTA
 };
 
+// One reconstruction of a batch: its geometry (index into a ProjParams table), estimate, ratio
+// scratch (projection data of its geometry), numerator image and forward epilogue.
+struct BatchFrameDev {
+  int geom;
+  const float* x;
+  float* ratio;
+  float* u;
+  FwdEpilogue ep;
+};
+struct BatchItem {
+  int frame;
+  int bin;
+};
+
 // launchers (project.cu)
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
                            cudaStream_t st, const FwdEpilogue* ep = nullptr);
+// persistent batched projectors: `grid` CTAs take (frame, basic bin) items from *counter (zeroed by the caller)
+cudaError_t launch_forward_batch(const ProjParams* geoms, int npa, size_t smem_bytes, const BatchFrameDev* frames,
+                                 const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st);
+cudaError_t launch_back_batch(const ProjParams* geoms, int npa, size_t smem_bytes, const BatchFrameDev* frames,
+                              const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st);
+// resident CTAs per SM of the batched kernels (0 on error); also sets their shared-memory limit
+int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward);
+// dynamic shared memory of the projection kernels for a row length bound
+size_t proj_smem_bytes(int max_row_len);
 // projdata == nullptr back-projects ones
 cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, float* image,
                                cudaStream_t st, int zero_ends = 0);

@@ -226,20 +226,17 @@ __device__ __forceinline__ void back_pass(const ProjParams& p, const RowElem* sr
   }
 }
 
+// All related lines of one basic bin (one CTA).
 template <int NPA, int EPI>
-__global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                           const float* __restrict__ img, float* __restrict__ out,
-                                                           FwdEpilogue ep) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+__device__ __forceinline__ void forward_bin(const ProjParams& p, const ProjBinDev& pb, unsigned char* smem,
+                                            const float* __restrict__ img, float* __restrict__ out, const FwdEpilogue& ep,
+                                            double& ll, unsigned& ncancel) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   XElem* xbuf = reinterpret_cast<XElem*>(smem) + warp * kChunk;
   RowElem* srow = reinterpret_cast<RowElem*>(smem + sizeof(XElem) * kWarps * kChunk);
   const int n = pb.row_len;
   stage_row(p, pb, srow);
   __syncthreads();
-  double ll = 0.0;
-  unsigned ncancel = 0;
   for (int l = warp; l < pb.num_lines; l += kWarps) {
     const LineDev L = p.lines[pb.first_line + l];
     LineSetup s;
@@ -254,6 +251,18 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
       }
     }
   }
+}
+
+template <int NPA, int EPI>
+__global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                           const float* __restrict__ img, float* __restrict__ out,
+                                                           FwdEpilogue ep) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double ll = 0.0;
+  unsigned ncancel = 0;
+  forward_bin<NPA, EPI>(p, pb, smem, img, out, ep, ll, ncancel);
   if (EPI == kEpiRatio || EPI == kEpiGradient) {
     // cancelled singularities (distributable.cxx:590-594)
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
@@ -274,10 +283,8 @@ __global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const i
 }
 
 template <int NPA, typename Acc>
-__global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                               const float* __restrict__ pd, Acc img, int zero_ends) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+__device__ __forceinline__ void back_bin(const ProjParams& p, const ProjBinDev& pb, unsigned char* smem,
+                                         const float* __restrict__ pd, const Acc& img, int zero_ends) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   XElem* xbuf = reinterpret_cast<XElem*>(smem) + warp * kChunk;
   RowElem* srow = reinterpret_cast<RowElem*>(smem + sizeof(XElem) * kWarps * kChunk);
@@ -297,6 +304,64 @@ __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, con
         default: back_pass<NPA, 4>(p, srow, n, L, s, a0, nact, xbuf, lane, pd, img, zero_ends); break;
       }
     }
+  }
+}
+
+template <int NPA, typename Acc>
+__global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                               const float* __restrict__ pd, Acc img, int zero_ends) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
+  back_bin<NPA, Acc>(p, pb, smem, pd, img, zero_ends);
+}
+
+// ---- batched (several reconstructions in one launch) ------------------------
+// A persistent grid takes work items (frame, basic bin) from a queue in list order: the list is
+// frame-major, so at any time the CTAs work on one or two frames and their images stay in L2.
+__device__ __forceinline__ int next_item(unsigned* counter) {
+  __shared__ int s_item;
+  __syncthreads();  // every thread has finished with the previous item (shared row, s_item)
+  if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+  __syncthreads();
+  return s_item;
+}
+
+template <int NPA>
+__global__ void __launch_bounds__(kThreads) forward_batch_kernel(const ProjParams* __restrict__ geoms,
+                                                                 const BatchFrameDev* __restrict__ frames,
+                                                                 const BatchItem* __restrict__ items, int nitems,
+                                                                 unsigned* counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const int it = next_item(counter);
+    if (it >= nitems) break;
+    const BatchItem wi = items[it];
+    const BatchFrameDev& f = frames[wi.frame];
+    const ProjParams& p = geoms[f.geom];
+    const ProjBinDev pb = p.bins[wi.bin];
+    double ll = 0.0;
+    unsigned ncancel = 0;
+    forward_bin<NPA, kEpiRatio>(p, pb, smem, f.x, f.ratio, f.ep, ll, ncancel);
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && f.ep.cancelled) atomicAdd(f.ep.cancelled, ncancel);
+  }
+}
+
+template <int NPA>
+__global__ void __launch_bounds__(kThreads) back_batch_kernel(const ProjParams* __restrict__ geoms,
+                                                              const BatchFrameDev* __restrict__ frames,
+                                                              const BatchItem* __restrict__ items, int nitems,
+                                                              unsigned* counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  for (;;) {
+    const int it = next_item(counter);
+    if (it >= nitems) break;
+    const BatchItem wi = items[it];
+    const BatchFrameDev& f = frames[wi.frame];
+    const ProjParams& p = geoms[f.geom];
+    const ProjBinDev pb = p.bins[wi.bin];
+    back_bin<NPA, FloatAcc>(p, pb, smem, f.ratio, FloatAcc{f.u}, 0);
   }
 }
 
@@ -331,9 +396,11 @@ cudaError_t transpose(const float* in, float* out, int rows, int64_t cols, cudaS
 
 }  // namespace
 
-static size_t proj_smem_bytes(const ProjParams& p) {
-  return sizeof(XElem) * kWarps * kChunk + sizeof(RowElem) * static_cast<size_t>(p.max_row_len > 0 ? p.max_row_len : 1);
+size_t proj_smem_bytes(int max_row_len) {
+  return sizeof(XElem) * kWarps * kChunk + sizeof(RowElem) * static_cast<size_t>(max_row_len > 0 ? max_row_len : 1);
 }
+
+static size_t proj_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p.max_row_len); }
 
 static cudaError_t prepare_smem(const void* fn, size_t bytes) {
   if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
@@ -390,6 +457,56 @@ cudaError_t launch_back_atomic(const ProjParams& p, const int* bin_list, int nbi
 cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbins, const float* projdata,
                               unsigned long long* acc, const double* scale, cudaStream_t st, int zero_ends) {
   return launch_back_acc(p, bin_list, nbins, projdata, FixedAcc{acc, scale}, st, zero_ends);
+}
+
+cudaError_t launch_forward_batch(const ProjParams* geoms, int npa, size_t smem_bytes, const BatchFrameDev* frames,
+                                 const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  const void* fn = npa == 1 ? reinterpret_cast<const void*>(forward_batch_kernel<1>)
+                 : npa == 2 ? reinterpret_cast<const void*>(forward_batch_kernel<2>)
+                            : reinterpret_cast<const void*>(forward_batch_kernel<0>);
+  cudaError_t e = prepare_smem(fn, smem_bytes);
+  if (e != cudaSuccess) return e;
+  if (npa == 1)
+    forward_batch_kernel<1><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  else if (npa == 2)
+    forward_batch_kernel<2><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  else
+    forward_batch_kernel<0><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_batch(const ProjParams* geoms, int npa, size_t smem_bytes, const BatchFrameDev* frames,
+                              const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  const void* fn = npa == 1 ? reinterpret_cast<const void*>(back_batch_kernel<1>)
+                 : npa == 2 ? reinterpret_cast<const void*>(back_batch_kernel<2>)
+                            : reinterpret_cast<const void*>(back_batch_kernel<0>);
+  cudaError_t e = prepare_smem(fn, smem_bytes);
+  if (e != cudaSuccess) return e;
+  if (npa == 1)
+    back_batch_kernel<1><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  else if (npa == 2)
+    back_batch_kernel<2><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  else
+    back_batch_kernel<0><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward) {
+  const void* fn;
+  if (forward)
+    fn = npa == 1 ? reinterpret_cast<const void*>(forward_batch_kernel<1>)
+       : npa == 2 ? reinterpret_cast<const void*>(forward_batch_kernel<2>)
+                  : reinterpret_cast<const void*>(forward_batch_kernel<0>);
+  else
+    fn = npa == 1 ? reinterpret_cast<const void*>(back_batch_kernel<1>)
+       : npa == 2 ? reinterpret_cast<const void*>(back_batch_kernel<2>)
+                  : reinterpret_cast<const void*>(back_batch_kernel<0>);
+  if (prepare_smem(fn, smem_bytes) != cudaSuccess) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, smem_bytes) != cudaSuccess) return 0;
+  return n;
 }
 
 cudaError_t launch_image_to_dev(const float* stir, float* dev, int nz, int ny, int nx, cudaStream_t st) {

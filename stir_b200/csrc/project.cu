@@ -25,6 +25,10 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kAxPerLane = 4;  // axial positions per lane per pass: 128 per warp
+// resident CTAs per SM the projection kernels are compiled for (registers <= 65536 / (CTAs * kThreads)):
+// on the clinical geometry a sixth CTA per SM gains more than the few registers it spills cost
+constexpr int kMinCtasForward = 6;
+constexpr int kMinCtasBack = 6;
 
 struct LineSetup {
   int64_t out_base;  // device-layout index of (line, axial 0)
@@ -254,7 +258,7 @@ __device__ __forceinline__ void forward_bin(const ProjParams& p, const ProjBinDe
 }
 
 template <int NPA, int EPI>
-__global__ void __launch_bounds__(kThreads) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
+__global__ void __launch_bounds__(kThreads, kMinCtasForward) forward_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                            const float* __restrict__ img, float* __restrict__ out,
                                                            FwdEpilogue ep) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -308,7 +312,7 @@ __device__ __forceinline__ void back_bin(const ProjParams& p, const ProjBinDev& 
 }
 
 template <int NPA, typename Acc>
-__global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
+__global__ void __launch_bounds__(kThreads, kMinCtasBack) back_atomic_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                                const float* __restrict__ pd, Acc img, int zero_ends) {
   extern __shared__ __align__(16) unsigned char smem[];
   const ProjBinDev pb = p.bins[bin_list[blockIdx.x]];
@@ -318,51 +322,67 @@ __global__ void __launch_bounds__(kThreads) back_atomic_kernel(ProjParams p, con
 // ---- batched (several reconstructions in one launch) ------------------------
 // A persistent grid takes work items (frame, basic bin) from a queue in list order: the list is
 // frame-major, so at any time the CTAs work on one or two frames and their images stay in L2.
-__device__ __forceinline__ int next_item(unsigned* counter) {
+// The current item's frame, geometry and basic bin, copied to shared memory by the CTA so that the
+// projection loops read them like kernel parameters instead of holding them in registers.
+struct BatchStage {
+  ProjParams p;
+  BatchFrameDev f;
+  ProjBinDev pb;
+};
+static_assert(sizeof(ProjParams) % 4 == 0 && sizeof(BatchFrameDev) % 4 == 0 && sizeof(ProjBinDev) % 4 == 0,
+              "staged structures are copied as 32-bit words");
+
+__device__ __forceinline__ bool next_item(unsigned* counter, const BatchItem* __restrict__ items, int nitems,
+                                          const ProjParams* __restrict__ geoms, const BatchFrameDev* __restrict__ frames,
+                                          BatchStage& st) {
   __shared__ int s_item;
-  __syncthreads();  // every thread has finished with the previous item (shared row, s_item)
+  __syncthreads();  // every thread has finished with the previous item (shared row, stage, s_item)
   if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
   __syncthreads();
-  return s_item;
+  const int it = s_item;
+  if (it >= nitems) return false;
+  const BatchItem wi = items[it];
+  const int g = frames[wi.frame].geom;
+  constexpr int nf = sizeof(BatchFrameDev) / 4, np = sizeof(ProjParams) / 4, nb = sizeof(ProjBinDev) / 4;
+  static_assert(nf + np + nb <= kThreads, "one word per thread");
+  const int t = threadIdx.x;
+  if (t < nf) {
+    reinterpret_cast<uint32_t*>(&st.f)[t] = reinterpret_cast<const uint32_t*>(frames + wi.frame)[t];
+  } else if (t < nf + np) {
+    reinterpret_cast<uint32_t*>(&st.p)[t - nf] = reinterpret_cast<const uint32_t*>(geoms + g)[t - nf];
+  } else if (t < nf + np + nb) {
+    reinterpret_cast<uint32_t*>(&st.pb)[t - nf - np] = reinterpret_cast<const uint32_t*>(geoms[g].bins + wi.bin)[t - nf - np];
+  }
+  __syncthreads();
+  return true;
 }
 
 template <int NPA>
-__global__ void __launch_bounds__(kThreads) forward_batch_kernel(const ProjParams* __restrict__ geoms,
-                                                                 const BatchFrameDev* __restrict__ frames,
-                                                                 const BatchItem* __restrict__ items, int nitems,
-                                                                 unsigned* counter) {
+__global__ void __launch_bounds__(kThreads, kMinCtasForward) forward_batch_kernel(const ProjParams* __restrict__ geoms,
+                                                                           const BatchFrameDev* __restrict__ frames,
+                                                                           const BatchItem* __restrict__ items,
+                                                                           int nitems, unsigned* counter) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BatchStage st;
   const int lane = threadIdx.x & 31;
-  for (;;) {
-    const int it = next_item(counter);
-    if (it >= nitems) break;
-    const BatchItem wi = items[it];
-    const BatchFrameDev& f = frames[wi.frame];
-    const ProjParams& p = geoms[f.geom];
-    const ProjBinDev pb = p.bins[wi.bin];
+  while (next_item(counter, items, nitems, geoms, frames, st)) {
     double ll = 0.0;
     unsigned ncancel = 0;
-    forward_bin<NPA, kEpiRatio>(p, pb, smem, f.x, f.ratio, f.ep, ll, ncancel);
+    forward_bin<NPA, kEpiRatio>(st.p, st.pb, smem, st.f.x, st.f.ratio, st.f.ep, ll, ncancel);
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
-    if (lane == 0 && ncancel && f.ep.cancelled) atomicAdd(f.ep.cancelled, ncancel);
+    if (lane == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
   }
 }
 
 template <int NPA>
-__global__ void __launch_bounds__(kThreads) back_batch_kernel(const ProjParams* __restrict__ geoms,
-                                                              const BatchFrameDev* __restrict__ frames,
-                                                              const BatchItem* __restrict__ items, int nitems,
-                                                              unsigned* counter) {
+__global__ void __launch_bounds__(kThreads, kMinCtasBack) back_batch_kernel(const ProjParams* __restrict__ geoms,
+                                                                        const BatchFrameDev* __restrict__ frames,
+                                                                        const BatchItem* __restrict__ items,
+                                                                        int nitems, unsigned* counter) {
   extern __shared__ __align__(16) unsigned char smem[];
-  for (;;) {
-    const int it = next_item(counter);
-    if (it >= nitems) break;
-    const BatchItem wi = items[it];
-    const BatchFrameDev& f = frames[wi.frame];
-    const ProjParams& p = geoms[f.geom];
-    const ProjBinDev pb = p.bins[wi.bin];
-    back_bin<NPA, FloatAcc>(p, pb, smem, f.ratio, FloatAcc{f.u}, 0);
-  }
+  __shared__ BatchStage st;
+  while (next_item(counter, items, nitems, geoms, frames, st))
+    back_bin<NPA, FloatAcc>(st.p, st.pb, smem, st.f.ratio, FloatAcc{st.f.u}, 0);
 }
 
 // image [z][y][x] <-> [y][x][z]: a transpose of (nz) x (ny*nx)

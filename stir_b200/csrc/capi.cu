@@ -8,6 +8,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/stir_b200.h"
@@ -107,6 +108,20 @@ struct b200rt_projector {
   float det_bound_value = 0.f;
   bool colmax_ready = false;
   float prior_w[27] = {0};
+  // column-staged projection (paths.cu): path items, their lines, rows in path order
+  bool use_paths = false;
+  DevBuf<PathElem> path_elems;
+  DevBuf<uint32_t> path_cols;
+  DevBuf<PathLineDev> path_lines;
+  DevBuf<PathItemDev> path_items;
+  DevBuf<int> path_chunks;
+  DevBuf<PathCElem> path_cmaj;
+  DevBuf<int> path_col_starts;
+  PathParams pparams{};
+  std::vector<int> h_item_view;  // basic view of each path item
+  std::vector<PathItemDev> h_path_items;
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf<int>>> path_lists;
+  std::map<std::pair<int, int>, int> path_counts;
   // staging for the host API
   DevBuf<float> st_img_a, st_img_b, st_pd_a, st_pd_b;
   cudaStream_t stream = nullptr;
@@ -132,6 +147,198 @@ int status_of(const std::exception& e) {
 }
 
 // Builds all basic rows on the device (ProjMatrixByBin cache fill) and the projector tables.
+// Path items of a non-TOF projector (paths.cu): for each basic view and tangential position, the union of
+// the columns (x, y) of its basic rows (one per basic segment; all the same path), each row re-sorted by
+// (column slot, z), and one item per transaxial symmetry operation used by the related lines.  Leaves
+// use_paths false where the column-staged kernels do not apply.
+void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std::vector<LineDev>& lines,
+                 int nviews, int nsegs, int ntangs, const std::vector<int>& bviews) {
+  const Geometry& g = *h.geo;
+  const ProjParams& p = h.params;
+  const int nz = p.nz;
+  if (g.num_tof() != 1 || nz < 1) return;
+  int nax_max = 1;
+  for (int sg = -g.S(); sg <= g.S(); ++sg) nax_max = std::max(nax_max, g.nax(sg));
+  const int K = std::max(8, 32768 / (4 * nz));  // 32 KB of staged float columns
+  const int ngroups = nviews * ntangs;
+
+  struct Group {
+    std::vector<uint32_t> cols;
+    std::vector<PathElem> elems;
+    std::vector<int64_t> member_off;  // per segment: first element (relative)
+    std::vector<int> chunks;
+    std::vector<int> member_chunk;    // per segment: first chunk-table entry (relative)
+    std::vector<PathCElem> cmaj;      // the elements in column order: slot, member, z
+    std::vector<int> col_starts;      // first element of each column in cmaj, ncols + 1 entries
+    bool ok = true;
+  };
+  std::vector<Group> groups(ngroups);
+  auto work = [&](int g0, int g1) {
+    std::vector<std::pair<uint64_t, float>> tmp;
+    for (int gi = g0; gi < g1; ++gi) {
+      Group& G = groups[gi];
+      const int vi = gi / ntangs, ti = gi % ntangs;
+      std::vector<uint32_t> keys;
+      for (int si = 0; si < nsegs; ++si) {
+        const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
+        for (int k = 0; k < pb.row_len; ++k) keys.push_back(hr[pb.row_offset + k].zyx & 0x3fffffu);  // x, y bits
+      }
+      std::sort(keys.begin(), keys.end());
+      keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+      if (keys.size() > 65535) {
+        G.ok = false;
+        continue;
+      }
+      G.cols = keys;
+      const int ncols = static_cast<int>(keys.size());
+      const int nch = (ncols + K - 1) / K;
+      for (int si = 0; si < nsegs; ++si) {
+        const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
+        tmp.clear();
+        for (int k = 0; k < pb.row_len; ++k) {
+          const RowElem e = hr[pb.row_offset + k];
+          const uint32_t slot =
+              static_cast<uint32_t>(std::lower_bound(keys.begin(), keys.end(), e.zyx & 0x3fffffu) - keys.begin());
+          const uint32_t zb = e.zyx >> 22;  // z + 512
+          tmp.push_back({(static_cast<uint64_t>(slot) << 32) | (static_cast<uint64_t>(zb) << 16) | 0u, e.v});
+        }
+        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<uint64_t, float>& a,
+                                                    const std::pair<uint64_t, float>& b) { return a.first < b.first; });
+        G.member_off.push_back(static_cast<int64_t>(G.elems.size()));
+        G.member_chunk.push_back(static_cast<int>(G.chunks.size()));
+        for (const auto& t : tmp) {
+          const uint32_t slot = static_cast<uint32_t>(t.first >> 32);
+          const uint32_t zb = static_cast<uint32_t>((t.first >> 16) & 0xffffu);
+          G.elems.push_back(PathElem{slot | (zb << 16), t.second});
+        }
+        // chunk c covers the elements with slot in [c K, (c + 1) K)
+        size_t k = 0;
+        for (int c = 0; c <= nch; ++c) {
+          const uint32_t lim = static_cast<uint32_t>(std::min(c * K, ncols));
+          while (k < tmp.size() && (tmp[k].first >> 32) < lim) ++k;
+          G.chunks.push_back(static_cast<int>(k));
+        }
+      }
+      // the same elements in column order (slot, then member, then z) for the back projection
+      std::vector<size_t> cur(nsegs);
+      for (int si = 0; si < nsegs; ++si) cur[si] = static_cast<size_t>(G.member_off[si]);
+      for (int slot = 0; slot < ncols; ++slot) {
+        G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
+        for (int si = 0; si < nsegs; ++si) {
+          const size_t end = si + 1 < nsegs ? static_cast<size_t>(G.member_off[si + 1]) : G.elems.size();
+          while (cur[si] < end && static_cast<int>(G.elems[cur[si]].sz & 0xffffu) == slot) {
+            const PathElem& e = G.elems[cur[si]];
+            G.cmaj.push_back(PathCElem{(e.sz >> 16) | (static_cast<uint32_t>(si) << 16), e.v});
+            ++cur[si];
+          }
+        }
+      }
+      G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
+    }
+  };
+  const int nthreads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nthreads; ++t) {
+    const int g0 = static_cast<int>(static_cast<int64_t>(ngroups) * t / nthreads);
+    const int g1 = static_cast<int>(static_cast<int64_t>(ngroups) * (t + 1) / nthreads);
+    pool.emplace_back(work, g0, g1);
+  }
+  for (auto& th : pool) th.join();
+  for (const Group& G : groups)
+    if (!G.ok) return;
+
+  std::vector<PathElem> elems;
+  std::vector<PathCElem> cmaj;
+  std::vector<int> col_starts;
+  std::vector<uint32_t> cols;
+  std::vector<int> chunks;
+  std::vector<PathLineDev> plines;
+  std::vector<PathItemDev> items;
+  std::vector<int> item_view;
+  int max_lines = 1;
+  for (int gi = 0; gi < ngroups; ++gi) {
+    const Group& G = groups[gi];
+    const int vi = gi / ntangs, ti = gi % ntangs;
+    const int64_t elem_base = static_cast<int64_t>(elems.size());
+    const int chunk_base = static_cast<int>(chunks.size());
+    const int col_base = static_cast<int>(cols.size());
+    const int64_t cmaj_base = static_cast<int64_t>(cmaj.size());
+    const int cs_base = static_cast<int>(col_starts.size());
+    cmaj.insert(cmaj.end(), G.cmaj.begin(), G.cmaj.end());
+    col_starts.insert(col_starts.end(), G.col_starts.begin(), G.col_starts.end());
+    elems.insert(elems.end(), G.elems.begin(), G.elems.end());
+    chunks.insert(chunks.end(), G.chunks.begin(), G.chunks.end());
+    cols.insert(cols.end(), G.cols.begin(), G.cols.end());
+    for (int T = 0; T < 8; ++T) {
+      PathItemDev it{};
+      it.col_offset = col_base;
+      it.ncols = static_cast<int>(G.cols.size());
+      it.first_line = static_cast<int>(plines.size());
+      it.flags = T;
+      it.col_starts = cs_base;
+      it.cmaj_off = cmaj_base;
+      for (int si = 0; si < nsegs; ++si) {
+        const int b = (vi * nsegs + si) * ntangs + ti;
+        const ProjBinDev& pb = h.h_bins[b];
+        for (int l = 0; l < pb.num_lines; ++l) {
+          if ((lines[pb.first_line + l].flags & 7) != T) continue;
+          PathLineDev pl{};
+          pl.line = pb.first_line + l;
+          pl.bin = b;
+          pl.elem_off = elem_base + G.member_off[si];
+          pl.chunk_off = chunk_base + G.member_chunk[si];
+          pl.member = si;
+          plines.push_back(pl);
+        }
+      }
+      it.num_lines = static_cast<int>(plines.size()) - it.first_line;
+      if (it.num_lines == 0) continue;
+      max_lines = std::max(max_lines, it.num_lines);
+      items.push_back(it);
+      item_view.push_back(bviews[vi]);
+    }
+  }
+  if (elems.size() >= (size_t(1) << 31) || chunks.size() >= (size_t(1) << 31) || col_starts.size() >= (size_t(1) << 31))
+    return;
+  int npa_max = 1;
+  for (int sg = -g.S(); sg <= g.S(); ++sg) npa_max = std::max(npa_max, g.npa(sg));
+  int max_chunk = 1;
+  for (const Group& G : groups)
+    for (size_t m = 0; m < G.member_chunk.size(); ++m) {
+      const int c1 = m + 1 < G.member_chunk.size() ? G.member_chunk[m + 1] : static_cast<int>(G.chunks.size());
+      for (int c = G.member_chunk[m]; c + 1 < c1; ++c) max_chunk = std::max(max_chunk, G.chunks[c + 1] - G.chunks[c]);
+    }
+  if (path_smem_fwd(K, nz, max_lines, nax_max, npa_max).total > 200 * 1024 ||
+      path_smem_back(nz, max_lines, nsegs, nax_max, npa_max).total > 200 * 1024)
+    return;
+
+  h.path_elems.upload(elems, h.stream);
+  h.path_cols.upload(cols, h.stream);
+  h.path_lines.upload(plines, h.stream);
+  h.path_items.upload(items, h.stream);
+  h.path_chunks.upload(chunks, h.stream);
+  h.path_cmaj.upload(cmaj, h.stream);
+  h.path_col_starts.upload(col_starts, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "path tables");
+  PathParams& pp = h.pparams;
+  pp.elems = h.path_elems.p;
+  pp.cols = h.path_cols.p;
+  pp.lines = h.path_lines.p;
+  pp.items = h.path_items.p;
+  pp.chunks = h.path_chunks.p;
+  pp.K = K;
+  pp.max_lines = max_lines;
+  pp.nax_max = nax_max;
+  pp.npa_max = npa_max;
+  pp.max_chunk_elems = max_chunk;
+  pp.cmaj = h.path_cmaj.p;
+  pp.col_starts = h.path_col_starts.p;
+  pp.max_members = nsegs;
+  h.h_item_view = item_view;
+  h.h_path_items = items;
+  h.use_paths = true;
+}
+
 void setup_projector(b200rt_projector& h) {
   Geometry& g = *h.geo;
   DeviceGuard dg(h.device);
@@ -445,6 +652,9 @@ void setup_projector(b200rt_projector& h) {
       }
     }
     h.total_nnz = t;
+    if (g.num_tof() == 1)
+      build_paths(h, hr, lines, static_cast<int>(bviews.size()), static_cast<int>(bsegs.size()),
+                  static_cast<int>(btangs.size()), bviews);
   }
 }
 
@@ -467,6 +677,41 @@ const int* subset_list(b200rt_projector& h, int subset, int nsub, int& count) {
   const int* p = buf->p;
   h.subset_lists[key] = std::move(buf);
   return p;
+}
+
+// path items (column-staged kernels) of a subset: those whose basic view v has v mod nsub == subset
+const int* path_list(b200rt_projector& h, int subset, int nsub, int& count) {
+  const auto key = std::make_pair(subset, nsub);
+  auto it = h.path_lists.find(key);
+  if (it != h.path_lists.end()) {
+    count = h.path_counts[key];
+    return it->second->p;
+  }
+  std::vector<int> list;
+  for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i)
+    if (h.h_item_view[i] % nsub == subset) list.push_back(i);
+  auto buf = std::make_unique<DevBuf<int>>();
+  buf->upload(list, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "path list");
+  count = static_cast<int>(list.size());
+  h.path_counts[key] = count;
+  const int* p = buf->p;
+  h.path_lists[key] = std::move(buf);
+  return p;
+}
+
+// forward projection of one subset with the column-staged kernel where it applies (not for the
+// log-likelihood, whose per-CTA partial sums follow the basic bins), else the per-basic-bin kernel
+void forward_subset(b200rt_projector& h, const float* image, float* out, int subset, int nsub, cudaStream_t st,
+                    const FwdEpilogue* ep = nullptr) {
+  int n = 0;
+  if (h.use_paths && (!ep || ep->mode != kEpiLoglik)) {
+    const int* list = path_list(h, subset, nsub, n);
+    ck(launch_forward_paths(h.params, h.pparams, list, n, image, out, st, ep), "forward projection");
+  } else {
+    const int* list = subset_list(h, subset, nsub, n);
+    ck(launch_forward(h.params, list, n, image, out, st, ep), "forward projection");
+  }
 }
 
 // device list of every view of the subset: the basic views and their symmetry partners
@@ -523,10 +768,13 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
   const Geometry& g = *h.geo;
   const int64_t ni = g.image_size();
   int n = 0;
-  const int* list = subset_list(h, subset, nsub, n);
+  const int* list = h.use_paths ? path_list(h, subset, nsub, n) : subset_list(h, subset, nsub, n);
   if (mode == B200RT_BACKPROJECT_ATOMIC) {
     ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
-    ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
+    if (h.use_paths)
+      ck(launch_back_paths_atomic(h.params, h.pparams, list, n, pd, image, st, zero_ends), "back projection");
+    else
+      ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
     return;
   }
   h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(g.projdata_size(), ni)), 1));
@@ -534,9 +782,12 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
     // largest column sum of A (A^T 1 over every bin): bounds every voxel's sum of |w d| / max|d|
     h.colmax.alloc(1);
     int nall = 0;
-    const int* all = subset_list(h, 0, 1, nall);
+    const int* all = h.use_paths ? path_list(h, 0, 1, nall) : subset_list(h, 0, 1, nall);
     ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
-    ck(launch_back_atomic(h.params, all, nall, nullptr, image, st, 0), "column sums");
+    if (h.use_paths)
+      ck(launch_back_paths_atomic(h.params, h.pparams, all, nall, nullptr, image, st, 0), "column sums");
+    else
+      ck(launch_back_atomic(h.params, all, nall, nullptr, image, st, 0), "column sums");
     ck(launch_max(image, ni, h.det_partial.p, h.colmax.p, st), "column sums");
     h.colmax_ready = true;
   }
@@ -553,7 +804,11 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
     ck(launch_fixed_scale(pd, pd ? g.projdata_size() : 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
   }
   ck(cudaMemsetAsync(h.acc64.p, 0, sizeof(unsigned long long) * ni, st), "memset");
-  ck(launch_back_fixed(h.params, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends), "back projection");
+  if (h.use_paths)
+    ck(launch_back_paths_fixed(h.params, h.pparams, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends),
+       "back projection");
+  else
+    ck(launch_back_fixed(h.params, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends), "back projection");
   ck(launch_fixed_to_float(h.acc64.p, h.fixed_scale.p, image, ni, st), "back projection");
 }
 
@@ -614,6 +869,14 @@ void b200rt_destroy(b200rt_projector* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->subset_lists.clear();
     h->subset_views.clear();
+    h->path_lists.clear();
+    h->path_elems.release();
+    h->path_cols.release();
+    h->path_lines.release();
+    h->path_items.release();
+    h->path_chunks.release();
+    h->path_cmaj.release();
+    h->path_col_starts.release();
     h->ratio.release();
     h->upd.release();
     h->grad.release();
@@ -736,9 +999,7 @@ int b200rt_forward_project_dev(b200rt_projector* h, const float* image_dev, floa
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
   try {
     DeviceGuard dg(h->device);
-    int n = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    ck(launch_forward(h->params, list, n, image_dev, projdata_dev, static_cast<cudaStream_t>(stream)), "forward projection");
+    forward_subset(*h, image_dev, projdata_dev, subset_num, num_subsets, static_cast<cudaStream_t>(stream));
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());
@@ -775,9 +1036,7 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
     ck(cudaMemcpyAsync(h->st_img_a.p, image_host, sizeof(float) * g.image_size(), cudaMemcpyHostToDevice, st), "H2D");
     ck(launch_image_to_dev(h->st_img_a.p, h->st_img_b.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
     ck(cudaMemsetAsync(h->st_pd_b.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
-    int n = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
-    ck(launch_forward(h->params, list, n, h->st_img_b.p, h->st_pd_b.p, st), "forward projection");
+    forward_subset(*h, h->st_img_b.p, h->st_pd_b.p, subset_num, num_subsets, st);
     ck(projdata_layout(g, h->st_pd_b.p, h->st_pd_a.p, false, st), "layout");
     ck(cudaMemcpyAsync(projdata_host, h->st_pd_a.p, sizeof(float) * g.projdata_size(), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "forward projection");
@@ -843,8 +1102,7 @@ void osmaposl_numerator(b200rt_projector& h, const float* x, const float* y, con
   }
   h.small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
   h.cancelled.alloc(1);
-  int n = 0, nv = 0;
-  const int* list = subset_list(h, subset, nsub, n);
+  int nv = 0;
   const int* views = subset_views(h, subset, nsub, nv);
   ck(launch_viewgram_small_values(y, h.segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_ends, g.num_tof(),
                                   g.tof_stride(), h.small_value.p, st),
@@ -857,7 +1115,7 @@ void osmaposl_numerator(b200rt_projector& h, const float* x, const float* y, con
   ep.add = add;
   ep.small_value = h.small_value.p;
   ep.cancelled = h.cancelled.p;
-  ck(launch_forward(h.params, list, n, x, h.ratio.p, st, &ep), "forward projection");
+  forward_subset(h, x, h.ratio.p, subset, nsub, st, &ep);
   back_project_into(h, h.ratio.p, u, subset, nsub, mode, 0, st, 10000.F);
 }
 
@@ -1035,8 +1293,7 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
     }
     h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
     h->cancelled.alloc(1);
-    int n = 0, nv = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    int nv = 0;
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
                                     g.num_tof(), g.tof_stride(), h->small_value.p, st),
@@ -1050,7 +1307,7 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
     ep.mult = mult_dev;
     ep.small_value = h->small_value.p;
     ep.cancelled = h->cancelled.p;
-    ck(launch_forward(h->params, list, n, image_dev, h->ratio.p, st, &ep), "forward projection");
+    forward_subset(*h, image_dev, h->ratio.p, subset_num, num_subsets, st, &ep);
     back_project_into(*h, h->ratio.p, gradient_dev, subset_num, num_subsets, back_projection_mode, 0, st);
     return B200RT_OK;
   } catch (const std::exception& e) {
@@ -1218,6 +1475,9 @@ struct b200rt_batch {
   std::vector<std::unique_ptr<Frame>> frames;
   std::vector<b200rt_projector*> geoms;
   DevBuf<b200::ProjParams> d_geoms;
+  DevBuf<b200::PathParams> d_pgeoms;
+  bool paths = false;  // every frame's projector has path items: the column-staged batched kernels
+  int smem_f = 0, smem_b = 0;
   DevBuf<b200::BatchFrameDev> d_frames;
   DevBuf<unsigned int> counters;  // work-queue heads of the forward and back launches
   bool ready = false;
@@ -1261,6 +1521,20 @@ void batch_finalize(b200rt_batch& b) {
   b.smem = b200::proj_smem_bytes(max_row);
   cudaStream_t st = b.capture_stream;
   b.d_geoms.upload(gp, st);
+  b.paths = true;
+  for (auto* h : b.geoms) b.paths = b.paths && h->use_paths;
+  if (b.paths) {
+    std::vector<b200::PathParams> pg;
+    b.smem_f = b.smem_b = 0;
+    for (auto* h : b.geoms) {
+      const b200::PathParams& pp = h->pparams;
+      pg.push_back(pp);
+      b.smem_f = std::max(b.smem_f, b200::path_smem_fwd(pp.K, h->params.nz, pp.max_lines, pp.nax_max, pp.npa_max).total);
+      b.smem_b = std::max(b.smem_b, b200::path_smem_back(h->params.nz, pp.max_lines, pp.max_members, pp.nax_max,
+                                                          pp.npa_max).total);
+    }
+    b.d_pgeoms.upload(pg, st);
+  }
   std::vector<BatchFrameDev> fd;
   for (auto& fp : b.frames) {
     auto& f = *fp;
@@ -1292,8 +1566,13 @@ void batch_finalize(b200rt_batch& b) {
   b.d_frames.upload(fd, st);
   b.counters.alloc(2);
   ck(cudaDeviceGetAttribute(&b.num_sms, cudaDevAttrMultiProcessorCount, b.device), "device attribute");
-  b.max_fwd = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
-  b.max_back = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
+  if (b.paths) {
+    b.max_fwd = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
+    b.max_back = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
+  } else {
+    b.max_fwd = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
+    b.max_back = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
+  }
   if (b.max_fwd < 1 || b.max_back < 1) throw std::runtime_error("batched projector does not fit on an SM");
   ck(cudaStreamSynchronize(st), "batch set-up");
   b.ready = true;
@@ -1313,15 +1592,27 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
     if (key[fi + 1] < 0) continue;
     const auto& f = *b.frames[fi];
     const b200rt_projector& h = *f.h;
-    std::vector<int> bins;
-    for (int bin = 0; bin < static_cast<int>(h.h_bins.size()); ++bin)
-      if (h.h_bin_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
-    if (order == 1) {
-      std::stable_sort(bins.begin(), bins.end(), [&](int a, int c) {
-        const auto& pa = h.h_bins[a];
-        const auto& pc = h.h_bins[c];
-        return static_cast<int64_t>(pa.row_len) * pa.num_lines > static_cast<int64_t>(pc.row_len) * pc.num_lines;
-      });
+    std::vector<int> bins;  // basic bins, or path items with the column-staged kernels
+    if (b.paths) {
+      for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i)
+        if (h.h_item_view[i] % f.nsub == key[fi + 1]) bins.push_back(i);
+      if (order == 1) {
+        std::stable_sort(bins.begin(), bins.end(), [&](int a, int c) {
+          const auto& pa = h.h_path_items[a];
+          const auto& pc = h.h_path_items[c];
+          return static_cast<int64_t>(pa.ncols) * pa.num_lines > static_cast<int64_t>(pc.ncols) * pc.num_lines;
+        });
+      }
+    } else {
+      for (int bin = 0; bin < static_cast<int>(h.h_bins.size()); ++bin)
+        if (h.h_bin_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
+      if (order == 1) {
+        std::stable_sort(bins.begin(), bins.end(), [&](int a, int c) {
+          const auto& pa = h.h_bins[a];
+          const auto& pc = h.h_bins[c];
+          return static_cast<int64_t>(pa.row_len) * pa.num_lines > static_cast<int64_t>(pc.row_len) * pc.num_lines;
+        });
+      }
     }
     for (int bin : bins) list.push_back(BatchItem{static_cast<int>(fi), bin});
   }
@@ -1355,16 +1646,24 @@ void batch_thresholds(b200rt_batch& b, int k, cudaStream_t st) {
   }
 }
 
+// one batched launch of one direction (0 forward with the ratio epilogue, 1 back projection of the ratios)
+cudaError_t batch_launch(b200rt_batch& b, int dir, const BatchItem* items, int n, int grid, cudaStream_t st) {
+  if (b.paths)
+    return dir == 0 ? b200::launch_forward_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.npa, b.smem_f, b.d_frames.p, items,
+                                                       n, b.counters.p, grid, st)
+                    : b200::launch_back_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.smem_b, b.d_frames.p, items, n,
+                                                    b.counters.p + 1, grid, st);
+  return dir == 0 ? b200::launch_forward_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p, grid, st)
+                  : b200::launch_back_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p + 1, grid,
+                                            st);
+}
+
 void batch_projections(b200rt_batch& b, int k, cudaStream_t st) {
   int n = 0;
   const BatchItem* items = batch_items(b, k, b.cfg.order, n);
   ck(cudaMemsetAsync(b.counters.p, 0, 2 * sizeof(unsigned int), st), "memset");
-  ck(b200::launch_forward_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p,
-                                grid_of(b, b.cfg.ctas_per_sm_forward, b.max_fwd), st),
-     "batched forward projection");
-  ck(b200::launch_back_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p + 1,
-                             grid_of(b, b.cfg.ctas_per_sm_back, b.max_back), st),
-     "batched back projection");
+  ck(batch_launch(b, 0, items, n, grid_of(b, b.cfg.ctas_per_sm_forward, b.max_fwd), st), "batched forward projection");
+  ck(batch_launch(b, 1, items, n, grid_of(b, b.cfg.ctas_per_sm_back, b.max_back), st), "batched back projection");
 }
 
 void batch_subiteration(b200rt_batch& b, int k, cudaStream_t st) {
@@ -1412,6 +1711,7 @@ void b200rt_batch_destroy(b200rt_batch* b) {
     b->items.clear();
     b->frames.clear();
     b->d_geoms.release();
+    b->d_pgeoms.release();
     b->d_frames.release();
     b->counters.release();
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
@@ -1533,12 +1833,7 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
       for (int rep = 0; rep < 3; ++rep) {
         ck(cudaMemsetAsync(b->counters.p, 0, 2 * sizeof(unsigned int), st), "memset");
         ck(cudaEventRecord(e0, st), "cudaEventRecord");
-        if (dir == 0)
-          ck(b200::launch_forward_batch(b->d_geoms.p, b->npa, b->smem, b->d_frames.p, items, n, b->counters.p, grid, st),
-             "batched forward projection");
-        else
-          ck(b200::launch_back_batch(b->d_geoms.p, b->npa, b->smem, b->d_frames.p, items, n, b->counters.p + 1, grid, st),
-             "batched back projection");
+        ck(batch_launch(*b, dir, items, n, grid, st), dir == 0 ? "batched forward projection" : "batched back projection");
         ck(cudaEventRecord(e1, st), "cudaEventRecord");
         ck(cudaEventSynchronize(e1), "cudaEventSynchronize");
         float ms = 0.f;

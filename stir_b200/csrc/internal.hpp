@@ -117,6 +117,134 @@ struct BatchItem {
   int bin;
 };
 
+// ---- column-staged projection (paths.cu) --------------------------------------------------------
+// The basic bins that share a basic view and tangential position (one per segment) trace the same
+// transaxial path, so their rows cross the same voxel columns (x, y).  A "path item" is such a group
+// together with one transaxial symmetry operation T (swap, -x, -y): its lines (every segment, both z
+// orientations) read the columns T(x, y) of the path, which one CTA copies to shared memory in chunks
+// of K columns (all z of a column, contiguous in the [y][x][z] layout).
+
+// Row element of a path: the column's index in the path ("slot", bits 0..15) and z + 512 (bits 16..31).
+struct __align__(8) PathElem {
+  uint32_t sz;
+  float v;
+};
+struct PathLineDev {
+  int line;          // index into lines[]
+  int bin;           // basic bin (projection data position, tangential position)
+  int64_t elem_off;  // first element of the bin's row in path order (sorted by slot, then z)
+  int chunk_off;     // the row's chunk table in chunks[]: chunk c covers elements [tab[c], tab[c+1])
+  int member;        // the bin's position among the path's basic bins (its segment)
+};
+struct PathItemDev {
+  int col_offset, ncols;        // path columns in cols[], packed (x + 1024) | (y + 1024) << 11
+  int first_line, num_lines;    // into path lines[]; the lines of one member are consecutive
+  int flags;                    // T: bit 0 swap x/y, bit 1 negate x, bit 2 negate y
+  int col_starts;               // the path's column table in col_starts[] (ncols + 1 entries)
+  int64_t cmaj_off;             // the path's elements in column order in cmaj[]
+};
+// A path element in column order: z + 512 (bits 0..15), the member (bits 16..31), the value.
+struct __align__(8) PathCElem {
+  uint32_t mz;
+  float v;
+};
+struct PathParams {
+  const PathElem* elems;
+  const uint32_t* cols;
+  const PathLineDev* lines;
+  const PathItemDev* items;
+  const int* chunks;
+  int K;          // columns per chunk
+  int max_lines;  // lines of the largest item
+  int nax_max;    // axial positions of the longest segment
+  int npa_max;    // largest planes per axial position
+  int max_chunk_elems;  // most elements of one row in one chunk
+  const PathCElem* cmaj;  // every path's elements ordered by column, then member, then z
+  const int* col_starts;  // per path: first element of each column in cmaj (relative), ncols + 1 entries
+  int max_members;        // basic bins per path (basic segments)
+};
+
+// parts each line's elements are split into (forward), so that an item's lines keep all warps busy
+__host__ __device__ inline int path_parts(int num_lines) { return num_lines >= 8 ? 2 : (num_lines >= 4 ? 4 : 8); }
+
+struct PathLineSmem {
+  int64_t out_base;  // device-layout projection index of (line, axial 0)
+  int64_t elem_off;
+  int chunk_off;
+  int nax, npa;
+  int zsign, zadd;  // z index in the image = zsign * (sz >> 16) + zadd  (z reflection, -512 bias, -min_z)
+  int seg, view, tofi;
+  int active;       // tangential position inside the projection data
+  int member;
+};
+// a row element of one line and one pass, in shared memory (forward)
+struct __align__(16) PathXElem {
+  int base;  // staged-column index of axial position 0
+  int zt;    // image z of axial position 0
+  float v;
+  int full;  // z stays inside the image for every lane of the pass
+};
+constexpr int kPathWarpsH = 8;
+
+__host__ __device__ inline int path_align16(int x) { return (x + 15) & ~15; }
+// the back projection's per-line data, padded with zeros: d(a) at index F + a npa, F = path_dl_front(nz),
+// read at F + z - zt for planes z in [0, nz + 127) and windows [zt, zt + (nax - 1) npa] that meet the image;
+// indices [0, F) are zero
+__host__ __device__ inline int path_dl_front(int nz) { return nz + 128; }
+__host__ __device__ inline int path_dl_len(int nz, int nax_max, int npa_max) {
+  return (2 * nz + 256 + (nax_max - 1) * npa_max + 3) & ~3;
+}
+
+// dynamic shared memory of a forward path CTA: staged columns, their image offsets, line set-up,
+// per-warp element buffers, per (line, part) accumulators
+struct PathSmemFwd {
+  int colbase, lines, xbuf, acc, total;
+};
+__host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int max_lines, int nax_max, int npa_max) {
+  PathSmemFwd s;
+  s.colbase = path_align16((K * nz + 128 * npa_max) * 4);  // staged columns and a pass's overshoot
+  s.lines = path_align16(s.colbase + K * 4);
+  s.xbuf = path_align16(s.lines + max_lines * static_cast<int>(sizeof(PathLineSmem)));
+  s.acc = s.xbuf + kPathWarpsH * 32 * static_cast<int>(sizeof(PathXElem));
+  int acc_rows = 0;  // the most (line, part) pairs of any item
+  for (int n = 1; n <= max_lines; ++n) acc_rows = acc_rows > n * path_parts(n) ? acc_rows : n * path_parts(n);
+  s.total = path_align16(s.acc + acc_rows * nax_max * 4);
+  return s;
+}
+// back path CTA: line set-up, per line (z sign, z offset, window length, data offset), per member its
+// first line and line count, padded line data
+struct PathSmemBack {
+  int lines, lz, members, dl, total;
+};
+__host__ __device__ inline PathSmemBack path_smem_back(int nz, int max_lines, int max_members, int nax_max,
+                                                       int npa_max) {
+  PathSmemBack s;
+  s.lines = 0;
+  s.lz = path_align16(max_lines * static_cast<int>(sizeof(PathLineSmem)));
+  s.members = path_align16(s.lz + max_lines * 16);
+  s.dl = path_align16(s.members + max_members * 8);
+  s.total = path_align16(s.dl + max_lines * path_dl_len(nz, nax_max, npa_max) * 4);
+  return s;
+}
+
+// launchers (paths.cu); the item lists hold indices into PathParams::items
+cudaError_t launch_forward_paths(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                 const float* image, float* projdata, cudaStream_t st, const FwdEpilogue* ep);
+cudaError_t launch_back_paths_atomic(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                     const float* projdata, float* image, cudaStream_t st, int zero_ends);
+cudaError_t launch_back_paths_fixed(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                    const float* projdata, unsigned long long* acc, const double* scale,
+                                    cudaStream_t st, int zero_ends);
+
+// persistent batched projectors over (frame, path item) work items (BatchItem::bin holds the path item)
+cudaError_t launch_forward_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int npa, int smem_bytes,
+                                       const BatchFrameDev* frames, const BatchItem* items, int nitems, unsigned* counter,
+                                       int grid, cudaStream_t st);
+cudaError_t launch_back_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int smem_bytes,
+                                    const BatchFrameDev* frames, const BatchItem* items, int nitems, unsigned* counter,
+                                    int grid, cudaStream_t st);
+int batch_paths_max_ctas_per_sm(int npa, int smem_bytes, bool forward);
+
 // launchers (project.cu)
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
                            cudaStream_t st, const FwdEpilogue* ep = nullptr);

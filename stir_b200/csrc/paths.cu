@@ -1,0 +1,537 @@
+// Column-staged forward and back projection.
+//
+// All basic bins with the same basic view and tangential position -- one per segment -- trace the same
+// transaxial path (the x/y crossings of STIR's Siddon tracer, RayTraceVoxelsOnCartesianGrid.cxx:51-269,
+// do not depend on the ring difference), so their rows cross the same voxel columns (x, y) at different
+// z.  A path item is such a path with one transaxial symmetry operation T (swap x/y, negate x, negate y;
+// SymmetryOperations_PET_CartesianGrid.h:48-482): its lines are the related lines of every segment
+// (both z orientations) that use T.  One CTA per item, over chunks of K columns of the path:
+//
+//   forward: the image columns T(x, y) -- all nz planes, contiguous in the [y][x][z] layout -- are copied
+//     to shared memory (one L2 read per column and item instead of one per line and row element); every
+//     (line, part) unit, one warp each, walks the part of its row in the chunk (rows are stored sorted by
+//     path slot, then z) with its lanes on the axial positions, as the per-basic-bin kernel does but
+//     gathering from shared memory; the parts of a line are added in a fixed order and go through the
+//     same epilogue as the per-basic-bin kernel;
+//   back: a warp owns a column and its lanes the planes z; it sums, in registers, the contributions of
+//     every line of the item to its voxels and adds them to the image once (a gather instead of a
+//     scatter: no shared-memory atomics, and a fixed order within the item).
+//
+// Sums are taken in path order rather than in the stored row order of ProjMatrixElemsForOneBin, so the
+// results differ from the per-basic-bin kernels by float rounding only; the fixed-point back projection
+// gives the same integers (each contribution is rounded the same way, integer addition is associative).
+#include "internal.hpp"
+#include "epilogue.cuh"
+
+namespace b200 {
+
+namespace {
+
+constexpr int kPathWarps = 8;
+constexpr int kPathThreads = kPathWarps * 32;
+constexpr int kPathMinCtas = 4;
+static_assert(kPathWarps == kPathWarpsH, "shared-memory layout and kernels agree on the warps per CTA");
+
+// line set-up of the item's lines (one thread per line)
+__device__ __forceinline__ void setup_path_lines(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+                                                 PathLineSmem* ls) {
+  for (int l = threadIdx.x; l < it.num_lines; l += blockDim.x) {
+    const PathLineDev pl = pp.lines[it.first_line + l];
+    const LineDev L = p.lines[pl.line];
+    const ProjBinDev pb = p.bins[pl.bin];
+    PathLineSmem s{};
+    const int tang = static_cast<int>(L.tang_sign) * pb.tang;
+    s.active = tang >= p.min_tang && tang <= p.max_tang;
+    const SegDev sd = p.segs[L.seg + p.S];
+    s.nax = sd.nax;
+    s.npa = sd.npa;
+    s.tofi = pb.tof - p.min_tof;
+    s.out_base = static_cast<int64_t>(s.tofi) * p.tof_stride + sd.dev_offset +
+                 (static_cast<int64_t>(L.view) * p.num_tang + (tang - p.min_tang)) * sd.nax;
+    s.elem_off = pl.elem_off;
+    s.chunk_off = pl.chunk_off;
+    // z index in the image of element z (stored as z + 512): zq ? q - z : z, minus min_z
+    if (L.flags & 8) {
+      s.zsign = -1;
+      s.zadd = static_cast<int>(L.q) + 512 - p.min_z;
+    } else {
+      s.zsign = 1;
+      s.zadd = -512 - p.min_z;
+    }
+    s.seg = L.seg;
+    s.view = L.view;
+    s.member = pl.member;
+    ls[l] = s;
+  }
+}
+
+// image offsets of the chunk's columns under the item's symmetry operation (-1 outside the image)
+__device__ __forceinline__ void chunk_columns(const ProjParams& p, const PathParams& pp, const PathItemDev& it, int c0,
+                                              int kc, int* colbase) {
+  const int swap = it.flags & 1;
+  const int sx = (it.flags & 2) ? -1 : 1;
+  const int sy = (it.flags & 4) ? -1 : 1;
+  for (int i = threadIdx.x; i < kc; i += blockDim.x) {
+    const uint32_t pk = pp.cols[it.col_offset + c0 + i];
+    const int x = static_cast<int>(pk & 2047u) - 1024;
+    const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
+    const int xi = (swap ? y : x) * sx - p.min_x;
+    const int yi = (swap ? x : y) * sy - p.min_y;
+    colbase[i] = (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * p.nz : -1;
+  }
+}
+
+// the element range of unit (line, part) in chunk c; P = 1 << lgP parts
+__device__ __forceinline__ void unit_range(const PathParams& pp, const PathLineSmem& L, int c, int part, int lgP, int& e0,
+                                           int& e1) {
+  const int lo = __ldg(pp.chunks + L.chunk_off + c);
+  const int n = __ldg(pp.chunks + L.chunk_off + c + 1) - lo;
+  e0 = lo + ((n * part) >> lgP);
+  e1 = lo + ((n * (part + 1)) >> lgP);
+}
+
+__device__ __forceinline__ int log2_parts(int P) { return P == 2 ? 1 : (P == 4 ? 2 : 3); }
+
+// 4-byte asynchronous copy global -> shared (completed by cp_async_wait)
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One pass of one unit over elements [e0, e1) of its row: NJ groups of 32 axial positions from a0.
+// The warp's lanes transform 32 elements at a time (column slot -> staged index, z reflection) into
+// the warp's buffer; then every element costs one broadcast read and NJ shared loads and FMAs.
+template <int NPA, int NJ>
+__device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int e0, int e1, int c0, const float* cols,
+                                            int nz, const PathLineSmem& L, int a0, int nact, int lane, float* acc_row,
+                                            PathXElem* xb) {
+  const int npa = NPA ? NPA : L.npa;
+  // lane's plane offset of group j: zo0 + 32 j npa.  In the full path inactive lanes (axial positions past
+  // the line's end) read up to 127 npa floats past the staged columns, into the zero-cost padding of the
+  // staging buffer, and their sums are dropped: the full path needs no per-lane tests.
+  const int zo0 = (a0 + lane) * npa;
+  bool act[NJ];
+  float acc[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    act[j] = j * 32 + lane < nact;
+    acc[j] = act[j] ? acc_row[a0 + j * 32 + lane] : 0.f;
+  }
+  const int zlo = a0 * npa, zhi = (a0 + nact - 1) * npa;
+  for (int k0 = e0; k0 < e1; k0 += 32) {
+    const int cnt = min(32, e1 - k0);
+    __syncwarp();
+    if (lane < cnt) {
+      const PathElem m = E[k0 + lane];
+      PathXElem x;
+      x.zt = L.zsign * static_cast<int>(m.sz >> 16) + L.zadd;
+      x.base = (static_cast<int>(m.sz & 0xffffu) - c0) * nz + x.zt;
+      x.v = m.v;
+      x.full = (x.zt + zlo >= 0) && (x.zt + zhi < nz);
+      xb[lane] = x;
+    }
+    __syncwarp();
+    for (int i = 0; i < cnt; ++i) {
+      const PathXElem e = xb[i];
+      const float* q = cols + (e.base + zo0);
+      if (e.full) {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) acc[j] += q[j * 32 * npa] * e.v;
+      } else {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const int zz = e.zt + zo0 + j * 32 * npa;
+          if (act[j] && static_cast<unsigned>(zz) < static_cast<unsigned>(nz)) acc[j] += q[j * 32 * npa] * e.v;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NJ; ++j)
+    if (act[j]) acc_row[a0 + j * 32 + lane] = acc[j];
+}
+
+template <int NPA, int EPI>
+__device__ __forceinline__ void forward_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+                                                  unsigned char* smem, const float* __restrict__ img,
+                                                  float* __restrict__ out, const FwdEpilogue& ep, double& ll,
+                                                  unsigned& ncancel) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nz = p.nz;
+  const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.max_lines, pp.nax_max, pp.npa_max);
+  float* cols = reinterpret_cast<float*>(smem);
+  int* colbase = reinterpret_cast<int*>(smem + lay.colbase);
+  PathLineSmem* ls = reinterpret_cast<PathLineSmem*>(smem + lay.lines);
+  PathXElem* xb = reinterpret_cast<PathXElem*>(smem + lay.xbuf) + warp * 32;
+  float* lacc = reinterpret_cast<float*>(smem + lay.acc);
+  const int nl = it.num_lines, P = path_parts(nl), lgP = log2_parts(P), U = nl * P;
+  setup_path_lines(p, pp, it, ls);
+  for (int i = threadIdx.x; i < U * pp.nax_max; i += blockDim.x) lacc[i] = 0.f;
+  const int nch = (it.ncols + pp.K - 1) / pp.K;
+  for (int c = 0; c < nch; ++c) {
+    const int c0 = c * pp.K, kc = min(pp.K, it.ncols - c0);
+    __syncthreads();  // previous chunk done (and the line set-up / zeroing visible)
+    chunk_columns(p, pp, it, c0, kc, colbase);
+    __syncthreads();
+    for (int ci = warp; ci < kc; ci += kPathWarps) {
+      const int b = colbase[ci];
+      float* dst = cols + ci * nz;
+      if (b >= 0) {
+        for (int z = lane; z < nz; z += 32) cp_async4(dst + z, img + b + z);
+      } else {
+        for (int z = lane; z < nz; z += 32) dst[z] = 0.f;
+      }
+    }
+    cp_async_wait();
+    __syncthreads();
+    for (int u = warp; u < U; u += kPathWarps) {
+      const int l = u >> lgP, part = u & (P - 1);
+      const PathLineSmem L = ls[l];
+      if (!L.active) continue;
+      int e0, e1;
+      unit_range(pp, L, c, part, lgP, e0, e1);
+      if (e0 >= e1) continue;
+      const PathElem* E = pp.elems + L.elem_off;
+      float* acc_row = lacc + u * pp.nax_max;
+      for (int a0 = 0; a0 < L.nax; a0 += 128) {
+        const int nact = min(L.nax - a0, 128);
+        switch ((nact + 31) >> 5) {
+          case 1: gather_pass<NPA, 1>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
+          case 2: gather_pass<NPA, 2>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
+          case 3: gather_pass<NPA, 3>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
+          default: gather_pass<NPA, 4>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // the parts of each line, added in order, through the epilogue
+  for (int l = warp; l < nl; l += kPathWarps) {
+    const PathLineSmem L = ls[l];
+    if (!L.active) continue;
+    for (int a = lane; a < L.nax; a += 32) {
+      float v = 0.f;
+      for (int q = 0; q < P; ++q) v += lacc[(l * P + q) * pp.nax_max + a];
+      forward_store<EPI>(p, L.seg, L.view, L.tofi, L.nax, L.out_base + a, a, v, out, ep, ll, ncancel);
+    }
+  }
+}
+
+// Back projection as a gather over the voxels of each column: image[col][z] += the sum, over the path's
+// elements e in the column and the item's lines l of e's basic bin, of w_e * d_l[a] with z = zt + npa a.
+// A warp owns a column at a time (the path's elements are also stored in column order) and its lanes the
+// planes z; the sums stay in registers (no shared-memory atomics, a fixed order within the item) and
+// are added to the image once per column and item.  Each line's data is kept in shared memory padded
+// with zeros, so that every lane reads d at F + z - zt without range tests.
+struct FloatCols {
+  using T = float;
+  float* img;
+  __device__ __forceinline__ void load() {}
+  __device__ __forceinline__ T term(float v) const { return v; }
+  __device__ __forceinline__ void flush(int64_t i, float v) const {
+    if (v != 0.f) atomicAdd(img + i, v);
+  }
+};
+struct FixedCols {
+  using T = long long;
+  unsigned long long* acc;
+  const double* scale_ptr;  // 2^k of the fixed-point format, computed on the device
+  double scale;
+  __device__ __forceinline__ void load() { scale = *scale_ptr; }
+  // the same rounding of each contribution as the per-basic-bin fixed-point kernel
+  __device__ __forceinline__ T term(float v) const { return __double2ll_rn(static_cast<double>(v) * scale); }
+  __device__ __forceinline__ void flush(int64_t i, long long v) const {
+    if (v != 0) atomicAdd(acc + i, static_cast<unsigned long long>(v));
+  }
+};
+
+// planes [zp, zp + 128) of one column: elements [k0, k1) of the path in column order
+template <typename Cols>
+__device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int k0, int k1, const int4* lz,
+                                            const int2* members, const float* dl, int zp, int nz, int lane, int b,
+                                            const Cols& acc) {
+  typename Cols::T sum[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) sum[j] = typename Cols::T(0);
+  for (int kb = k0; kb < k1; kb += 32) {
+    PathCElem mine{0u, 0.f};
+    if (kb + lane < k1) mine = E[kb + lane];
+    const int cnt = min(32, k1 - kb);
+    for (int i = 0; i < cnt; ++i) {
+      const uint32_t mz = __shfl_sync(0xffffffffu, mine.mz, i);
+      const float v = __shfl_sync(0xffffffffu, mine.v, i);
+      const int zr = static_cast<int>(mz & 0xffffu);
+      const int2 mem = members[mz >> 16];  // (first line, number of lines) of the element's basic bin
+      for (int l = mem.x; l < mem.x + mem.y; ++l) {
+        const int4 L = lz[l];  // (z sign, z offset, window length, data offset)
+        int zt = L.x * zr + L.y;
+        // a window that misses the image (or an inactive line) reads the zero padding [0, F)
+        if (!(zt < nz && zt + L.z >= 0)) zt = zp + 128 + nz;
+        const float* q = dl + (L.w + zp + lane - zt);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sum[j] += acc.term(v * q[32 * j]);
+      }
+    }
+  }
+  if (b < 0) return;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int z = zp + 32 * j + lane;
+    if (z < nz) acc.flush(static_cast<int64_t>(b) + z, sum[j]);
+  }
+}
+
+template <typename Cols>
+__device__ __forceinline__ void back_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+                                               unsigned char* smem, const float* __restrict__ pd, const Cols& acc,
+                                               int zero_ends) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nz = p.nz;
+  const PathSmemBack lay = path_smem_back(nz, pp.max_lines, pp.max_members, pp.nax_max, pp.npa_max);
+  const int dl_len = path_dl_len(nz, pp.nax_max, pp.npa_max), front = path_dl_front(nz);
+  PathLineSmem* ls = reinterpret_cast<PathLineSmem*>(smem + lay.lines);
+  int4* lz = reinterpret_cast<int4*>(smem + lay.lz);
+  int2* members = reinterpret_cast<int2*>(smem + lay.members);
+  float* dl = reinterpret_cast<float*>(smem + lay.dl);
+  const int nl = it.num_lines;
+  setup_path_lines(p, pp, it, ls);
+  for (int m = threadIdx.x; m < pp.max_members; m += blockDim.x) members[m] = make_int2(0, 0);
+  __syncthreads();
+  if (threadIdx.x == 0) {  // the lines of one member are consecutive
+    for (int l = 0; l < nl; ++l) {
+      int2& m = members[ls[l].member];
+      if (m.y == 0) m.x = l;
+      ++m.y;
+    }
+  }
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+    const PathLineSmem& L = ls[l];
+    // an inactive line gets an empty window (zt + window < 0 for every zt < nz)
+    lz[l] = make_int4(L.zsign, L.zadd, L.active ? (L.nax - 1) * L.npa : -(1 << 30), l * dl_len + front);
+  }
+  // padded line data: dl[l][front + a npa] = d(a), zero elsewhere and for skipped bins
+  for (int l = warp; l < nl; l += kPathWarps) {
+    const PathLineSmem L = ls[l];
+    for (int t = lane; t < dl_len; t += 32) {
+      const int r = t - front;
+      float d = 0.f;
+      if (L.active && r >= 0 && r % L.npa == 0) {
+        const int a = r / L.npa;
+        if (a < L.nax && !(zero_ends && L.seg == 0 && (a == 0 || a == L.nax - 1)))
+          d = pd ? __ldg(pd + L.out_base + a) : 1.f;  // pd == nullptr back-projects ones
+      }
+      dl[l * dl_len + t] = d;
+    }
+  }
+  __syncthreads();
+  const int swap = it.flags & 1;
+  const int sx = (it.flags & 2) ? -1 : 1;
+  const int sy = (it.flags & 4) ? -1 : 1;
+  const PathCElem* E = pp.cmaj + it.cmaj_off;
+  const int* cs = pp.col_starts + it.col_starts;
+  for (int ci = warp; ci < it.ncols; ci += kPathWarps) {
+    const uint32_t pk = pp.cols[it.col_offset + ci];
+    const int x = static_cast<int>(pk & 2047u) - 1024;
+    const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
+    const int xi = (swap ? y : x) * sx - p.min_x;
+    const int yi = (swap ? x : y) * sy - p.min_y;
+    const int b = (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * nz : -1;
+    const int k0 = __ldg(cs + ci), k1 = __ldg(cs + ci + 1);
+    for (int zp = 0; zp < nz; zp += 128) back_column<Cols>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+  }
+}
+
+template <int NPA, int EPI>
+__global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
+    forward_paths_kernel(ProjParams p, PathParams pp, const int* __restrict__ list, const float* __restrict__ img,
+                         float* __restrict__ out, FwdEpilogue ep) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const PathItemDev it = pp.items[list[blockIdx.x]];
+  double ll = 0.0;
+  unsigned ncancel = 0;
+  forward_path_item<NPA, EPI>(p, pp, it, smem, img, out, ep, ll, ncancel);
+  if (EPI == kEpiRatio || EPI == kEpiGradient) {
+    // cancelled singularities (distributable.cxx:590-594)
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if ((threadIdx.x & 31) == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
+  }
+}
+
+template <typename Cols>
+__global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
+    back_paths_kernel(ProjParams p, PathParams pp, const int* __restrict__ list, const float* __restrict__ pd, Cols acc,
+                      int zero_ends) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const PathItemDev it = pp.items[list[blockIdx.x]];
+  Cols a = acc;
+  a.load();
+  back_path_item<Cols>(p, pp, it, smem, pd, a, zero_ends);
+}
+
+// ---- batched reconstructions: a persistent grid over (frame, path item) work items ----------------
+// The current item's frame, geometry (projector and path tables) and path item, copied to shared memory
+// by the CTA so that the loops read them like kernel parameters.
+struct BatchPathStage {
+  ProjParams p;
+  PathParams pp;
+  BatchFrameDev f;
+  PathItemDev it;
+};
+static_assert(sizeof(ProjParams) % 4 == 0 && sizeof(PathParams) % 4 == 0 && sizeof(BatchFrameDev) % 4 == 0 &&
+                  sizeof(PathItemDev) % 4 == 0,
+              "staged structures are copied as 32-bit words");
+
+__device__ __forceinline__ bool next_path_item(unsigned* counter, const BatchItem* __restrict__ items, int nitems,
+                                               const ProjParams* __restrict__ geoms,
+                                               const PathParams* __restrict__ pgeoms,
+                                               const BatchFrameDev* __restrict__ frames, BatchPathStage& st) {
+  __shared__ int s_item;
+  __syncthreads();  // every thread has finished with the previous item
+  if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(counter, 1u));
+  __syncthreads();
+  const int it = s_item;
+  if (it >= nitems) return false;
+  const BatchItem wi = items[it];
+  const int g = frames[wi.frame].geom;
+  constexpr int nf = sizeof(BatchFrameDev) / 4, np = sizeof(ProjParams) / 4, npp = sizeof(PathParams) / 4,
+                ni = sizeof(PathItemDev) / 4;
+  static_assert(nf + np + npp + ni <= kPathThreads, "one word per thread");
+  const int t = threadIdx.x;
+  if (t < nf) {
+    reinterpret_cast<uint32_t*>(&st.f)[t] = reinterpret_cast<const uint32_t*>(frames + wi.frame)[t];
+  } else if (t < nf + np) {
+    reinterpret_cast<uint32_t*>(&st.p)[t - nf] = reinterpret_cast<const uint32_t*>(geoms + g)[t - nf];
+  } else if (t < nf + np + npp) {
+    reinterpret_cast<uint32_t*>(&st.pp)[t - nf - np] = reinterpret_cast<const uint32_t*>(pgeoms + g)[t - nf - np];
+  } else if (t < nf + np + npp + ni) {
+    reinterpret_cast<uint32_t*>(&st.it)[t - nf - np - npp] =
+        reinterpret_cast<const uint32_t*>(pgeoms[g].items + wi.bin)[t - nf - np - npp];
+  }
+  __syncthreads();
+  return true;
+}
+
+template <int NPA>
+__global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
+    forward_batch_paths_kernel(const ProjParams* __restrict__ geoms, const PathParams* __restrict__ pgeoms,
+                               const BatchFrameDev* __restrict__ frames, const BatchItem* __restrict__ items, int nitems,
+                               unsigned* counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BatchPathStage st;
+  while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st)) {
+    double ll = 0.0;
+    unsigned ncancel = 0;
+    forward_path_item<NPA, kEpiRatio>(st.p, st.pp, st.it, smem, st.f.x, st.f.ratio, st.f.ep, ll, ncancel);
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if ((threadIdx.x & 31) == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
+  }
+}
+
+__global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
+    back_batch_paths_kernel(const ProjParams* __restrict__ geoms, const PathParams* __restrict__ pgeoms,
+                            const BatchFrameDev* __restrict__ frames, const BatchItem* __restrict__ items, int nitems,
+                            unsigned* counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BatchPathStage st;
+  while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st))
+    back_path_item<FloatCols>(st.p, st.pp, st.it, smem, st.f.ratio, FloatCols{st.f.u}, 0);
+}
+
+const void* forward_batch_paths_fn(int npa) {
+  return npa == 1 ? reinterpret_cast<const void*>(forward_batch_paths_kernel<1>)
+       : npa == 2 ? reinterpret_cast<const void*>(forward_batch_paths_kernel<2>)
+                  : reinterpret_cast<const void*>(forward_batch_paths_kernel<0>);
+}
+
+cudaError_t prepare_path_smem(const void* fn, int bytes) {
+  if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return cudaSuccess;
+}
+
+template <typename K, typename... A>
+cudaError_t launch_path(K kernel, int nitems, int smem_bytes, cudaStream_t st, A... args) {
+  if (nitems <= 0) return cudaSuccess;
+  cudaError_t e = prepare_path_smem(reinterpret_cast<const void*>(kernel), smem_bytes);
+  if (e != cudaSuccess) return e;
+  kernel<<<nitems, kPathThreads, smem_bytes, st>>>(args...);
+  return cudaGetLastError();
+}
+
+template <int EPI>
+cudaError_t launch_forward_paths_epi(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* image,
+                                     float* out, cudaStream_t st, const FwdEpilogue& ep) {
+  const int sm = path_smem_fwd(pp.K, p.nz, pp.max_lines, pp.nax_max, pp.npa_max).total;
+  switch (p.uniform_npa) {
+    case 1: return launch_path(forward_paths_kernel<1, EPI>, n, sm, st, p, pp, list, image, out, ep);
+    case 2: return launch_path(forward_paths_kernel<2, EPI>, n, sm, st, p, pp, list, image, out, ep);
+    default: return launch_path(forward_paths_kernel<0, EPI>, n, sm, st, p, pp, list, image, out, ep);
+  }
+}
+
+template <typename Cols>
+cudaError_t launch_back_paths(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* pd,
+                              const Cols& acc, cudaStream_t st, int zero_ends) {
+  const int sm = path_smem_back(p.nz, pp.max_lines, pp.max_members, pp.nax_max, pp.npa_max).total;
+  return launch_path(back_paths_kernel<Cols>, n, sm, st, p, pp, list, pd, acc, zero_ends);
+}
+
+}  // namespace
+
+cudaError_t launch_forward_paths(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                 const float* image, float* projdata, cudaStream_t st, const FwdEpilogue* ep) {
+  FwdEpilogue e{};
+  if (ep) e = *ep;
+  switch (e.mode) {
+    case kEpiNone: return launch_forward_paths_epi<kEpiNone>(p, pp, items, nitems, image, projdata, st, e);
+    case kEpiRatio: return launch_forward_paths_epi<kEpiRatio>(p, pp, items, nitems, image, projdata, st, e);
+    case kEpiGradient: return launch_forward_paths_epi<kEpiGradient>(p, pp, items, nitems, image, projdata, st, e);
+    default: return cudaErrorInvalidValue;  // the log-likelihood keeps the per-basic-bin kernel
+  }
+}
+
+cudaError_t launch_forward_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int npa, int smem_bytes,
+                                       const BatchFrameDev* frames, const BatchItem* items, int nitems, unsigned* counter,
+                                       int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  cudaError_t e = prepare_path_smem(forward_batch_paths_fn(npa), smem_bytes);
+  if (e != cudaSuccess) return e;
+  if (npa == 1)
+    forward_batch_paths_kernel<1><<<grid, kPathThreads, smem_bytes, st>>>(geoms, pgeoms, frames, items, nitems, counter);
+  else if (npa == 2)
+    forward_batch_paths_kernel<2><<<grid, kPathThreads, smem_bytes, st>>>(geoms, pgeoms, frames, items, nitems, counter);
+  else
+    forward_batch_paths_kernel<0><<<grid, kPathThreads, smem_bytes, st>>>(geoms, pgeoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int smem_bytes,
+                                    const BatchFrameDev* frames, const BatchItem* items, int nitems, unsigned* counter,
+                                    int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  cudaError_t e = prepare_path_smem(reinterpret_cast<const void*>(back_batch_paths_kernel), smem_bytes);
+  if (e != cudaSuccess) return e;
+  back_batch_paths_kernel<<<grid, kPathThreads, smem_bytes, st>>>(geoms, pgeoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+int batch_paths_max_ctas_per_sm(int npa, int smem_bytes, bool forward) {
+  const void* fn = forward ? forward_batch_paths_fn(npa) : reinterpret_cast<const void*>(back_batch_paths_kernel);
+  if (prepare_path_smem(fn, smem_bytes) != cudaSuccess) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kPathThreads, smem_bytes) != cudaSuccess) return 0;
+  return n;
+}
+
+cudaError_t launch_back_paths_atomic(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                     const float* projdata, float* image, cudaStream_t st, int zero_ends) {
+  return launch_back_paths(p, pp, items, nitems, projdata, FloatCols{image}, st, zero_ends);
+}
+
+cudaError_t launch_back_paths_fixed(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                    const float* projdata, unsigned long long* acc, const double* scale,
+                                    cudaStream_t st, int zero_ends) {
+  return launch_back_paths(p, pp, items, nitems, projdata, FixedCols{acc, scale, 0.0}, st, zero_ends);
+}
+
+}  // namespace b200

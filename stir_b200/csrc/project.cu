@@ -17,6 +17,7 @@
 // Back:    image[col_k][z_k + npa*a] += w_k * projdata[line][a] for projdata != 0
 //          (ProjMatrixElemsForOneBin::back_project, :333-351), with float atomics.
 #include "internal.hpp"
+#include "epilogue.cuh"
 
 namespace b200 {
 
@@ -131,41 +132,7 @@ __device__ __forceinline__ void forward_pass(const ProjParams& p, const RowElem*
   for (int j = 0; j < NJ; ++j)
     if (act[j]) {
       const int a = a0 + j * 32 + lane;
-      const int64_t idx = s.out_base + a;
-      if (EPI == kEpiNone) {
-        out[idx] = acc[j];
-      } else {
-        // segment 0 end planes zeroed (distributable.cxx:146-158,216-221)
-        const bool zend = ep.zero_ends && L.seg == 0 && (a == 0 || a == s.nax - 1);
-        const float y = zend ? 0.f : __ldg(ep.y + idx);
-        const float av = (ep.add && !zend) ? __ldg(ep.add + idx) : 0.f;
-        const float sv = ep.small_value[(s.tofi * (2 * p.S + 1) + L.seg + p.S) * p.num_views + L.view];
-        if (EPI == kEpiRatio || EPI == kEpiGradient) {
-          // divide_and_truncate (recon_array_functions.cxx:171-266) of y by A x + a
-          const float den = acc[j] + av;
-          float r;
-          if (y <= sv) {
-            r = 0.f;
-          } else if (y > 10000.F * den) {
-            r = 10000.F;
-            ++ncancel;
-          } else {
-            r = y / den;
-          }
-          if (EPI == kEpiGradient) r -= zend ? 0.f : (ep.mult ? __ldg(ep.mult + idx) : 1.f);
-          out[idx] = r;
-        } else {
-          // accumulate_loglikelihood (recon_array_functions.cxx:335-377) of ybar = (A x + a) * m
-          float e = acc[j] + av;
-          if (zend)
-            e *= 0.f;
-          else if (ep.mult)
-            e *= __ldg(ep.mult + idx);
-          const float ne = fmaxf(e, y / 10000.F);
-          ll += (y <= sv) ? -static_cast<double>(ne) : y * log(static_cast<double>(ne)) - static_cast<double>(ne);
-          if (out) out[idx] = e;
-        }
-      }
+      forward_store<EPI>(p, L.seg, L.view, s.tofi, s.nax, s.out_base + a, a, acc[j], out, ep, ll, ncancel);
     }
 }
 

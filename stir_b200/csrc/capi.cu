@@ -255,7 +255,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   std::vector<PathLineDev> plines;
   std::vector<PathItemDev> items;
   std::vector<int> item_view;
-  int max_lines = 1;
+  int max_lines = 1, max_acc = 1;
   for (int gi = 0; gi < ngroups; ++gi) {
     const Group& G = groups[gi];
     const int vi = gi / ntangs, ti = gi % ntangs;
@@ -294,6 +294,9 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
       it.num_lines = static_cast<int>(plines.size()) - it.first_line;
       if (it.num_lines == 0) continue;
       max_lines = std::max(max_lines, it.num_lines);
+      int nax_sum = 0;
+      for (int l = it.first_line; l < it.first_line + it.num_lines; ++l) nax_sum += g.nax(lines[plines[l].line].seg);
+      max_acc = std::max(max_acc, path_parts(it.num_lines) * nax_sum);
       items.push_back(it);
       item_view.push_back(bviews[vi]);
     }
@@ -308,7 +311,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
       const int c1 = m + 1 < G.member_chunk.size() ? G.member_chunk[m + 1] : static_cast<int>(G.chunks.size());
       for (int c = G.member_chunk[m]; c + 1 < c1; ++c) max_chunk = std::max(max_chunk, G.chunks[c + 1] - G.chunks[c]);
     }
-  if (path_smem_fwd(K, nz, max_lines, nax_max, npa_max).total > 200 * 1024 ||
+  if (path_smem_fwd(K, nz, max_lines, max_acc, npa_max).total > 200 * 1024 ||
       path_smem_back(nz, max_lines, nsegs, nax_max, npa_max).total > 200 * 1024)
     return;
 
@@ -334,6 +337,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   pp.cmaj = h.path_cmaj.p;
   pp.col_starts = h.path_col_starts.p;
   pp.max_members = nsegs;
+  pp.max_acc = max_acc;
   h.h_item_view = item_view;
   h.h_path_items = items;
   h.use_paths = true;
@@ -1529,7 +1533,7 @@ void batch_finalize(b200rt_batch& b) {
     for (auto* h : b.geoms) {
       const b200::PathParams& pp = h->pparams;
       pg.push_back(pp);
-      b.smem_f = std::max(b.smem_f, b200::path_smem_fwd(pp.K, h->params.nz, pp.max_lines, pp.nax_max, pp.npa_max).total);
+      b.smem_f = std::max(b.smem_f, b200::path_smem_fwd(pp.K, h->params.nz, pp.max_lines, pp.max_acc, pp.npa_max).total);
       b.smem_b = std::max(b.smem_b, b200::path_smem_back(h->params.nz, pp.max_lines, pp.max_members, pp.nax_max,
                                                           pp.npa_max).total);
     }

@@ -162,10 +162,12 @@ struct PathParams {
   const PathCElem* cmaj;  // every path's elements ordered by column, then member, then z
   const int* col_starts;  // per path: first element of each column in cmaj (relative), ncols + 1 entries
   int max_members;        // basic bins per path (basic segments)
+  int max_acc;            // forward accumulators of the largest item: path_parts(lines) x sum of the lines' nax
 };
 
-// parts each line's elements are split into (forward), so that an item's lines keep all warps busy
-__host__ __device__ inline int path_parts(int num_lines) { return num_lines >= 8 ? 2 : (num_lines >= 4 ? 4 : 8); }
+// parts each line's elements are split into (forward): an item's lines are processed in pairs (the two
+// z orientations of a basic bin), so (pairs x parts) units keep the 8 warps of a CTA busy
+__host__ __device__ inline int path_parts(int num_lines) { return num_lines >= 8 ? 4 : 8; }
 
 struct PathLineSmem {
   int64_t out_base;  // device-layout projection index of (line, axial 0)
@@ -177,12 +179,12 @@ struct PathLineSmem {
   int active;       // tangential position inside the projection data
   int member;
 };
-// a row element of one line and one pass, in shared memory (forward)
+// a row element of one or two lines and one pass, in shared memory (forward)
 struct __align__(16) PathXElem {
-  int base;  // staged-column index of axial position 0
-  int zt;    // image z of axial position 0
+  int base;  // staged index of axial position 0, line 1
+  int zt;    // staged index of axial position 0, line 2
   float v;
-  int full;  // z stays inside the image for every lane of the pass
+  int full;  // column slot in the chunk (bits 0..15); bit 30: z stays inside the image for every lane
 };
 constexpr int kPathWarpsH = 8;
 
@@ -195,20 +197,21 @@ __host__ __device__ inline int path_dl_len(int nz, int nax_max, int npa_max) {
   return (2 * nz + 256 + (nax_max - 1) * npa_max + 3) & ~3;
 }
 
-// dynamic shared memory of a forward path CTA: staged columns, their image offsets, line set-up,
-// per-warp element buffers, per (line, part) accumulators
+// dynamic shared memory of a forward path CTA: staged columns, their image offsets, line set-up, line
+// pairs and accumulator offsets, per-warp element buffers, per (line, part) accumulators (max_acc floats:
+// the most, over the items, of path_parts(lines) x the lines' axial positions)
 struct PathSmemFwd {
-  int colbase, lines, xbuf, acc, total;
+  int colbase, lines, pairs, rowoff, xbuf, acc, total;
 };
-__host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int max_lines, int nax_max, int npa_max) {
+__host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int max_lines, int max_acc, int npa_max) {
   PathSmemFwd s;
   s.colbase = path_align16((K * nz + 128 * npa_max) * 4);  // staged columns and a pass's overshoot
   s.lines = path_align16(s.colbase + K * 4);
-  s.xbuf = path_align16(s.lines + max_lines * static_cast<int>(sizeof(PathLineSmem)));
+  s.pairs = path_align16(s.lines + max_lines * static_cast<int>(sizeof(PathLineSmem)));
+  s.rowoff = path_align16(s.pairs + max_lines * 8);
+  s.xbuf = path_align16(s.rowoff + max_lines * 4);
   s.acc = s.xbuf + kPathWarpsH * 32 * static_cast<int>(sizeof(PathXElem));
-  int acc_rows = 0;  // the most (line, part) pairs of any item
-  for (int n = 1; n <= max_lines; ++n) acc_rows = acc_rows > n * path_parts(n) ? acc_rows : n * path_parts(n);
-  s.total = path_align16(s.acc + acc_rows * nax_max * 4);
+  s.total = path_align16(s.acc + max_acc * 4);
   return s;
 }
 // back path CTA: line set-up, per line (z sign, z offset, window length, data offset), per member its

@@ -102,54 +102,91 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_al
 // One pass of one unit over elements [e0, e1) of its row: NJ groups of 32 axial positions from a0.
 // The warp's lanes transform 32 elements at a time (column slot -> staged index, z reflection) into
 // the warp's buffer; then every element costs one broadcast read and NJ shared loads and FMAs.
-template <int NPA, int NJ>
+template <int NPA, int NJ, bool TWO>
 __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int e0, int e1, int c0, const float* cols,
-                                            int nz, const PathLineSmem& L, int a0, int nact, int lane, float* acc_row,
-                                            PathXElem* xb) {
-  const int npa = NPA ? NPA : L.npa;
+                                            int nz, const PathLineSmem& L1, const PathLineSmem& L2, int a0, int nact,
+                                            int lane, float* acc_row1, float* acc_row2, PathXElem* xb) {
+  const int npa = NPA ? NPA : L1.npa;
   // lane's plane offset of group j: zo0 + 32 j npa.  In the full path inactive lanes (axial positions past
-  // the line's end) read up to 127 npa floats past the staged columns, into the zero-cost padding of the
-  // staging buffer, and their sums are dropped: the full path needs no per-lane tests.
+  // the line's end) read up to 127 npa floats past the staged columns, into the padding of the staging
+  // buffer, and their sums are dropped: the full path needs no per-lane tests.
   const int zo0 = (a0 + lane) * npa;
   bool act[NJ];
-  float acc[NJ];
+  float acc1[NJ], acc2[NJ];
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
     act[j] = j * 32 + lane < nact;
-    acc[j] = act[j] ? acc_row[a0 + j * 32 + lane] : 0.f;
+    acc1[j] = act[j] ? acc_row1[a0 + j * 32 + lane] : 0.f;
+    acc2[j] = (TWO && act[j]) ? acc_row2[a0 + j * 32 + lane] : 0.f;
   }
   const int zlo = a0 * npa, zhi = (a0 + nact - 1) * npa;
   for (int k0 = e0; k0 < e1; k0 += 32) {
     const int cnt = min(32, e1 - k0);
     __syncwarp();
     if (lane < cnt) {
+      // x = (staged index of axial position 0 for line 1, for line 2, value, column slot | full flags)
       const PathElem m = E[k0 + lane];
+      const int zr = static_cast<int>(m.sz >> 16);
+      const int sl = static_cast<int>(m.sz & 0xffffu) - c0;
+      const int zt1 = L1.zsign * zr + L1.zadd;
+      const int zt2 = TWO ? L2.zsign * zr + L2.zadd : 0;
+      const int f1 = (zt1 + zlo >= 0) && (zt1 + zhi < nz);
+      const int f2 = TWO ? ((zt2 + zlo >= 0) && (zt2 + zhi < nz)) : 1;
       PathXElem x;
-      x.zt = L.zsign * static_cast<int>(m.sz >> 16) + L.zadd;
-      x.base = (static_cast<int>(m.sz & 0xffffu) - c0) * nz + x.zt;
+      x.base = sl * nz + zt1;
+      x.zt = sl * nz + zt2;
       x.v = m.v;
-      x.full = (x.zt + zlo >= 0) && (x.zt + zhi < nz);
+      x.full = sl | ((f1 & f2) << 30);
       xb[lane] = x;
     }
     __syncwarp();
     for (int i = 0; i < cnt; ++i) {
       const PathXElem e = xb[i];
-      const float* q = cols + (e.base + zo0);
-      if (e.full) {
-#pragma unroll
-        for (int j = 0; j < NJ; ++j) acc[j] += q[j * 32 * npa] * e.v;
-      } else {
+      const float* q1 = cols + (e.base + zo0);
+      const float* q2 = cols + (e.zt + zo0);
+      if (e.full >> 30) {
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
-          const int zz = e.zt + zo0 + j * 32 * npa;
-          if (act[j] && static_cast<unsigned>(zz) < static_cast<unsigned>(nz)) acc[j] += q[j * 32 * npa] * e.v;
+          acc1[j] += q1[j * 32 * npa] * e.v;
+          if (TWO) acc2[j] += q2[j * 32 * npa] * e.v;
+        }
+      } else {
+        const int sb = (e.full & 0xffff) * nz;  // column start in the staging buffer
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const int zz1 = e.base - sb + zo0 + j * 32 * npa;
+          if (act[j] && static_cast<unsigned>(zz1) < static_cast<unsigned>(nz)) acc1[j] += q1[j * 32 * npa] * e.v;
+          if (TWO) {
+            const int zz2 = e.zt - sb + zo0 + j * 32 * npa;
+            if (act[j] && static_cast<unsigned>(zz2) < static_cast<unsigned>(nz)) acc2[j] += q2[j * 32 * npa] * e.v;
+          }
         }
       }
     }
   }
 #pragma unroll
   for (int j = 0; j < NJ; ++j)
-    if (act[j]) acc_row[a0 + j * 32 + lane] = acc[j];
+    if (act[j]) {
+      acc_row1[a0 + j * 32 + lane] = acc1[j];
+      if (TWO) acc_row2[a0 + j * 32 + lane] = acc2[j];
+    }
+}
+
+// the lines of an item processed together: consecutive active lines of one basic bin (its two z
+// orientations), in pairs, and the remaining active lines alone (thread 0; lines of a bin are consecutive)
+__device__ __forceinline__ int pair_lines(const PathLineSmem* ls, int nl, int2* pairs) {
+  int n = 0;
+  for (int l = 0; l < nl; ++l) {
+    if (!ls[l].active) continue;
+    if (l + 1 < nl && ls[l + 1].active && ls[l + 1].member == ls[l].member && ls[l + 1].nax == ls[l].nax &&
+        ls[l + 1].npa == ls[l].npa) {
+      pairs[n++] = make_int2(l, l + 1);
+      ++l;
+    } else {
+      pairs[n++] = make_int2(l, -1);
+    }
+  }
+  return n;
 }
 
 template <int NPA, int EPI>
@@ -159,19 +196,36 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
                                                   unsigned& ncancel) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nz = p.nz;
-  const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.max_lines, pp.nax_max, pp.npa_max);
+  const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.max_lines, pp.max_acc, pp.npa_max);
   float* cols = reinterpret_cast<float*>(smem);
   int* colbase = reinterpret_cast<int*>(smem + lay.colbase);
   PathLineSmem* ls = reinterpret_cast<PathLineSmem*>(smem + lay.lines);
+  int2* pairs = reinterpret_cast<int2*>(smem + lay.pairs);
+  int* rowoff = reinterpret_cast<int*>(smem + lay.rowoff);
   PathXElem* xb = reinterpret_cast<PathXElem*>(smem + lay.xbuf) + warp * 32;
   float* lacc = reinterpret_cast<float*>(smem + lay.acc);
-  const int nl = it.num_lines, P = path_parts(nl), lgP = log2_parts(P), U = nl * P;
+  __shared__ int s_npairs, s_nacc;
+  const int nl = it.num_lines;
+  // units: (pair of lines, part of the elements); the accumulators are per (line, part): nax floats each
+  const int P = path_parts(nl), lgP = log2_parts(P);
   setup_path_lines(p, pp, it, ls);
-  for (int i = threadIdx.x; i < U * pp.nax_max; i += blockDim.x) lacc[i] = 0.f;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_npairs = pair_lines(ls, nl, pairs);
+    int o = 0;
+    for (int l = 0; l < nl; ++l) {
+      rowoff[l] = o;
+      o += P * ls[l].nax;
+    }
+    s_nacc = o;
+  }
+  __syncthreads();
+  const int U = s_npairs * P;
+  for (int i = threadIdx.x; i < s_nacc; i += blockDim.x) lacc[i] = 0.f;
   const int nch = (it.ncols + pp.K - 1) / pp.K;
   for (int c = 0; c < nch; ++c) {
     const int c0 = c * pp.K, kc = min(pp.K, it.ncols - c0);
-    __syncthreads();  // previous chunk done (and the line set-up / zeroing visible)
+    __syncthreads();  // previous chunk done (and the zeroing visible)
     chunk_columns(p, pp, it, c0, kc, colbase);
     __syncthreads();
     for (int ci = warp; ci < kc; ci += kPathWarps) {
@@ -186,21 +240,35 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
     cp_async_wait();
     __syncthreads();
     for (int u = warp; u < U; u += kPathWarps) {
-      const int l = u >> lgP, part = u & (P - 1);
-      const PathLineSmem L = ls[l];
-      if (!L.active) continue;
+      const int pr = u >> lgP, part = u & (P - 1);
+      const int2 pl = pairs[pr];
+      const PathLineSmem L1 = ls[pl.x];
       int e0, e1;
-      unit_range(pp, L, c, part, lgP, e0, e1);
+      unit_range(pp, L1, c, part, lgP, e0, e1);
       if (e0 >= e1) continue;
-      const PathElem* E = pp.elems + L.elem_off;
-      float* acc_row = lacc + u * pp.nax_max;
-      for (int a0 = 0; a0 < L.nax; a0 += 128) {
-        const int nact = min(L.nax - a0, 128);
-        switch ((nact + 31) >> 5) {
-          case 1: gather_pass<NPA, 1>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
-          case 2: gather_pass<NPA, 2>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
-          case 3: gather_pass<NPA, 3>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
-          default: gather_pass<NPA, 4>(E, e0, e1, c0, cols, nz, L, a0, nact, lane, acc_row, xb); break;
+      const PathElem* E = pp.elems + L1.elem_off;
+      float* row1 = lacc + rowoff[pl.x] + part * L1.nax;
+      if (pl.y >= 0) {
+        const PathLineSmem L2 = ls[pl.y];
+        float* row2 = lacc + rowoff[pl.y] + part * L2.nax;
+        for (int a0 = 0; a0 < L1.nax; a0 += 128) {
+          const int nact = min(L1.nax - a0, 128);
+          switch ((nact + 31) >> 5) {
+            case 1: gather_pass<NPA, 1, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            case 2: gather_pass<NPA, 2, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            case 3: gather_pass<NPA, 3, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            default: gather_pass<NPA, 4, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
+          }
+        }
+      } else {
+        for (int a0 = 0; a0 < L1.nax; a0 += 128) {
+          const int nact = min(L1.nax - a0, 128);
+          switch ((nact + 31) >> 5) {
+            case 1: gather_pass<NPA, 1, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            case 2: gather_pass<NPA, 2, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            case 3: gather_pass<NPA, 3, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            default: gather_pass<NPA, 4, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
+          }
         }
       }
     }
@@ -212,7 +280,7 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
     if (!L.active) continue;
     for (int a = lane; a < L.nax; a += 32) {
       float v = 0.f;
-      for (int q = 0; q < P; ++q) v += lacc[(l * P + q) * pp.nax_max + a];
+      for (int q = 0; q < P; ++q) v += lacc[rowoff[l] + q * L.nax + a];
       forward_store<EPI>(p, L.seg, L.view, L.tofi, L.nax, L.out_base + a, a, v, out, ep, ll, ncancel);
     }
   }
@@ -461,7 +529,7 @@ cudaError_t launch_path(K kernel, int nitems, int smem_bytes, cudaStream_t st, A
 template <int EPI>
 cudaError_t launch_forward_paths_epi(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* image,
                                      float* out, cudaStream_t st, const FwdEpilogue& ep) {
-  const int sm = path_smem_fwd(pp.K, p.nz, pp.max_lines, pp.nax_max, pp.npa_max).total;
+  const int sm = path_smem_fwd(pp.K, p.nz, pp.max_lines, pp.max_acc, pp.npa_max).total;
   switch (p.uniform_npa) {
     case 1: return launch_path(forward_paths_kernel<1, EPI>, n, sm, st, p, pp, list, image, out, ep);
     case 2: return launch_path(forward_paths_kernel<2, EPI>, n, sm, st, p, pp, list, image, out, ep);

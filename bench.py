@@ -191,7 +191,7 @@ def profile_traffic(kernel_name):
             txt = open(path).read()
         except OSError:
             continue
-        m = re.search(rf"^traffic_per_launch\\[{kernel_name}\\]:\\s*([0-9.eE+]+)", txt, re.M)
+        m = re.search(r"^traffic_per_launch\[" + re.escape(kernel_name) + r"\]:\s*([0-9.eE+]+)", txt, re.M)
         if m:
             return float(m.group(1))
     return None

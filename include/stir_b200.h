@@ -55,6 +55,11 @@ extern "C" {
 #define B200RT_BACKPROJECT_DETERMINISTIC 1 /* contributions summed as 64-bit fixed point: order-independent,
                                               bit-identical from run to run */
 
+/* attenuation modes (BinNormalisationFromAttenuationImage.cxx:138-170) */
+#define B200RT_ATTENUATION_FACTORS 0 /* projdata = undo of ones: 1 / exp(A mu), the multiplicative factors */
+#define B200RT_ATTENUATION_APPLY 1   /* projdata *= exp(A mu)   (apply: attenuation correction) */
+#define B200RT_ATTENUATION_UNDO 2    /* projdata /= exp(A mu)   (undo: attenuate) */
+
 /* priors (src/recon_buildblock/QuadraticPrior.cxx, RelativeDifferencePrior.cxx) */
 #define B200RT_PRIOR_NONE 0
 #define B200RT_PRIOR_QUADRATIC 1
@@ -263,6 +268,12 @@ int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const float* image_de
  * images in device layout. */
 int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, float* gradient_dev,
                               void* stream);
+
+/* BinNormalisationFromAttenuationImage on device-resident projection data (all bins, device layout):
+ * the line integrals A mu of the attenuation image mu_dev (device layout, 1/mm) by this projector, then
+ * `mode` (B200RT_ATTENUATION_*) with exp as STIR's in_place_exp.  Replaces set_up + apply/undo
+ * (src/recon_buildblock/BinNormalisationFromAttenuationImage.cxx:122-170); non-TOF only, as STIR. */
+int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* projdata_dev, int mode, void* stream);
 
 /* ---- projectors on host arrays in STIR order (copies included) ---------- */
 int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host,

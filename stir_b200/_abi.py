@@ -23,6 +23,9 @@ ERR_TOO_LARGE = -7
 BACKPROJECT_ATOMIC = 0
 BACKPROJECT_DETERMINISTIC = 1
 
+ATTENUATION_FACTORS = 0
+ATTENUATION_APPLY = 1
+ATTENUATION_UNDO = 2
 PRIOR_NONE = 0
 PRIOR_QUADRATIC = 1
 PRIOR_RELATIVE_DIFFERENCE = 2
@@ -151,6 +154,7 @@ EXPORTS = [
     ("b200rt_prior_gradient_dev", _I, [_P, ctypes.POINTER(Prior), _P, _P, _P]),
     ("b200rt_forward_project", _I, [_P, _P, _P, _I, _I]),
     ("b200rt_back_project", _I, [_P, _P, _P, _I, _I, _I]),
+    ("b200rt_attenuation_dev", _I, [_P, _P, _P, _I, _P]),
     ("b200rt_batch_create", _I, [_I, ctypes.POINTER(_P)]),
     ("b200rt_batch_destroy", None, [_P]),
     ("b200rt_batch_last_error", ctypes.c_char_p, [_P]),

@@ -1319,6 +1319,29 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
   }
 }
 
+int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* projdata_dev, int mode, void* stream) {
+  if (!h || !mu_dev || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (mode < B200RT_ATTENUATION_FACTORS || mode > B200RT_ATTENUATION_UNDO)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown attenuation mode");
+  if (h->geo->num_tof() > 1)
+    return fail(h, B200RT_ERR_UNSUPPORTED,
+                "BinNormalisationFromAttenuationImage limitation: currently can only handle non_TOF data.");
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Geometry& g = *h->geo;
+    if (!h->ratio.p) {
+      h->ratio.alloc(g.projdata_size());
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+    }
+    forward_subset(*h, mu_dev, h->ratio.p, 0, 1, st);
+    ck(launch_attenuation(h->ratio.p, projdata_dev, g.projdata_size(), mode, st), "attenuation");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
                            void* stream) {
   if (!h || !prior || !image_dev || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");

@@ -275,6 +275,7 @@ cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbin
 // max |projdata| (nullptr data = 1) and the fixed-point scale 2^floor(62 - log2(max|d| * colmax * 1.01)) (osem.cu)
 cudaError_t launch_fixed_scale(const float* projdata, int64_t n, const float* colmax, float* partial, double* scale,
                                cudaStream_t st);
+cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int64_t n, int mode, cudaStream_t st);
 cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* scale, float* image, int64_t n,
                                   cudaStream_t st);
 cudaError_t launch_max(const float* data, int64_t n, float* partial, float* out, cudaStream_t st);

@@ -299,6 +299,28 @@ cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* s
   return cudaGetLastError();
 }
 
+// BinNormalisationFromAttenuationImage (BinNormalisationFromAttenuationImage.cxx:138-170) given the line
+// integrals A mu: apply multiplies by exp(A mu), undo divides by it; factors = undo of ones
+__global__ void attenuation_kernel(const float* __restrict__ line_integrals, float* __restrict__ pd, int64_t n,
+                                   int mode) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float e = expf(line_integrals[i]);
+    if (mode == B200RT_ATTENUATION_FACTORS)
+      pd[i] = 1.F / e;
+    else if (mode == B200RT_ATTENUATION_APPLY)
+      pd[i] *= e;
+    else
+      pd[i] /= e;
+  }
+}
+
+cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int64_t n, int mode, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  attenuation_kernel<<<update_num_blocks(n), 256, 0, st>>>(line_integrals, projdata, n, mode);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
                                          float* out, cudaStream_t st) {

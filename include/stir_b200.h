@@ -275,6 +275,25 @@ int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, co
  * (src/recon_buildblock/BinNormalisationFromAttenuationImage.cxx:122-170); non-TOF only, as STIR. */
 int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* projdata_dev, int mode, void* stream);
 
+/* ---- OSSPS (src/iterative/OSSPS/OSSPSReconstruction.cxx) on device-resident data ---- */
+/* precompute_denominator_of_conditioner_without_penalty (OSSPSReconstruction.cxx:184-221): minus the
+ * approximate Hessian of the log-likelihood times ones, A^T divide_and_truncate(A 1, (y n) n) over all bins
+ * (...AndProjData.cxx:955-1064), n = the normalisation's correction factors (NULL: none). */
+int b200rt_ossps_denominator_dev(b200rt_projector* h, const float* y_dev, const float* norm_dev, float* denominator_dev,
+                                 int back_projection_mode, void* stream);
+/* OSSPSReconstruction::update_estimate (OSSPSReconstruction.cxx:284-410) on estimate_dev: at the first
+ * sub-iteration (subiteration_num == start_subiteration_num) voxels with zero sensitivity (sens_dev: the total
+ * sensitivity) are zeroed and denominator_dev is completed with 2 x the Quadratic prior's parabolic surrogate
+ * curvature and thresholded to positive values, in place; then
+ *   x += relax * (num_subsets * (g - prior_gradient / num_subsets)) / denominator, clamped to [0, upper_bound],
+ * g = A_S^T [divide_and_truncate(y, A_S x + a) - m], relax = relaxation_parameter /
+ * (1 + relaxation_gamma * (subiteration_num / num_subsets)).  prior: NULL, none or Quadratic. */
+int b200rt_ossps_subiteration_dev(b200rt_projector* h, float* estimate_dev, float* denominator_dev, const float* y_dev,
+                                  const float* additive_dev, const float* mult_dev, const float* sens_dev,
+                                  int subset_num, int num_subsets, int subiteration_num, int start_subiteration_num,
+                                  int zero_seg0_end_planes, const b200rt_prior* prior, float relaxation_parameter,
+                                  float relaxation_gamma, float upper_bound, int back_projection_mode, void* stream);
+
 /* ---- projectors on host arrays in STIR order (copies included) ---------- */
 int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host,
                            int subset_num, int num_subsets);

@@ -59,6 +59,10 @@ def _load():
         "or_prior_gradient_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_prior_value_f32": (_D, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F]),
         "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
+        "or_ossps_denominator_f32": (_I, [_P, _P, _P, _I, _P]),
+        "or_prior_curvature_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _I, _I, _I, _F, _F, _F, _P]),
+        "or_ossps_update_f32": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P,
+                                     _F, _F, _F, _I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -199,6 +203,34 @@ class Oracle:
             raise RuntimeError("oracle update failed")
         return x
 
+    def ossps_denominator(self, y, norm=None, nthreads=None):
+        """OSSPS precomputed denominator A^T divide_and_truncate(A 1, (y n) n) (STIR order image)."""
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        n = None if norm is None else np.ascontiguousarray(norm, np.float32).ravel()
+        d = np.zeros(self.image_shape, np.float32)
+        if lib().or_ossps_denominator_f32(self.h, _ptr(y), _ptr(n), nthreads or default_threads(), _ptr(d)) != 0:
+            raise RuntimeError("oracle OSSPS denominator failed")
+        return d
+
+    def ossps_update(self, estimate, denom, y, additive, mult, sens, subset, nsub, subiteration_num,
+                     start_subiteration_num=1, zero_seg0_end_planes=False, prior=None, kappa=None,
+                     relaxation_parameter=1.0, relaxation_gamma=0.1, upper_bound=3.4028234663852886e38, nthreads=None):
+        """One OSSPS sub-iteration; returns (estimate, denominator) after it."""
+        x = np.ascontiguousarray(estimate, np.float32).copy().reshape(self.image_shape)
+        d = np.ascontiguousarray(denom, np.float32).copy().reshape(self.image_shape)
+        y = np.ascontiguousarray(y, np.float32).ravel()
+        a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+        m = None if mult is None else np.ascontiguousarray(mult, np.float32).ravel()
+        s = np.ascontiguousarray(sens, np.float32).ravel()
+        k = None if kappa is None else np.ascontiguousarray(kappa, np.float32).ravel()
+        p = prior if prior is not None else _abi.Prior(type=_abi.PRIOR_NONE)
+        if lib().or_ossps_update_f32(self.h, _ptr(x), _ptr(d), _ptr(y), _ptr(a), _ptr(m), _ptr(s), subset, nsub,
+                                     subiteration_num, start_subiteration_num, int(zero_seg0_end_planes),
+                                     ctypes.byref(p), _ptr(k), float(relaxation_parameter), float(relaxation_gamma),
+                                     float(upper_bound), nthreads or default_threads()) != 0:
+            raise RuntimeError("oracle OSSPS update failed")
+        return x, d
+
     def log_likelihood_gradient(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
                                 nthreads=None):
         x = np.ascontiguousarray(image, np.float32).ravel()
@@ -235,6 +267,16 @@ def prior_value(prior: _abi.Prior, image, voxel_size, kappa=None):
     nz, ny, nx = image.shape
     k = None if kappa is None else np.ascontiguousarray(kappa, np.float32)
     return lib().or_prior_value_f32(ctypes.byref(prior), _ptr(image), _ptr(k), nz, ny, nx, *map(float, voxel_size))
+
+
+def prior_curvature(prior: _abi.Prior, shape, voxel_size, kappa=None):
+    """QuadraticPrior::parabolic_surrogate_curvature of an image of `shape` [z][y][x]."""
+    nz, ny, nx = shape
+    k = None if kappa is None else np.ascontiguousarray(kappa, np.float32).ravel()
+    c = np.zeros(shape, np.float32)
+    if lib().or_prior_curvature_f32(ctypes.byref(prior), _ptr(k), nz, ny, nx, *map(float, voxel_size), _ptr(c)) != 0:
+        raise RuntimeError("oracle curvature failed")
+    return c
 
 
 def ray_trace(start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity=1 << 14):

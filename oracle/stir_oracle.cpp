@@ -1469,6 +1469,144 @@ double or_log_likelihood_f32(or_handle* h, const float* x, const float* y, const
   return accum;
 }
 
+/* OSSPS precomputed denominator (OSSPSReconstruction.cxx:184-221): minus the approximate Hessian of the
+   log-likelihood times an image of ones, i.e. A^T divide_and_truncate(A 1, (y n) n) over all bins, where n is
+   the normalisation's correction (BinNormalisation::apply multiplies by it; NULL: no normalisation)
+   (...AndProjData.cxx:955-1064; the small value of divide_and_truncate is taken on A 1) */
+int or_ossps_denominator_f32(or_handle* h, const float* y, const float* norm, int nthreads, float* denom) {
+  if (!h->f) return -1;
+  try {
+    auto& H = *h->f;
+    auto& g = H.g;
+    const int64_t ni = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+    std::vector<float> ones(ni, 1.f), fp(g.projdata_size, 0.f);
+    H.forward(ones.data(), fp.data(), 0, 1, nthreads);
+    const auto vs = basic_vs_in_subset(g, 0, 1);
+    for (const auto& b : vs)
+      for (int k = g.min_tof; k <= g.max_tof; ++k) {
+        std::vector<std::pair<int, int>> rel;
+        related_vs(g, b.first, b.second, rel);
+        for (const auto& r : rel) {
+          const int seg = r.second, view = r.first;
+          float vmax = -std::numeric_limits<float>::infinity();
+          for_viewgram(g, seg, view, k, [&](int, int, int64_t i) { vmax = std::max(vmax, fp[i]); });
+          const float small_value = std::max(vmax * SMALL_NUM, 0.F);
+          for_viewgram(g, seg, view, k, [&](int, int, int64_t i) {
+            float num = fp[i];
+            float den = y[i];
+            if (norm) {
+              den *= norm[i];
+              den *= norm[i];
+            }
+            if (num <= small_value) {
+              num = 0;
+            } else {
+              const float max_quotient = 10000.F;
+              num = (num > max_quotient * den) ? max_quotient : num / den;
+            }
+            fp[i] = num;
+          });
+        }
+      }
+    H.back(fp.data(), denom, 0, 1, nthreads);
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "oracle: %s\n", e.what());
+    return -1;
+  }
+}
+
+/* QuadraticPrior::parabolic_surrogate_curvature (QuadraticPrior.cxx:460-522): beta sum_k w_k (kappa_j kappa_k) */
+int or_prior_curvature_f32(const b200rt_prior* p, const float* kappa, int nz, int ny, int nx, float vz, float vy,
+                           float vx, float* out) {
+  const int64_t ni = static_cast<int64_t>(nz) * ny * nx;
+  if (!p || p->type == B200RT_PRIOR_NONE || p->penalisation_factor == 0) {
+    std::fill(out, out + ni, 0.f);
+    return 0;
+  }
+  if (p->type != B200RT_PRIOR_QUADRATIC) return -1;
+  float w[3][3][3];
+  prior_weights(w, vz, vy, vx, p->only_2D != 0);
+  const int dzmin = p->only_2D ? 0 : -1, dzmax = p->only_2D ? 0 : 1;
+  auto at = [&](int z, int y, int x) { return (static_cast<int64_t>(z) * ny + y) * nx + x; };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const int min_dz = std::max(dzmin, -z), max_dz = std::min(dzmax, nz - 1 - z);
+        const int min_dy = std::max(-1, -y), max_dy = std::min(1, ny - 1 - y);
+        const int min_dx = std::max(-1, -x), max_dx = std::min(1, nx - 1 - x);
+        float c = 0;
+        for (int dz = min_dz; dz <= max_dz; ++dz)
+          for (int dy = min_dy; dy <= max_dy; ++dy)
+            for (int dx = min_dx; dx <= max_dx; ++dx) {
+              float cur = w[dz + 1][dy + 1][dx + 1] * 1;
+              if (kappa) cur *= kappa[at(z, y, x)] * kappa[at(z + dz, y + dy, x + dx)];
+              c += cur;
+            }
+        out[at(z, y, x)] = c * p->penalisation_factor;
+      }
+  return 0;
+}
+
+/* One OSSPS sub-iteration (OSSPSReconstruction.cxx:284-410) on x (in/out).  denom: the precomputed denominator,
+   replaced at the first sub-iteration by the thresholded denominator including the prior's curvature (the
+   Quadratic prior's does not depend on x, :292-299,325-346).  sens: the total sensitivity, for
+   fill_nonidentifiable_target_parameters at the first sub-iteration. */
+int or_ossps_update_f32(or_handle* h, float* x, float* denom, const float* y, const float* add, const float* mult,
+                        const float* sens, int subset, int nsub, int subiter, int start_subiter, int zero_ends,
+                        const b200rt_prior* prior, const float* kappa, float relaxation_parameter,
+                        float relaxation_gamma, float upper_bound, int nthreads) {
+  if (!h->f) return -1;
+  auto& g = h->f->g;
+  const int64_t ni = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  if (subiter == start_subiter)
+    for (int64_t i = 0; i < ni; ++i)
+      if (sens[i] == 0) x[i] = 0;
+  std::vector<float> num(ni, 0.f);
+  if (or_loglik_gradient_f32(h, x, y, add, mult, subset, nsub, zero_ends, nthreads, num.data()) != 0) return -1;
+  if (has_prior) {
+    /* GeneralisedObjectiveFunction::compute_sub_gradient (GeneralisedObjectiveFunction.cxx:139-156) */
+    std::vector<float> pg(ni);
+    prior_gradient(*prior, x, kappa, g.nz, g.ny, g.nx, g.d.voxel_size_z, g.d.voxel_size_y, g.d.voxel_size_x, pg.data());
+    for (int64_t i = 0; i < ni; ++i) num[i] -= pg[i] / nsub;
+  }
+  for (int64_t i = 0; i < ni; ++i) num[i] = num[i] * nsub;
+  if (subiter == start_subiter) {
+    if (has_prior) {
+      std::vector<float> c(ni);
+      if (or_prior_curvature_f32(prior, kappa, g.nz, g.ny, g.nx, g.d.voxel_size_z, g.d.voxel_size_y,
+                                 g.d.voxel_size_x, c.data()) != 0)
+        return -1;
+      for (int64_t i = 0; i < ni; ++i) denom[i] = c[i] * 2 + denom[i];
+    }
+    /* threshold_min_to_small_positive_value(.., 10.E-6F) (thresholding.h:99-109) */
+    float minpos = std::numeric_limits<float>::infinity();
+    for (int64_t i = 0; i < ni; ++i)
+      if (denom[i] > 0 && denom[i] < minpos) minpos = denom[i];
+    if (minpos == std::numeric_limits<float>::infinity()) {
+      std::fill(denom, denom + ni, 10.E-6F);
+    } else {
+      const float lo = minpos * 10.E-6F;
+      for (int64_t i = 0; i < ni; ++i)
+        if (denom[i] < lo) denom[i] = lo;
+    }
+  }
+  for (int64_t i = 0; i < ni; ++i) num[i] = num[i] / denom[i];
+  const float relax = relaxation_parameter / (1 + relaxation_gamma * (subiter / nsub));
+  const float alpha = 1.F;
+  for (int64_t i = 0; i < ni; ++i) num[i] = num[i] * relax * alpha;
+  for (int64_t i = 0; i < ni; ++i) {
+    x[i] += num[i];
+    /* threshold_upper_lower(.., 0, upper_bound) */
+    if (x[i] > upper_bound)
+      x[i] = upper_bound;
+    else if (0.F > x[i])
+      x[i] = 0.F;
+  }
+  return 0;
+}
+
 int or_prior_gradient_f32(const b200rt_prior* p, const float* img, const float* kappa, int nz, int ny, int nx, float vz,
                           float vy, float vx, float* grad) {
   prior_gradient(*p, img, kappa, nz, ny, nx, vz, vy, vx, grad);

@@ -78,6 +78,17 @@ double or_log_likelihood_f32(or_handle* h, const float* image, const float* y, c
 int or_loglik_gradient_f32(or_handle* h, const float* image, const float* y, const float* additive, const float* mult,
                            int subset, int nsub, int zero_seg0_end_planes, int nthreads, float* gradient);
 
+/* OSSPS (src/iterative/OSSPS/OSSPSReconstruction.cxx): the precomputed denominator
+   A^T divide_and_truncate(A 1, (y n) n) (n: normalisation correction factors or NULL), the Quadratic prior's
+   parabolic surrogate curvature, and one sub-iteration (x and denom in/out; sens = total sensitivity). */
+int or_ossps_denominator_f32(or_handle* h, const float* y, const float* norm, int nthreads, float* denom);
+int or_prior_curvature_f32(const b200rt_prior* prior, const float* kappa, int nz, int ny, int nx, float vz, float vy,
+                           float vx, float* out);
+int or_ossps_update_f32(or_handle* h, float* x, float* denom, const float* y, const float* additive, const float* mult,
+                        const float* sens, int subset, int nsub, int subiteration_num, int start_subiteration_num,
+                        int zero_seg0_end_planes, const b200rt_prior* prior, const float* kappa,
+                        float relaxation_parameter, float relaxation_gamma, float upper_bound, int nthreads);
+
 /* Prior gradient and value (QuadraticPrior.cxx:233-372, RelativeDifferencePrior.cxx:280-452);
    image [z][y][x]; voxel sizes z,y,x. */
 int or_prior_gradient_f32(const b200rt_prior* prior, const float* image, const float* kappa, int nz, int ny, int nx,

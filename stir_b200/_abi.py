@@ -155,6 +155,9 @@ EXPORTS = [
     ("b200rt_forward_project", _I, [_P, _P, _P, _I, _I]),
     ("b200rt_back_project", _I, [_P, _P, _P, _I, _I, _I]),
     ("b200rt_attenuation_dev", _I, [_P, _P, _P, _I, _P]),
+    ("b200rt_ossps_denominator_dev", _I, [_P, _P, _P, _P, _I, _P]),
+    ("b200rt_ossps_subiteration_dev", _I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(Prior),
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _P]),
     ("b200rt_batch_create", _I, [_I, ctypes.POINTER(_P)]),
     ("b200rt_batch_destroy", None, [_P]),
     ("b200rt_batch_last_error", ctypes.c_char_p, [_P]),

@@ -108,6 +108,8 @@ struct b200rt_projector {
   float det_bound_value = 0.f;
   bool colmax_ready = false;
   float prior_w[27] = {0};
+  // OSSPS scratch: sub-gradient, prior gradient, image of ones, block minima
+  DevBuf<float> ossps_g, ossps_pg, ones, ossps_partial, ossps_minpos;
   // column-staged projection (paths.cu): path items, their lines, rows in path order
   bool use_paths = false;
   DevBuf<PathElem> path_elems;
@@ -874,6 +876,11 @@ void b200rt_destroy(b200rt_projector* h) {
     h->subset_lists.clear();
     h->subset_views.clear();
     h->path_lists.clear();
+    h->ossps_g.release();
+    h->ossps_pg.release();
+    h->ones.release();
+    h->ossps_partial.release();
+    h->ossps_minpos.release();
     h->path_elems.release();
     h->path_cols.release();
     h->path_lines.release();
@@ -1336,6 +1343,82 @@ int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* proj
     }
     forward_subset(*h, mu_dev, h->ratio.p, 0, 1, st);
     ck(launch_attenuation(h->ratio.p, projdata_dev, g.projdata_size(), mode, st), "attenuation");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_ossps_denominator_dev(b200rt_projector* h, const float* y_dev, const float* norm_dev, float* denominator_dev,
+                                 int back_projection_mode, void* stream) {
+  if (!h || !y_dev || !denominator_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_mode_prior(h, back_projection_mode, nullptr)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!h->ratio.p) {
+      h->ratio.alloc(g.projdata_size());
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+    }
+    if (!h->ones.p) {
+      h->ones.alloc(g.image_size());
+      ck(launch_fill(h->ones.p, g.image_size(), 1.F, st), "fill");
+    }
+    h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
+    forward_subset(*h, h->ones.p, h->ratio.p, 0, 1, st);
+    int nv = 0;
+    const int* views = subset_views(*h, 0, 1, nv);
+    // divide_and_truncate's small value from the forward projection of ones
+    ck(launch_viewgram_small_values(h->ratio.p, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, 0, g.num_tof(),
+                                    g.tof_stride(), h->small_value.p, st),
+       "viewgram thresholds");
+    ck(launch_hessian_ratio(h->ratio.p, y_dev, norm_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv,
+                            g.num_tof(), g.tof_stride(), h->small_value.p, st),
+       "Hessian data term");
+    back_project_into(*h, h->ratio.p, denominator_dev, 0, 1, back_projection_mode, 0, st);
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_ossps_subiteration_dev(b200rt_projector* h, float* estimate_dev, float* denominator_dev, const float* y_dev,
+                                  const float* additive_dev, const float* mult_dev, const float* sens_dev,
+                                  int subset_num, int num_subsets, int subiteration_num, int start_subiteration_num,
+                                  int zero_seg0_end_planes, const b200rt_prior* prior, float relaxation_parameter,
+                                  float relaxation_gamma, float upper_bound, int back_projection_mode, void* stream) {
+  if (!h || !estimate_dev || !denominator_dev || !y_dev || !sens_dev)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (int st = check_mode_prior(h, back_projection_mode, prior)) return st;
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  if (has_prior && prior->type != B200RT_PRIOR_QUADRATIC)
+    return fail(h, B200RT_ERR_UNSUPPORTED, "OSSPS needs a prior with a parabolic surrogate (QuadraticPrior)");
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t ni = g.image_size();
+    h->ossps_g.alloc(ni);
+    if (has_prior) h->ossps_pg.alloc(ni);
+    h->ossps_partial.alloc(update_num_blocks(ni));
+    h->ossps_minpos.alloc(1);
+    const bool first = subiteration_num == start_subiteration_num;
+    // fill_nonidentifiable_target_parameters at the first sub-iteration (OSSPSReconstruction.cxx:287-291)
+    if (first) ck(launch_zero_unidentifiable(estimate_dev, sens_dev, ni, st), "unidentifiable voxels");
+    if (int rc = b200rt_log_likelihood_gradient_dev(h, estimate_dev, y_dev, additive_dev, mult_dev, subset_num,
+                                                    num_subsets, zero_seg0_end_planes, back_projection_mode,
+                                                    h->ossps_g.p, stream))
+      return rc;
+    // relaxation_parameter / (1 + relaxation_gamma * (subiteration_num / num_subsets)), integer division
+    // (OSSPSReconstruction.cxx:370-372)
+    const float relax = relaxation_parameter / (1 + relaxation_gamma * (subiteration_num / num_subsets));
+    if (has_prior) prior_weights(g, prior->only_2D, h->prior_w);
+    ck(launch_ossps_update(estimate_dev, denominator_dev, h->ossps_g.p, has_prior ? h->ossps_pg.p : nullptr, sens_dev,
+                           has_prior ? prior : nullptr, h->prior_w, g.desc().ny, g.desc().nx, g.desc().nz, num_subsets,
+                           first ? 1 : 0, relax, upper_bound, h->ossps_partial.p, h->ossps_minpos.p, st),
+       "OSSPS update");
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());

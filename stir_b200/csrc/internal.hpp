@@ -275,6 +275,16 @@ cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbin
 // max |projdata| (nullptr data = 1) and the fixed-point scale 2^floor(62 - log2(max|d| * colmax * 1.01)) (osem.cu)
 cudaError_t launch_fixed_scale(const float* projdata, int64_t n, const float* colmax, float* partial, double* scale,
                                cudaStream_t st);
+cudaError_t launch_fill(float* p, int64_t n, float v, cudaStream_t st);
+cudaError_t launch_zero_unidentifiable(float* x, const float* sens, int64_t n, cudaStream_t st);
+// OSSPS: divide_and_truncate(A 1, (y n) n) in place per viewgram; the update (with, at the first sub-iteration,
+// the unidentifiable voxels zeroed and the denominator completed and thresholded in place)
+cudaError_t launch_hessian_ratio(float* fp, const float* y, const float* norm, const SegDev* segs, int S, int num_views,
+                                 int num_tang, const int* views, int nviews, int num_tof, int64_t tof_stride,
+                                 const float* small_value, cudaStream_t st);
+cudaError_t launch_ossps_update(float* x, float* den, const float* g, float* pg, const float* sens, const b200rt_prior* prior,
+                                const float prior_weights[27], int ny, int nx, int nz, int num_subsets, int first,
+                                float relax, float upper, float* partial, float* minpos, cudaStream_t st);
 cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int64_t n, int mode, cudaStream_t st);
 cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* scale, float* image, int64_t n,
                                   cudaStream_t st);

@@ -321,6 +321,205 @@ cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int
   return cudaGetLastError();
 }
 
+// ---- OSSPS (OSSPSReconstruction.cxx) ----------------------------------------------------------------
+
+namespace {
+
+__global__ void fill_kernel(float* __restrict__ p, int64_t n, float v) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
+// one block per (segment, view) of the data: divide_and_truncate(A 1, (y n) n) in place on the forward
+// projection (...AndProjData.cxx:1021-1046), small value from the forward projection's viewgram maximum
+__global__ void hessian_ratio_kernel(float* __restrict__ fp, const float* __restrict__ y, const float* __restrict__ norm,
+                                     const SegDev* __restrict__ segs, int S, int num_views, int num_tang,
+                                     const int* __restrict__ views, int64_t tof_stride,
+                                     const float* __restrict__ small_value) {
+  const int seg = static_cast<int>(blockIdx.y) - S;
+  const int view = views[blockIdx.x];
+  const int tofi = blockIdx.z;
+  const SegDev sd = segs[seg + S];
+  const int64_t base = tofi * tof_stride + sd.dev_offset + static_cast<int64_t>(view) * num_tang * sd.nax;
+  const int n = num_tang * sd.nax;
+  const float sv = small_value[(tofi * (2 * S + 1) + seg + S) * num_views + view];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    float num = fp[base + i];
+    float den = y[base + i];
+    if (norm) {
+      den *= norm[base + i];
+      den *= norm[base + i];
+    }
+    if (num <= sv)
+      num = 0.f;
+    else
+      num = (num > 10000.F * den) ? 10000.F : num / den;
+    fp[base + i] = num;
+  }
+}
+
+// x = 0 where the sensitivity is 0 (fill_nonidentifiable_target_parameters,
+// PoissonLogLikelihoodWithLinearModelForMean.cxx:459-471)
+__global__ void zero_unidentifiable_kernel(float* __restrict__ x, const float* __restrict__ sens, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    if (sens[i] == 0) x[i] = 0.f;
+}
+
+// den = curvature * 2 + den with the Quadratic prior's parabolic surrogate curvature
+// (QuadraticPrior.cxx:460-522; OSSPSReconstruction.cxx:330-339), and the block minimum of its positive values
+__global__ void ossps_denominator_kernel(float* __restrict__ den, PriorDev pr, int ny, int nx, int nz,
+                                         float* __restrict__ partial_min) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  float m = INFINITY;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float d = den[i];
+    if (pr.type != 0) {
+      const int zi = static_cast<int>(i % nz);
+      const int64_t c = i / nz;
+      const int xi = static_cast<int>(c % nx), yi = static_cast<int>(c / nx);
+      const int dz0 = max(pr.dzmin, -zi), dz1 = min(pr.dzmax, nz - 1 - zi);
+      const int dy0 = max(-1, -yi), dy1 = min(1, ny - 1 - yi);
+      const int dx0 = max(-1, -xi), dx1 = min(1, nx - 1 - xi);
+      float cv = 0.f;
+      for (int dz = dz0; dz <= dz1; ++dz)
+        for (int dy = dy0; dy <= dy1; ++dy)
+          for (int dx = dx0; dx <= dx1; ++dx) {
+            float cur = pr.w[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * 1;
+            if (pr.kappa) {
+              const int64_t j = i + (static_cast<int64_t>(dy) * nx + dx) * nz + dz;
+              cur *= pr.kappa[i] * pr.kappa[j];
+            }
+            cv += cur;
+          }
+      d = (cv * pr.beta) * 2 + d;
+      den[i] = d;
+    }
+    if (d > 0) m = fminf(m, d);
+  }
+  __shared__ float red[32];
+  for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : INFINITY;
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) partial_min[blockIdx.x] = m;
+  }
+}
+
+__global__ void reduce_min_kernel(const float* __restrict__ partial, int n, float* __restrict__ out) {
+  float m = INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fminf(m, partial[i]);
+  __shared__ float red[32];
+  for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : INFINITY;
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) *out = m;
+  }
+}
+
+// threshold_min_to_small_positive_value(den, small) (thresholding.h:99-109) given the smallest positive value
+__global__ void threshold_small_positive_kernel(float* __restrict__ den, int64_t n, const float* __restrict__ minpos,
+                                                float small) {
+  const float mp = *minpos;
+  const bool none = !(mp < INFINITY);
+  const float lo = mp * small;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (none)
+      den[i] = small;
+    else if (den[i] < lo)
+      den[i] = lo;
+  }
+}
+
+// the update of OSSPSReconstruction::update_estimate (:314-407) given the sub-gradient g, the prior gradient pg
+// (or nullptr) and the denominator
+__global__ void ossps_update_kernel(float* __restrict__ x, const float* __restrict__ g, const float* __restrict__ pg,
+                                    const float* __restrict__ den, int64_t n, int num_subsets, float relax,
+                                    float upper) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float num = g[i];
+    if (pg) num -= pg[i] / num_subsets;
+    num = num * num_subsets;
+    num = num / den[i];
+    num = num * relax * 1.F;
+    float v = x[i] + num;
+    if (v > upper)
+      v = upper;
+    else if (0.F > v)
+      v = 0.F;
+    x[i] = v;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_zero_unidentifiable(float* x, const float* sens, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  zero_unidentifiable_kernel<<<update_num_blocks(n), 256, 0, st>>>(x, sens, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(float* p, int64_t n, float v, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  fill_kernel<<<update_num_blocks(n), 256, 0, st>>>(p, n, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hessian_ratio(float* fp, const float* y, const float* norm, const SegDev* segs, int S, int num_views,
+                                 int num_tang, const int* views, int nviews, int num_tof, int64_t tof_stride,
+                                 const float* small_value, cudaStream_t st) {
+  if (nviews <= 0) return cudaSuccess;
+  hessian_ratio_kernel<<<dim3(nviews, 2 * S + 1, num_tof), 256, 0, st>>>(fp, y, norm, segs, S, num_views, num_tang, views,
+                                                                          tof_stride, small_value);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ossps_update(float* x, float* den, const float* g, float* pg, const float* sens, const b200rt_prior* prior,
+                                const float prior_weights[27], int ny, int nx, int nz, int num_subsets, int first,
+                                float relax, float upper, float* partial, float* minpos, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  const int blocks = update_num_blocks(n);
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  PriorDev pr{};
+  if (has_prior) {
+    pr.type = prior->type;
+    pr.beta = prior->penalisation_factor;
+    pr.gamma = prior->gamma;
+    pr.epsilon = prior->epsilon;
+    pr.dzmin = prior->only_2D ? 0 : -1;
+    pr.dzmax = prior->only_2D ? 0 : 1;
+    for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
+    pr.kappa = prior->kappa_dev;
+  }
+  cudaError_t e;
+  (void)sens;
+  if (has_prior) {
+    update_prepare_kernel<<<blocks, 256, 0, st>>>(x, x, pg, pr, ny, nx, nz, partial);  // prior gradient into pg
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (first) {
+    PriorDev pc = pr;  // the curvature term is added for the Quadratic prior only
+    if (pc.type != B200RT_PRIOR_QUADRATIC) pc.type = 0;
+    ossps_denominator_kernel<<<blocks, 256, 0, st>>>(den, pc, ny, nx, nz, partial);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    reduce_min_kernel<<<1, 1024, 0, st>>>(partial, blocks, minpos);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    threshold_small_positive_kernel<<<blocks, 256, 0, st>>>(den, n, minpos, 10.E-6F);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  ossps_update_kernel<<<blocks, 256, 0, st>>>(x, g, has_prior ? pg : nullptr, den, n, num_subsets, relax, upper);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
                                          float* out, cudaStream_t st) {

@@ -385,8 +385,8 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
     for (int t = lane; t < dl_len; t += 32) {
       const int r = t - front;
       float d = 0.f;
-      if (L.active && r >= 0 && r % L.npa == 0) {
-        const int a = r / L.npa;
+      if (L.active && r >= 0 && (L.npa == 1 || r % L.npa == 0)) {
+        const int a = L.npa == 1 ? r : r / L.npa;
         if (a < L.nax && !(zero_ends && L.seg == 0 && (a == 0 || a == L.nax - 1)))
           d = pd ? __ldg(pd + L.out_base + a) : 1.f;  // pd == nullptr back-projects ones
       }

@@ -275,6 +275,12 @@ int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, co
  * (src/recon_buildblock/BinNormalisationFromAttenuationImage.cxx:122-170); non-TOF only, as STIR. */
 int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* projdata_dev, int mode, void* stream);
 
+/* accumulate_Hessian_times_input of the prior (QuadraticPrior.cxx:603-688, RelativeDifferencePrior.cxx:535-621):
+ * output += beta sum_k w_jk (f20(x_j, x_k) in_j + f11(x_j, x_k) in_k) (kappa_j kappa_k) at x = image_dev;
+ * device layout images. */
+int b200rt_prior_hessian_times_input_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev,
+                                         const float* input_dev, float* output_dev, void* stream);
+
 /* ---- OSSPS (src/iterative/OSSPS/OSSPSReconstruction.cxx) on device-resident data ---- */
 /* precompute_denominator_of_conditioner_without_penalty (OSSPSReconstruction.cxx:184-221): minus the
  * approximate Hessian of the log-likelihood times ones, A^T divide_and_truncate(A 1, (y n) n) over all bins

@@ -60,6 +60,7 @@ def _load():
         "or_prior_value_f32": (_D, [ctypes.POINTER(_abi.Prior), _P, _P, _I, _I, _I, _F, _F, _F]),
         "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
         "or_ossps_denominator_f32": (_I, [_P, _P, _P, _I, _P]),
+        "or_prior_hessian_times_input_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_prior_curvature_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_ossps_update_f32": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P,
                                      _F, _F, _F, _I]),
@@ -267,6 +268,18 @@ def prior_value(prior: _abi.Prior, image, voxel_size, kappa=None):
     nz, ny, nx = image.shape
     k = None if kappa is None else np.ascontiguousarray(kappa, np.float32)
     return lib().or_prior_value_f32(ctypes.byref(prior), _ptr(image), _ptr(k), nz, ny, nx, *map(float, voxel_size))
+
+
+def prior_hessian_times_input(prior: _abi.Prior, image, input_image, voxel_size, kappa=None, out=None):
+    """out + the prior's Hessian at `image` times `input_image` ([z][y][x])."""
+    image = np.ascontiguousarray(image, np.float32)
+    nz, ny, nx = image.shape
+    inp = np.ascontiguousarray(input_image, np.float32)
+    k = None if kappa is None else np.ascontiguousarray(kappa, np.float32).ravel()
+    o = np.zeros(image.shape, np.float32) if out is None else np.ascontiguousarray(out, np.float32).copy()
+    lib().or_prior_hessian_times_input_f32(ctypes.byref(prior), _ptr(image), _ptr(inp), _ptr(k), nz, ny, nx,
+                                           *map(float, voxel_size), _ptr(o))
+    return o
 
 
 def prior_curvature(prior: _abi.Prior, shape, voxel_size, kappa=None):

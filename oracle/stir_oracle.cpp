@@ -1469,6 +1469,63 @@ double or_log_likelihood_f32(or_handle* h, const float* x, const float* y, const
   return accum;
 }
 
+/* RelativeDifferencePrior::derivative_20 / derivative_11 (RelativeDifferencePrior.cxx:623-641): pow of a float
+   by an int is evaluated in double, the quotient returned as float */
+inline float rdp_derivative_20(float xj, float xk, float gamma, float epsilon) {
+  if (xj > 0.0 || xk > 0.0 || epsilon > 0.0)
+    return static_cast<float>(2 * std::pow(2 * xk + epsilon, 2) / std::pow(xj + xk + gamma * std::abs(xj - xk) + epsilon, 3));
+  return std::numeric_limits<float>::infinity();
+}
+inline float rdp_derivative_11(float xj, float xk, float gamma, float epsilon) {
+  if (xj > 0.0 || xk > 0.0 || epsilon > 0.0)
+    return static_cast<float>(-2 * (2 * xj + epsilon) * (2 * xk + epsilon) /
+                              std::pow(xj + xk + gamma * std::abs(xj - xk) + epsilon, 3));
+  return std::numeric_limits<float>::infinity();
+}
+
+/* accumulate_Hessian_times_input (QuadraticPrior.cxx:603-688, RelativeDifferencePrior.cxx:535-621):
+   out += beta * sum_k w_k (f20(x_j, x_k) in_j + f11(x_j, x_k) in_k) (kappa_j kappa_k) */
+int or_prior_hessian_times_input_f32(const b200rt_prior* p, const float* x, const float* in, const float* kappa, int nz,
+                                     int ny, int nx, float vz, float vy, float vx, float* out) {
+  if (!p || p->type == B200RT_PRIOR_NONE || p->penalisation_factor == 0) return 0;
+  float w[3][3][3];
+  prior_weights(w, vz, vy, vx, p->only_2D != 0);
+  const int dzmin = p->only_2D ? 0 : -1, dzmax = p->only_2D ? 0 : 1;
+  auto at = [&](int z, int y, int xx) { return (static_cast<int64_t>(z) * ny + y) * nx + xx; };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int xx = 0; xx < nx; ++xx) {
+        const int min_dz = std::max(dzmin, -z), max_dz = std::min(dzmax, nz - 1 - z);
+        const int min_dy = std::max(-1, -y), max_dy = std::min(1, ny - 1 - y);
+        const int min_dx = std::max(-1, -xx), max_dx = std::min(1, nx - 1 - xx);
+        const int64_t j = at(z, y, xx);
+        float result = 0;
+        for (int dz = min_dz; dz <= max_dz; ++dz)
+          for (int dy = min_dy; dy <= max_dy; ++dy)
+            for (int dx = min_dx; dx <= max_dx; ++dx) {
+              float current = w[dz + 1][dy + 1][dx + 1];
+              if (current == 0.f) continue;
+              const int64_t k = at(z + dz, y + dy, xx + dx);
+              float f20, f11;
+              if (p->type == B200RT_PRIOR_QUADRATIC) {
+                f20 = 1.0;
+                f11 = -1.0;
+              } else {
+                f20 = rdp_derivative_20(x[j], x[k], p->gamma, p->epsilon);
+                f11 = rdp_derivative_11(x[j], x[k], p->gamma, p->epsilon);
+              }
+              if (dz == 0 && dy == 0 && dx == 0)
+                current *= f20 * in[j];
+              else
+                current *= (f20 * in[j] + f11 * in[k]);
+              if (kappa) current *= kappa[j] * kappa[k];
+              result += current;
+            }
+        out[j] += result * p->penalisation_factor;
+      }
+  return 0;
+}
+
 /* OSSPS precomputed denominator (OSSPSReconstruction.cxx:184-221): minus the approximate Hessian of the
    log-likelihood times an image of ones, i.e. A^T divide_and_truncate(A 1, (y n) n) over all bins, where n is
    the normalisation's correction (BinNormalisation::apply multiplies by it; NULL: no normalisation)

@@ -78,6 +78,12 @@ double or_log_likelihood_f32(or_handle* h, const float* image, const float* y, c
 int or_loglik_gradient_f32(or_handle* h, const float* image, const float* y, const float* additive, const float* mult,
                            int subset, int nsub, int zero_seg0_end_planes, int nthreads, float* gradient);
 
+/* prior Hessian times an image, accumulated into out (QuadraticPrior.cxx:603-688,
+   RelativeDifferencePrior.cxx:535-621); image [z][y][x] */
+int or_prior_hessian_times_input_f32(const b200rt_prior* prior, const float* image, const float* input,
+                                     const float* kappa, int nz, int ny, int nx, float vz, float vy, float vx,
+                                     float* out);
+
 /* OSSPS (src/iterative/OSSPS/OSSPSReconstruction.cxx): the precomputed denominator
    A^T divide_and_truncate(A 1, (y n) n) (n: normalisation correction factors or NULL), the Quadratic prior's
    parabolic surrogate curvature, and one sub-iteration (x and denom in/out; sens = total sensitivity). */

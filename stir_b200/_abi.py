@@ -155,6 +155,7 @@ EXPORTS = [
     ("b200rt_forward_project", _I, [_P, _P, _P, _I, _I]),
     ("b200rt_back_project", _I, [_P, _P, _P, _I, _I, _I]),
     ("b200rt_attenuation_dev", _I, [_P, _P, _P, _I, _P]),
+    ("b200rt_prior_hessian_times_input_dev", _I, [_P, ctypes.POINTER(Prior), _P, _P, _P, _P]),
     ("b200rt_ossps_denominator_dev", _I, [_P, _P, _P, _P, _I, _P]),
     ("b200rt_ossps_subiteration_dev", _I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(Prior),
                                            ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _P]),

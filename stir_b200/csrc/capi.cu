@@ -1425,6 +1425,24 @@ int b200rt_ossps_subiteration_dev(b200rt_projector* h, float* estimate_dev, floa
   }
 }
 
+int b200rt_prior_hessian_times_input_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev,
+                                         const float* input_dev, float* output_dev, void* stream) {
+  if (!h || !prior || !image_dev || !input_dev || !output_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_mode_prior(h, B200RT_BACKPROJECT_ATOMIC, prior)) return st;
+  try {
+    DeviceGuard dg(h->device);
+    const Geometry& g = *h->geo;
+    float w[27];
+    prior_weights(g, prior->only_2D, w);
+    ck(launch_prior_hessian_times_input(output_dev, image_dev, input_dev, prior, w, g.desc().ny, g.desc().nx,
+                                        g.desc().nz, static_cast<cudaStream_t>(stream)),
+       "prior Hessian");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
                            void* stream) {
   if (!h || !prior || !image_dev || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");

@@ -276,6 +276,8 @@ cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbin
 cudaError_t launch_fixed_scale(const float* projdata, int64_t n, const float* colmax, float* partial, double* scale,
                                cudaStream_t st);
 cudaError_t launch_fill(float* p, int64_t n, float v, cudaStream_t st);
+cudaError_t launch_prior_hessian_times_input(float* out, const float* x, const float* in, const b200rt_prior* prior,
+                                             const float prior_weights[27], int ny, int nx, int nz, cudaStream_t st);
 cudaError_t launch_zero_unidentifiable(float* x, const float* sens, int64_t n, cudaStream_t st);
 // OSSPS: divide_and_truncate(A 1, (y n) n) in place per viewgram; the update (with, at the first sub-iteration,
 // the unidentifiable voxels zeroed and the denominator completed and thresholded in place)

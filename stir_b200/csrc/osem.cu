@@ -321,6 +321,86 @@ cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int
   return cudaGetLastError();
 }
 
+// ---- prior Hessian times an image (QuadraticPrior.cxx:603-688, RelativeDifferencePrior.cxx:535-621) ----
+
+namespace {
+
+// RelativeDifferencePrior::derivative_20 / derivative_11 (RelativeDifferencePrior.cxx:623-641): the powers of
+// the float arguments are taken in double (STIR's pow(float, int)), the quotient returned as float
+__device__ __forceinline__ float rdp_derivative_20(float xj, float xk, float gamma, float epsilon) {
+  if (xj > 0.0f || xk > 0.0f || epsilon > 0.0f) {
+    const double a = static_cast<double>(2 * xk + epsilon);
+    const double b = static_cast<double>(xj + xk + gamma * fabsf(xj - xk) + epsilon);
+    return static_cast<float>(2 * (a * a) / (b * b * b));
+  }
+  return INFINITY;
+}
+__device__ __forceinline__ float rdp_derivative_11(float xj, float xk, float gamma, float epsilon) {
+  if (xj > 0.0f || xk > 0.0f || epsilon > 0.0f) {
+    const float num = -2 * (2 * xj + epsilon) * (2 * xk + epsilon);
+    const double b = static_cast<double>(xj + xk + gamma * fabsf(xj - xk) + epsilon);
+    return static_cast<float>(num / (b * b * b));
+  }
+  return INFINITY;
+}
+
+__global__ void hessian_times_input_kernel(float* __restrict__ out, const float* __restrict__ x,
+                                           const float* __restrict__ in, PriorDev pr, int ny, int nx, int nz) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int zi = static_cast<int>(i % nz);
+    const int64_t c = i / nz;
+    const int xi = static_cast<int>(c % nx), yi = static_cast<int>(c / nx);
+    const int dz0 = max(pr.dzmin, -zi), dz1 = min(pr.dzmax, nz - 1 - zi);
+    const int dy0 = max(-1, -yi), dy1 = min(1, ny - 1 - yi);
+    const int dx0 = max(-1, -xi), dx1 = min(1, nx - 1 - xi);
+    const float xj = x[i], inj = in[i];
+    float result = 0.f;
+    for (int dz = dz0; dz <= dz1; ++dz)
+      for (int dy = dy0; dy <= dy1; ++dy)
+        for (int dx = dx0; dx <= dx1; ++dx) {
+          float current = pr.w[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+          if (current == 0.f) continue;
+          const int64_t k = i + (static_cast<int64_t>(dy) * nx + dx) * nz + dz;
+          float f20, f11;
+          if (pr.type == B200RT_PRIOR_QUADRATIC) {
+            f20 = 1.0f;
+            f11 = -1.0f;
+          } else {
+            f20 = rdp_derivative_20(xj, x[k], pr.gamma, pr.epsilon);
+            f11 = rdp_derivative_11(xj, x[k], pr.gamma, pr.epsilon);
+          }
+          if (dz == 0 && dy == 0 && dx == 0)
+            current *= f20 * inj;
+          else
+            current *= (f20 * inj + f11 * in[k]);
+          if (pr.kappa) current *= pr.kappa[i] * pr.kappa[k];
+          result += current;
+        }
+    out[i] += result * pr.beta;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_prior_hessian_times_input(float* out, const float* x, const float* in, const b200rt_prior* prior,
+                                             const float prior_weights[27], int ny, int nx, int nz, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(ny) * nx * nz;
+  if (!prior || prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0 || n <= 0) return cudaSuccess;
+  PriorDev pr{};
+  pr.type = prior->type;
+  pr.beta = prior->penalisation_factor;
+  pr.gamma = prior->gamma;
+  pr.epsilon = prior->epsilon;
+  pr.dzmin = prior->only_2D ? 0 : -1;
+  pr.dzmax = prior->only_2D ? 0 : 1;
+  for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
+  pr.kappa = prior->kappa_dev;
+  hessian_times_input_kernel<<<update_num_blocks(n), 256, 0, st>>>(out, x, in, pr, ny, nx, nz);
+  return cudaGetLastError();
+}
+
 // ---- OSSPS (OSSPSReconstruction.cxx) ----------------------------------------------------------------
 
 namespace {

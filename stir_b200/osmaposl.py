@@ -167,3 +167,13 @@ def prior_gradient(projector: RayTracingProjector, prior, x, out=None, stream=No
     _abi.check(projector.lib.b200rt_prior_gradient_dev(projector.h, ctypes.byref(prior.as_abi()), _ptr(x), _ptr(out),
                                                        _stream_ptr(stream)), projector.h, "b200rt_prior_gradient_dev")
     return out
+
+
+def prior_hessian_times_input(projector: RayTracingProjector, prior, x, input_image, out=None, stream=None):
+    """out += the prior's Hessian at x times input_image (accumulate_Hessian_times_input of QuadraticPrior /
+    RelativeDifferencePrior); device-layout images.  out defaults to zeros."""
+    out = projector.empty_image() if out is None else out
+    _abi.check(projector.lib.b200rt_prior_hessian_times_input_dev(
+        projector.h, ctypes.byref(prior.as_abi()), _ptr(x), _ptr(input_image), _ptr(out), _stream_ptr(stream)),
+        projector.h, "b200rt_prior_hessian_times_input_dev")
+    return out

@@ -1236,10 +1236,11 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     const Geometry& g = *h->geo;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     int n = 0, nv = 0;
-    const int* list = subset_list(*h, subset_num, num_subsets, n);
+    // one partial sum per CTA: per path item with the column-staged kernel, else per basic bin
+    const int* list = h->use_paths ? path_list(*h, subset_num, num_subsets, n) : subset_list(*h, subset_num, num_subsets, n);
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
     h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
-    h->ll_partials.alloc(std::max(n, 1));
+    if (h->ll_partials.n < static_cast<size_t>(std::max(n, 1))) h->ll_partials.alloc(std::max(n, 1));
     h->ll_sum.alloc(1);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
                                     g.num_tof(), g.tof_stride(), h->small_value.p, st),
@@ -1252,7 +1253,10 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     ep.mult = mult_dev;
     ep.small_value = h->small_value.p;
     ep.partials = h->ll_partials.p;
-    ck(launch_forward(h->params, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
+    if (h->use_paths)
+      ck(launch_forward_paths(h->params, h->pparams, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
+    else
+      ck(launch_forward(h->params, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
     ck(launch_reduce_sum(h->ll_partials.p, n, h->ll_sum.p, st), "reduce");
     ck(cudaMemcpyAsync(out, h->ll_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "log-likelihood");

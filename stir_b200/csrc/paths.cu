@@ -425,6 +425,18 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if ((threadIdx.x & 31) == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
   }
+  if (EPI == kEpiLoglik) {
+    // per-CTA partial sums, reduced in a fixed order by the caller: deterministic
+    __shared__ double red[kPathWarps];
+    for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ll;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kPathWarps; ++w) t += red[w];
+      ep.partials[blockIdx.x] = t;
+    }
+  }
 }
 
 template <typename Cols>
@@ -555,7 +567,8 @@ cudaError_t launch_forward_paths(const ProjParams& p, const PathParams& pp, cons
     case kEpiNone: return launch_forward_paths_epi<kEpiNone>(p, pp, items, nitems, image, projdata, st, e);
     case kEpiRatio: return launch_forward_paths_epi<kEpiRatio>(p, pp, items, nitems, image, projdata, st, e);
     case kEpiGradient: return launch_forward_paths_epi<kEpiGradient>(p, pp, items, nitems, image, projdata, st, e);
-    default: return cudaErrorInvalidValue;  // the log-likelihood keeps the per-basic-bin kernel
+    case kEpiLoglik: return launch_forward_paths_epi<kEpiLoglik>(p, pp, items, nitems, image, projdata, st, e);
+    default: return cudaErrorInvalidValue;
   }
 }
 

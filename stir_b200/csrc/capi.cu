@@ -179,63 +179,67 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
     std::vector<std::pair<uint64_t, float>> tmp;
     for (int gi = g0; gi < g1; ++gi) {
       Group& G = groups[gi];
-      const int vi = gi / ntangs, ti = gi % ntangs;
-      std::vector<uint32_t> keys;
-      for (int si = 0; si < nsegs; ++si) {
-        const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
-        for (int k = 0; k < pb.row_len; ++k) keys.push_back(hr[pb.row_offset + k].zyx & 0x3fffffu);  // x, y bits
-      }
-      std::sort(keys.begin(), keys.end());
-      keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-      if (keys.size() > 65535) {
-        G.ok = false;
-        continue;
-      }
-      G.cols = keys;
-      const int ncols = static_cast<int>(keys.size());
-      const int nch = (ncols + K - 1) / K;
-      for (int si = 0; si < nsegs; ++si) {
-        const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
-        tmp.clear();
-        for (int k = 0; k < pb.row_len; ++k) {
-          const RowElem e = hr[pb.row_offset + k];
-          const uint32_t slot =
-              static_cast<uint32_t>(std::lower_bound(keys.begin(), keys.end(), e.zyx & 0x3fffffu) - keys.begin());
-          const uint32_t zb = e.zyx >> 22;  // z + 512
-          tmp.push_back({(static_cast<uint64_t>(slot) << 32) | (static_cast<uint64_t>(zb) << 16) | 0u, e.v});
-        }
-        std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<uint64_t, float>& a,
-                                                    const std::pair<uint64_t, float>& b) { return a.first < b.first; });
-        G.member_off.push_back(static_cast<int64_t>(G.elems.size()));
-        G.member_chunk.push_back(static_cast<int>(G.chunks.size()));
-        for (const auto& t : tmp) {
-          const uint32_t slot = static_cast<uint32_t>(t.first >> 32);
-          const uint32_t zb = static_cast<uint32_t>((t.first >> 16) & 0xffffu);
-          G.elems.push_back(PathElem{slot | (zb << 16), t.second});
-        }
-        // chunk c covers the elements with slot in [c K, (c + 1) K)
-        size_t k = 0;
-        for (int c = 0; c <= nch; ++c) {
-          const uint32_t lim = static_cast<uint32_t>(std::min(c * K, ncols));
-          while (k < tmp.size() && (tmp[k].first >> 32) < lim) ++k;
-          G.chunks.push_back(static_cast<int>(k));
-        }
-      }
-      // the same elements in column order (slot, then member, then z) for the back projection
-      std::vector<size_t> cur(nsegs);
-      for (int si = 0; si < nsegs; ++si) cur[si] = static_cast<size_t>(G.member_off[si]);
-      for (int slot = 0; slot < ncols; ++slot) {
-        G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
+      try {
+        const int vi = gi / ntangs, ti = gi % ntangs;
+        std::vector<uint32_t> keys;
         for (int si = 0; si < nsegs; ++si) {
-          const size_t end = si + 1 < nsegs ? static_cast<size_t>(G.member_off[si + 1]) : G.elems.size();
-          while (cur[si] < end && static_cast<int>(G.elems[cur[si]].sz & 0xffffu) == slot) {
-            const PathElem& e = G.elems[cur[si]];
-            G.cmaj.push_back(PathCElem{(e.sz >> 16) | (static_cast<uint32_t>(si) << 16), e.v});
-            ++cur[si];
+          const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
+          for (int k = 0; k < pb.row_len; ++k) keys.push_back(hr[pb.row_offset + k].zyx & 0x3fffffu);  // x, y bits
+        }
+        std::sort(keys.begin(), keys.end());
+        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+        if (keys.size() > 65535) {
+          G.ok = false;
+          continue;
+        }
+        G.cols = keys;
+        const int ncols = static_cast<int>(keys.size());
+        const int nch = (ncols + K - 1) / K;
+        for (int si = 0; si < nsegs; ++si) {
+          const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
+          tmp.clear();
+          for (int k = 0; k < pb.row_len; ++k) {
+            const RowElem e = hr[pb.row_offset + k];
+            const uint32_t slot =
+                static_cast<uint32_t>(std::lower_bound(keys.begin(), keys.end(), e.zyx & 0x3fffffu) - keys.begin());
+            const uint32_t zb = e.zyx >> 22;  // z + 512
+            tmp.push_back({(static_cast<uint64_t>(slot) << 32) | (static_cast<uint64_t>(zb) << 16) | 0u, e.v});
+          }
+          std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<uint64_t, float>& a,
+                                                      const std::pair<uint64_t, float>& b) { return a.first < b.first; });
+          G.member_off.push_back(static_cast<int64_t>(G.elems.size()));
+          G.member_chunk.push_back(static_cast<int>(G.chunks.size()));
+          for (const auto& t : tmp) {
+            const uint32_t slot = static_cast<uint32_t>(t.first >> 32);
+            const uint32_t zb = static_cast<uint32_t>((t.first >> 16) & 0xffffu);
+            G.elems.push_back(PathElem{slot | (zb << 16), t.second});
+          }
+          // chunk c covers the elements with slot in [c K, (c + 1) K)
+          size_t k = 0;
+          for (int c = 0; c <= nch; ++c) {
+            const uint32_t lim = static_cast<uint32_t>(std::min(c * K, ncols));
+            while (k < tmp.size() && (tmp[k].first >> 32) < lim) ++k;
+            G.chunks.push_back(static_cast<int>(k));
           }
         }
+        // the same elements in column order (slot, then member, then z) for the back projection
+        std::vector<size_t> cur(nsegs);
+        for (int si = 0; si < nsegs; ++si) cur[si] = static_cast<size_t>(G.member_off[si]);
+        for (int slot = 0; slot < ncols; ++slot) {
+          G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
+          for (int si = 0; si < nsegs; ++si) {
+            const size_t end = si + 1 < nsegs ? static_cast<size_t>(G.member_off[si + 1]) : G.elems.size();
+            while (cur[si] < end && static_cast<int>(G.elems[cur[si]].sz & 0xffffu) == slot) {
+              const PathElem& e = G.elems[cur[si]];
+              G.cmaj.push_back(PathCElem{(e.sz >> 16) | (static_cast<uint32_t>(si) << 16), e.v});
+              ++cur[si];
+            }
+          }
+        }
+        G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
+      } catch (const std::exception&) {
+        G.ok = false;  // the per-basic-bin kernels are used instead
       }
-      G.col_starts.push_back(static_cast<int>(G.cmaj.size()));
     }
   };
   const int nthreads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));

@@ -281,8 +281,9 @@ def batched_dynamic(local, iterations):
     err = max(float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
               for a, b in zip(x_b, x_one))
     nsub_max = max(fr["nsub"] for fr in frames)
-    launches = sum(2 + 4 * sum(1 for fr in frames if k <= iterations * fr["nsub"])
-                   for k in range(1, iterations * nsub_max + 1))
+    # per batched sub-iteration: the forward and back projections and the three update launches; once per
+    # run: one threshold launch per frame
+    launches = 5 * iterations * nsub_max + len(frames)
     batch.close()
     for p in projs.values():
         p.close()

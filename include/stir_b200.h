@@ -314,7 +314,8 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
  * num_subiterations >= k by its own sub-iteration k, subset (start_subset + k - 1) % num_subsets, with
  * the result of b200rt_osmaposl_subiteration_dev (atomic back projection) up to float rounding.  Per k:
  * one persistent forward launch (ratio epilogue) and one persistent back projection cover every
- * frame's subset; the thresholds and the update of each frame run around them.  Projectors passed to
+ * frame's subset, and the frames' updates run as three launches over all frames; the data thresholds of
+ * divide_and_truncate are computed once per b200rt_batch_run call.  Projectors passed to
  * add_frame must outlive the batch and are not used concurrently by the caller while it runs. */
 typedef struct b200rt_batch b200rt_batch;
 

@@ -1625,6 +1625,9 @@ struct b200rt_batch {
   std::map<std::vector<int>, std::unique_ptr<DevBuf<b200::BatchItem>>> items;
   std::map<std::vector<int>, int> item_counts;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  // per batched sub-iteration: the update arguments of its frames (device table), their count, the most blocks
+  std::map<int, std::unique_ptr<DevBuf<b200::BatchUpdateDev>>> updates;
+  std::map<int, std::pair<int, int>> update_counts;
   cudaStream_t capture_stream = nullptr;
 };
 
@@ -1685,6 +1688,10 @@ void batch_finalize(b200rt_batch& b) {
     for (int s = 0; s < f.nsub; ++s) {
       int nv = 0;
       subset_views(*f.h, s, f.nsub, nv);  // cached device view lists, uploaded now
+    }
+    {
+      int nv = 0;
+      subset_views(*f.h, 0, 1, nv);  // all views, for the thresholds
     }
     BatchFrameDev d{};
     d.geom = f.geom;
@@ -1767,18 +1774,28 @@ int grid_of(const b200rt_batch& b, int per_sm, int max_per_sm) {
   return c * b.num_sms;
 }
 
-void batch_thresholds(b200rt_batch& b, int k, cudaStream_t st) {
+// divide_and_truncate's threshold of every viewgram of every frame taking part in sub-iterations first.. (it
+// depends on the data only, so once per run covers all the run's subsets)
+void batch_thresholds(b200rt_batch& b, int first, cudaStream_t st) {
   for (auto& fp : b.frames) {
     auto& f = *fp;
-    if (k > f.num_subiters) continue;
+    if (first > f.num_subiters) continue;
     const b200::Geometry& g = *f.h->geo;
     int nv = 0;
-    const int* views = subset_views(*f.h, frame_subset(f, k), f.nsub, nv);
+    const int* views = subset_views(*f.h, 0, 1, nv);
     ck(launch_viewgram_small_values(f.y, f.h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, f.zero_ends,
                                     g.num_tof(), g.tof_stride(), f.small_value.p, st),
        "viewgram thresholds");
+  }
+}
+
+// zero the numerators and cancelled counts of the frames taking part in sub-iteration k
+void batch_zero(b200rt_batch& b, int k, cudaStream_t st) {
+  for (auto& fp : b.frames) {
+    auto& f = *fp;
+    if (k > f.num_subiters) continue;
     ck(cudaMemsetAsync(f.cancelled.p, 0, sizeof(unsigned int), st), "memset");
-    ck(cudaMemsetAsync(f.u.p, 0, sizeof(float) * g.image_size(), st), "memset");
+    ck(cudaMemsetAsync(f.u.p, 0, sizeof(float) * f.h->geo->image_size(), st), "memset");
   }
 }
 
@@ -1802,18 +1819,44 @@ void batch_projections(b200rt_batch& b, int k, cudaStream_t st) {
   ck(batch_launch(b, 1, items, n, grid_of(b, b.cfg.ctas_per_sm_back, b.max_back), st), "batched back projection");
 }
 
-void batch_subiteration(b200rt_batch& b, int k, cudaStream_t st) {
-  batch_thresholds(b, k, st);
-  batch_projections(b, k, st);
+// the update arguments of the frames taking part in sub-iteration k, uploaded on first use
+const b200::BatchUpdateDev* batch_updates(b200rt_batch& b, int k, int& count, int& max_blocks) {
+  auto it = b.updates.find(k);
+  if (it != b.updates.end()) {
+    count = b.update_counts[k].first;
+    max_blocks = b.update_counts[k].second;
+    return it->second->p;
+  }
+  std::vector<b200::BatchUpdateDev> v;
+  max_blocks = 1;
   for (auto& fp : b.frames) {
     auto& f = *fp;
     if (k > f.num_subiters) continue;
     const b200::Geometry& g = *f.h->geo;
-    ck(launch_update(f.u.p, f.x, f.sens[frame_subset(f, k)], f.has_prior ? f.grad.p : nullptr,
-                     f.has_prior ? &f.prior : nullptr, f.prior_w, f.nsub, k, f.min_rel, f.max_rel, g.desc().ny,
-                     g.desc().nx, g.desc().nz, f.partial_max.p, f.umax.p, st),
-       "update");
+    b200::BatchUpdateDev d;
+    b200::fill_batch_update(d, f.u.p, f.x, f.sens[frame_subset(f, k)], f.has_prior ? f.grad.p : nullptr,
+                            f.has_prior ? &f.prior : nullptr, f.prior_w, f.nsub, k, f.min_rel, f.max_rel, g.desc().ny,
+                            g.desc().nx, g.desc().nz, f.partial_max.p, f.umax.p);
+    max_blocks = std::max(max_blocks, d.nblocks);
+    v.push_back(d);
   }
+  auto buf = std::make_unique<DevBuf<b200::BatchUpdateDev>>();
+  buf->upload(v, b.capture_stream);
+  ck(cudaStreamSynchronize(b.capture_stream), "batch updates");
+  count = static_cast<int>(v.size());
+  b.update_counts[k] = {count, max_blocks};
+  const b200::BatchUpdateDev* p = buf->p;
+  b.updates[k] = std::move(buf);
+  return p;
+}
+
+void batch_subiteration(b200rt_batch& b, int k, cudaStream_t st) {
+  batch_zero(b, k, st);
+  batch_projections(b, k, st);
+  // every frame's update (OSMAPOSLReconstruction.cxx:394-510) in three launches
+  int n = 0, max_blocks = 1;
+  const b200::BatchUpdateDev* upd = batch_updates(b, k, n, max_blocks);
+  ck(b200::launch_batch_update(upd, n, max_blocks, st), "update");
 }
 
 }  // namespace
@@ -1845,6 +1888,8 @@ void b200rt_batch_destroy(b200rt_batch* b) {
     cudaDeviceSynchronize();  // graphs may still run on a caller's stream
     drop_graphs(*b);
     b->items.clear();
+    b->updates.clear();
+    b->update_counts.clear();
     b->frames.clear();
     b->d_geoms.release();
     b->d_pgeoms.release();
@@ -1897,6 +1942,8 @@ int b200rt_batch_add_frame(b200rt_batch* b, b200rt_projector* h, float* estimate
     f->max_rel = max_relative_change;
     drop_graphs(*b);
     b->items.clear();
+    b->updates.clear();
+    b->update_counts.clear();
     b->item_counts.clear();
     b->ready = false;
     b->frames.push_back(std::move(f));
@@ -1918,8 +1965,11 @@ int b200rt_batch_run(b200rt_batch* b, int first_subiteration, int count, int use
     for (int k = first_subiteration; k < first_subiteration + count; ++k) {
       int n = 0;
       batch_items(*b, k, b->cfg.order, n);  // uploads happen here, never inside a capture
+      int nu = 0, mb = 0;
+      batch_updates(*b, k, nu, mb);
     }
     if (!use_graph) {
+      batch_thresholds(*b, first_subiteration, st);
       for (int k = first_subiteration; k < first_subiteration + count; ++k) batch_subiteration(*b, k, st);
       return B200RT_OK;
     }
@@ -1929,6 +1979,7 @@ int b200rt_batch_run(b200rt_batch* b, int first_subiteration, int count, int use
       cudaStream_t cs = b->capture_stream;
       ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
       try {
+        batch_thresholds(*b, first_subiteration, cs);
         for (int k = first_subiteration; k < first_subiteration + count; ++k) batch_subiteration(*b, k, cs);
       } catch (...) {
         cudaGraph_t g = nullptr;
@@ -1962,7 +2013,8 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
     const cudaStream_t st = b->capture_stream;
     ck(cudaEventCreate(&e0), "cudaEventCreate");
     ck(cudaEventCreate(&e1), "cudaEventCreate");
-    batch_thresholds(*b, subiteration, st);  // the forward epilogue reads them; numerators are scratch
+    batch_thresholds(*b, subiteration, st);  // the forward epilogue reads them
+    batch_zero(*b, subiteration, st);        // numerators are scratch
     // time one launch of one direction: the best of two after a warm-up
     auto time_launch = [&](int dir, const BatchItem* items, int n, int grid) {
       float t = 1e30f;

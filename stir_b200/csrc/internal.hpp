@@ -248,6 +248,32 @@ cudaError_t launch_back_batch_paths(const ProjParams* geoms, const PathParams* p
                                     int grid, cudaStream_t st);
 int batch_paths_max_ctas_per_sm(int npa, int smem_bytes, bool forward);
 
+// One frame's OSMAPOSL update in a batched update launch (the arguments of launch_update)
+struct BatchUpdateDev {
+  float* u;
+  float* x;
+  const float* sens;
+  float* g;
+  int prior_type;
+  float beta, gamma, epsilon;
+  int dzmin, dzmax;
+  float w[27];
+  const float* kappa;
+  int ny, nx, nz;
+  int nblocks;
+  float* partial_max;
+  float* umax;
+  int prior, map_model;
+  float num_subsets, small_num;
+  int clamp;
+  float min_rel, max_rel;
+};
+void fill_batch_update(BatchUpdateDev& d, float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
+                       const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
+                       int ny, int nx, int nz, float* partial_max, float* umax);
+// the updates of several frames: three launches (grid.y = frame), max_blocks = the largest nblocks
+cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, cudaStream_t st);
+
 // launchers (project.cu)
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,
                            cudaStream_t st, const FwdEpilogue* ep = nullptr);

@@ -56,6 +56,17 @@ struct PriorDev {
   const float* kappa;
 };
 
+__device__ __forceinline__ void prior_dev_from(const BatchUpdateDev& f, PriorDev& pr) {
+  pr.type = f.prior_type;
+  pr.beta = f.beta;
+  pr.gamma = f.gamma;
+  pr.epsilon = f.epsilon;
+  pr.dzmin = f.dzmin;
+  pr.dzmax = f.dzmax;
+  for (int k = 0; k < 27; ++k) pr.w[k] = f.w[k];
+  pr.kappa = f.kappa;
+}
+
 // RelativeDifferencePrior::derivative_10 (RelativeDifferencePrior.cxx:287-300)
 __device__ __forceinline__ float rdp_derivative_10(float x, float y, float gamma, float epsilon) {
   if (epsilon == 0.0f && x == 0 && y == 0) return 0.f;
@@ -87,12 +98,12 @@ __device__ __forceinline__ float prior_gradient_at(const float* __restrict__ x, 
 }
 
 // pass 1: per-block max of the update image u, and the prior gradient (if any) into g
-__global__ void update_prepare_kernel(const float* __restrict__ u, const float* __restrict__ x, float* __restrict__ g, PriorDev pr,
-                                      int ny, int nx, int nz, float* __restrict__ partial_max) {
+__device__ __forceinline__ void update_prepare_body(int blk, int nblk, const float* __restrict__ u,
+                                                    const float* __restrict__ x, float* __restrict__ g, const PriorDev& pr,
+                                                    int ny, int nx, int nz, float* __restrict__ partial_max) {
   const int64_t n = static_cast<int64_t>(ny) * nx * nz;
   float m = -INFINITY;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  for (int64_t i = blk * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<int64_t>(nblk) * blockDim.x) {
     m = fmaxf(m, u[i]);
     if (pr.type != 0) {
       const int zi = static_cast<int>(i % nz);
@@ -108,11 +119,16 @@ __global__ void update_prepare_kernel(const float* __restrict__ u, const float* 
   if (threadIdx.x < 32) {
     m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
     m = warp_max(m);
-    if (threadIdx.x == 0) partial_max[blockIdx.x] = m;
+    if (threadIdx.x == 0) partial_max[blk] = m;
   }
 }
 
-__global__ void reduce_max_kernel(const float* __restrict__ partial, int n, float* __restrict__ out) {
+__global__ void update_prepare_kernel(const float* __restrict__ u, const float* __restrict__ x, float* __restrict__ g, PriorDev pr,
+                                      int ny, int nx, int nz, float* __restrict__ partial_max) {
+  update_prepare_body(blockIdx.x, gridDim.x, u, x, g, pr, ny, nx, nz, partial_max);
+}
+
+__device__ __forceinline__ void reduce_max_body(const float* __restrict__ partial, int n, float* __restrict__ out) {
   float m = -INFINITY;
   for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, partial[i]);
   __shared__ float red[32];
@@ -126,15 +142,18 @@ __global__ void reduce_max_kernel(const float* __restrict__ partial, int n, floa
   }
 }
 
+__global__ void reduce_max_kernel(const float* __restrict__ partial, int n, float* __restrict__ out) {
+  reduce_max_body(partial, n, out);
+}
+
 // pass 2: u /= denominator with divide()'s threshold, clamp, x *= u
-__global__ void update_apply_kernel(float* __restrict__ u, float* __restrict__ x, const float* __restrict__ sens,
-                                    const float* __restrict__ g, int prior, int map_model, float num_subsets,
-                                    const float* __restrict__ umax, float small_num, int clamp, float min_rel, float max_rel,
-                                    int64_t n) {
+__device__ __forceinline__ void update_apply_body(int blk, int nblk, float* __restrict__ u, float* __restrict__ x,
+                                                  const float* __restrict__ sens, const float* __restrict__ g, int prior,
+                                                  int map_model, float num_subsets, const float* __restrict__ umax,
+                                                  float small_num, int clamp, float min_rel, float max_rel, int64_t n) {
   float sv = *umax * small_num;
   sv = sv > 0 ? sv : 0;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  for (int64_t i = blk * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<int64_t>(nblk) * blockDim.x) {
     const float s = sens[i];
     float den;
     if (!prior) {
@@ -164,6 +183,34 @@ __global__ void update_apply_kernel(float* __restrict__ u, float* __restrict__ x
     u[i] = v;
     x[i] *= v;
   }
+}
+
+__global__ void update_apply_kernel(float* __restrict__ u, float* __restrict__ x, const float* __restrict__ sens,
+                                    const float* __restrict__ g, int prior, int map_model, float num_subsets,
+                                    const float* __restrict__ umax, float small_num, int clamp, float min_rel, float max_rel,
+                                    int64_t n) {
+  update_apply_body(blockIdx.x, gridDim.x, u, x, sens, g, prior, map_model, num_subsets, umax, small_num, clamp, min_rel,
+                    max_rel, n);
+}
+
+// the same three passes for several frames in one launch each (grid.y = frame); every frame keeps the block
+// count of its own launch, so the results are those of launch_update frame by frame
+__global__ void batch_update_prepare_kernel(const BatchUpdateDev* __restrict__ frames) {
+  const BatchUpdateDev& f = frames[blockIdx.y];
+  if (static_cast<int>(blockIdx.x) >= f.nblocks) return;
+  PriorDev pr;
+  prior_dev_from(f, pr);
+  update_prepare_body(blockIdx.x, f.nblocks, f.u, f.x, f.g, pr, f.ny, f.nx, f.nz, f.partial_max);
+}
+__global__ void batch_reduce_max_kernel(const BatchUpdateDev* __restrict__ frames) {
+  const BatchUpdateDev& f = frames[blockIdx.x];
+  reduce_max_body(f.partial_max, f.nblocks, f.umax);
+}
+__global__ void batch_update_apply_kernel(const BatchUpdateDev* __restrict__ frames) {
+  const BatchUpdateDev& f = frames[blockIdx.y];
+  if (static_cast<int>(blockIdx.x) >= f.nblocks) return;
+  update_apply_body(blockIdx.x, f.nblocks, f.u, f.x, f.sens, f.g, f.prior, f.map_model, f.num_subsets, f.umax,
+                    f.small_num, f.clamp, f.min_rel, f.max_rel, static_cast<int64_t>(f.ny) * f.nx * f.nz);
 }
 
 __global__ void reduce_sum_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
@@ -640,6 +687,52 @@ cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const
   update_apply_kernel<<<blocks, 256, 0, st>>>(u, x, sens, g, has_prior ? 1 : 0, has_prior ? prior->map_model : 0,
                                                static_cast<float>(num_subsets), umax, has_prior ? 0.000001F : 0.F,
                                                subiteration_num != 1, min_rel, max_rel, n);
+  return cudaGetLastError();
+}
+
+void fill_batch_update(BatchUpdateDev& d, float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
+                       const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
+                       int ny, int nx, int nz, float* partial_max, float* umax) {
+  d = BatchUpdateDev{};
+  const bool has_prior = prior && prior->type != B200RT_PRIOR_NONE && prior->penalisation_factor != 0;
+  d.u = u;
+  d.x = x;
+  d.sens = sens;
+  d.g = has_prior ? g : nullptr;
+  d.prior_type = has_prior ? prior->type : 0;
+  if (has_prior) {
+    d.beta = prior->penalisation_factor;
+    d.gamma = prior->gamma;
+    d.epsilon = prior->epsilon;
+    d.dzmin = prior->only_2D ? 0 : -1;
+    d.dzmax = prior->only_2D ? 0 : 1;
+    for (int k = 0; k < 27; ++k) d.w[k] = prior_weights[k];
+    d.kappa = prior->kappa_dev;
+  }
+  d.ny = ny;
+  d.nx = nx;
+  d.nz = nz;
+  d.nblocks = update_num_blocks(static_cast<int64_t>(ny) * nx * nz);
+  d.partial_max = partial_max;
+  d.umax = umax;
+  d.prior = has_prior ? 1 : 0;
+  d.map_model = has_prior ? prior->map_model : 0;
+  d.num_subsets = static_cast<float>(num_subsets);
+  d.small_num = has_prior ? 0.000001F : 0.F;
+  d.clamp = subiteration_num != 1;
+  d.min_rel = min_rel;
+  d.max_rel = max_rel;
+}
+
+cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, cudaStream_t st) {
+  if (nframes <= 0) return cudaSuccess;
+  batch_update_prepare_kernel<<<dim3(max_blocks, nframes), 256, 0, st>>>(frames_dev);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  batch_reduce_max_kernel<<<nframes, 1024, 0, st>>>(frames_dev);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  batch_update_apply_kernel<<<dim3(max_blocks, nframes), 256, 0, st>>>(frames_dev);
   return cudaGetLastError();
 }
 

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -161,7 +162,6 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   if (g.num_tof() != 1 || nz < 1) return;
   int nax_max = 1;
   for (int sg = -g.S(); sg <= g.S(); ++sg) nax_max = std::max(nax_max, g.nax(sg));
-  const int K = std::max(8, 32768 / (4 * nz));  // 32 KB of staged float columns
   const int ngroups = nviews * ntangs;
 
   struct Group {
@@ -172,6 +172,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
     std::vector<int> member_chunk;    // per segment: first chunk-table entry (relative)
     std::vector<PathCElem> cmaj;      // the elements in column order: slot, member, z
     std::vector<int> col_starts;      // first element of each column in cmaj, ncols + 1 entries
+    int over = 0;                     // how far (planes) a forward pass reads outside [0, nz): the staging's padding
     bool ok = true;
   };
   std::vector<Group> groups(ngroups);
@@ -194,7 +195,6 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
         }
         G.cols = keys;
         const int ncols = static_cast<int>(keys.size());
-        const int nch = (ncols + K - 1) / K;
         for (int si = 0; si < nsegs; ++si) {
           const ProjBinDev& pb = h.h_bins[(static_cast<size_t>(vi) * nsegs + si) * ntangs + ti];
           tmp.clear();
@@ -208,18 +208,26 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
           std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<uint64_t, float>& a,
                                                       const std::pair<uint64_t, float>& b) { return a.first < b.first; });
           G.member_off.push_back(static_cast<int64_t>(G.elems.size()));
-          G.member_chunk.push_back(static_cast<int>(G.chunks.size()));
           for (const auto& t : tmp) {
             const uint32_t slot = static_cast<uint32_t>(t.first >> 32);
             const uint32_t zb = static_cast<uint32_t>((t.first >> 16) & 0xffffu);
             G.elems.push_back(PathElem{slot | (zb << 16), t.second});
           }
-          // chunk c covers the elements with slot in [c K, (c + 1) K)
-          size_t k = 0;
-          for (int c = 0; c <= nch; ++c) {
-            const uint32_t lim = static_cast<uint32_t>(std::min(c * K, ncols));
-            while (k < tmp.size() && (tmp[k].first >> 32) < lim) ++k;
-            G.chunks.push_back(static_cast<int>(k));
+          // the planes a forward pass of each of the bin's lines reads for these elements
+          for (int l = 0; l < pb.num_lines; ++l) {
+            const LineDev& L = lines[pb.first_line + l];
+            const int nax = g.nax(L.seg), npa = g.npa(L.seg);
+            for (const auto& t : tmp) {
+              const int z = static_cast<int>((t.first >> 16) & 0xffffu) - 512;
+              const int zt = ((L.flags & 8) ? L.q - z : z) - p.min_z;
+              for (int a0 = 0; a0 < nax; a0 += 128) {
+                const int lo = zt + a0 * npa, hi = zt + (std::min(nax - a0, 128) + a0 - 1) * npa;
+                if (hi < 0 || lo > nz - 1)
+                  G.over = std::numeric_limits<int>::max();  // a window outside the image: no padded staging
+                else
+                  G.over = std::max(G.over, std::max(-lo, hi - (nz - 1)));
+              }
+            }
           }
         }
         // the same elements in column order (slot, then member, then z) for the back projection
@@ -250,8 +258,31 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
     pool.emplace_back(work, g0, g1);
   }
   for (auto& th : pool) th.join();
-  for (const Group& G : groups)
+  int over = 0;
+  for (const Group& G : groups) {
     if (!G.ok) return;
+    over = std::max(over, G.over);
+  }
+  // padded staging: zero planes between the staged columns cover every pass's reads outside [0, nz), so
+  // the forward needs no per-lane range tests (a cap keeps the staging buffer small)
+  const int zpad = over <= 64 ? (over + 3) & ~3 : -1;
+  const int K = std::max(8, 32768 / (4 * (nz + std::max(zpad, 0))));  // 32 KB of staged float columns
+  // chunk c of a row covers its elements with slot in [c K, (c + 1) K)
+  for (Group& G : groups) {
+    const int ncols = static_cast<int>(G.cols.size());
+    const int nch = (ncols + K - 1) / K;
+    for (size_t m = 0; m < G.member_off.size(); ++m) {
+      const size_t b0 = static_cast<size_t>(G.member_off[m]);
+      const size_t b1 = m + 1 < G.member_off.size() ? static_cast<size_t>(G.member_off[m + 1]) : G.elems.size();
+      G.member_chunk.push_back(static_cast<int>(G.chunks.size()));
+      size_t k = b0;
+      for (int c = 0; c <= nch; ++c) {
+        const uint32_t lim = static_cast<uint32_t>(std::min(c * K, ncols));
+        while (k < b1 && (G.elems[k].sz & 0xffffu) < lim) ++k;
+        G.chunks.push_back(static_cast<int>(k - b0));
+      }
+    }
+  }
 
   std::vector<PathElem> elems;
   std::vector<PathCElem> cmaj;
@@ -317,7 +348,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
       const int c1 = m + 1 < G.member_chunk.size() ? G.member_chunk[m + 1] : static_cast<int>(G.chunks.size());
       for (int c = G.member_chunk[m]; c + 1 < c1; ++c) max_chunk = std::max(max_chunk, G.chunks[c + 1] - G.chunks[c]);
     }
-  if (path_smem_fwd(K, nz, max_lines, max_acc, npa_max).total > 200 * 1024 ||
+  if (path_smem_fwd(K, nz, zpad, max_lines, max_acc, npa_max).total > 200 * 1024 ||
       path_smem_back(nz, max_lines, nsegs, nax_max, npa_max).total > 200 * 1024)
     return;
 
@@ -344,6 +375,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   pp.col_starts = h.path_col_starts.p;
   pp.max_members = nsegs;
   pp.max_acc = max_acc;
+  pp.zpad = zpad;
   h.h_item_view = item_view;
   h.h_path_items = items;
   h.use_paths = true;
@@ -1668,7 +1700,8 @@ void batch_finalize(b200rt_batch& b) {
     for (auto* h : b.geoms) {
       const b200::PathParams& pp = h->pparams;
       pg.push_back(pp);
-      b.smem_f = std::max(b.smem_f, b200::path_smem_fwd(pp.K, h->params.nz, pp.max_lines, pp.max_acc, pp.npa_max).total);
+      b.smem_f = std::max(b.smem_f, b200::path_smem_fwd(pp.K, h->params.nz, pp.zpad, pp.max_lines, pp.max_acc,
+                                                          pp.npa_max).total);
       b.smem_b = std::max(b.smem_b, b200::path_smem_back(h->params.nz, pp.max_lines, pp.max_members, pp.nax_max,
                                                           pp.npa_max).total);
     }

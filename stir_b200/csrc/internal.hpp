@@ -163,6 +163,8 @@ struct PathParams {
   const int* col_starts;  // per path: first element of each column in cmaj (relative), ncols + 1 entries
   int max_members;        // basic bins per path (basic segments)
   int max_acc;            // forward accumulators of the largest item: path_parts(lines) x sum of the lines' nax
+  int zpad;               // >= 0: the staged columns are nz + zpad apart with zeros between them, enough for every
+                          // forward pass to read all its planes without range tests; -1: tests per lane
 };
 
 // parts each line's elements are split into (forward): an item's lines are processed in pairs (the two
@@ -203,9 +205,13 @@ __host__ __device__ inline int path_dl_len(int nz, int nax_max, int npa_max) {
 struct PathSmemFwd {
   int colbase, lines, pairs, rowoff, xbuf, acc, total;
 };
-__host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int max_lines, int max_acc, int npa_max) {
+// staged column ci, plane z at ci * path_col_stride + path_col_offset + z
+__host__ __device__ inline int path_col_stride(int nz, int zpad) { return zpad >= 0 ? nz + zpad : nz; }
+__host__ __device__ inline int path_col_offset(int zpad) { return zpad > 0 ? zpad : 0; }
+__host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int zpad, int max_lines, int max_acc, int npa_max) {
   PathSmemFwd s;
-  s.colbase = path_align16((K * nz + 128 * npa_max) * 4);  // staged columns and a pass's overshoot
+  // staged columns (with the padding below the first and above the last) and a pass's overshoot
+  s.colbase = path_align16((K * path_col_stride(nz, zpad) + 2 * path_col_offset(zpad) + 128 * npa_max) * 4);
   s.lines = path_align16(s.colbase + K * 4);
   s.pairs = path_align16(s.lines + max_lines * static_cast<int>(sizeof(PathLineSmem)));
   s.rowoff = path_align16(s.pairs + max_lines * 8);

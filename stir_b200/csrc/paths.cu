@@ -103,10 +103,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_al
 // One pass of one unit over elements [e0, e1) of its row: NJ groups of 32 axial positions from a0.
 // The warp's lanes transform 32 elements at a time (column slot -> staged index, z reflection) into
 // the warp's buffer; then every element costs one broadcast read and NJ shared loads and FMAs.
-template <int NPA, int NJ, bool TWO>
+template <int NPA, int NJ, bool TWO, bool PADDED>
 __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int e0, int e1, int c0, const float* cols,
-                                            int nz, const PathLineSmem& L1, const PathLineSmem& L2, int a0, int nact,
-                                            int lane, float* acc_row1, float* acc_row2, PathXElem* xb) {
+                                            int nz, int cstride, int coff, const PathLineSmem& L1,
+                                            const PathLineSmem& L2, int a0, int nact, int lane, float* acc_row1,
+                                            float* acc_row2, PathXElem* xb) {
   const int npa = NPA ? NPA : L1.npa;
   // lane's plane offset of group j: zo0 + 32 j npa.  In the full path inactive lanes (axial positions past
   // the line's end) read up to 127 npa floats past the staged columns, into the padding of the staging
@@ -134,10 +135,10 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
       const int f1 = (zt1 + zlo >= 0) && (zt1 + zhi < nz);
       const int f2 = TWO ? ((zt2 + zlo >= 0) && (zt2 + zhi < nz)) : 1;
       PathXElem x;
-      x.base = sl * nz + zt1;
-      x.zt = sl * nz + zt2;
+      x.base = sl * cstride + coff + zt1;
+      x.zt = sl * cstride + coff + zt2;
       x.v = m.v;
-      x.full = sl | ((f1 & f2) << 30);
+      x.full = sl | ((PADDED ? 1 : (f1 & f2)) << 30);
       xb[lane] = x;
     }
     __syncwarp();
@@ -145,14 +146,14 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
       const PathXElem e = xb[i];
       const float* q1 = cols + (e.base + zo0);
       const float* q2 = cols + (e.zt + zo0);
-      if (e.full >> 30) {
+      if (PADDED || (e.full >> 30)) {
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
           acc1[j] += q1[j * 32 * npa] * e.v;
           if (TWO) acc2[j] += q2[j * 32 * npa] * e.v;
         }
       } else {
-        const int sb = (e.full & 0xffff) * nz;  // column start in the staging buffer
+        const int sb = (e.full & 0xffff) * cstride + coff;  // column start in the staging buffer
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
           const int zz1 = e.base - sb + zo0 + j * 32 * npa;
@@ -190,6 +191,11 @@ __device__ __forceinline__ int pair_lines(const PathLineSmem* ls, int nl, int2* 
   return n;
 }
 
+// one gather pass, with the padded staging or with per-lane range tests
+#define GATHER(NJ, TWO, LA, LB, ...)                                                                             \
+  (pp.zpad >= 0 ? gather_pass<NPA, NJ, TWO, true>(E, e0, e1, c0, cols, nz, cstride, coff, LA, LB, __VA_ARGS__)   \
+                : gather_pass<NPA, NJ, TWO, false>(E, e0, e1, c0, cols, nz, cstride, coff, LA, LB, __VA_ARGS__))
+
 template <int NPA, int EPI>
 __device__ __forceinline__ void forward_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
                                                   unsigned char* smem, const float* __restrict__ img,
@@ -197,7 +203,8 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
                                                   unsigned& ncancel) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nz = p.nz;
-  const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.max_lines, pp.max_acc, pp.npa_max);
+  const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.zpad, pp.max_lines, pp.max_acc, pp.npa_max);
+  const int cstride = path_col_stride(nz, pp.zpad), coff = path_col_offset(pp.zpad);
   float* cols = reinterpret_cast<float*>(smem);
   int* colbase = reinterpret_cast<int*>(smem + lay.colbase);
   PathLineSmem* ls = reinterpret_cast<PathLineSmem*>(smem + lay.lines);
@@ -223,6 +230,9 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
   __syncthreads();
   const int U = s_npairs * P;
   for (int i = threadIdx.x; i < s_nacc; i += blockDim.x) lacc[i] = 0.f;
+  // the staging buffer starts as zeros: with padded staging the planes between the columns stay zero
+  if (pp.zpad > 0)
+    for (int i = threadIdx.x; i < lay.colbase / 4; i += blockDim.x) cols[i] = 0.f;
   const int nch = (it.ncols + pp.K - 1) / pp.K;
   for (int c = 0; c < nch; ++c) {
     const int c0 = c * pp.K, kc = min(pp.K, it.ncols - c0);
@@ -231,7 +241,7 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
     __syncthreads();
     for (int ci = warp; ci < kc; ci += kPathWarps) {
       const int b = colbase[ci];
-      float* dst = cols + ci * nz;
+      float* dst = cols + ci * cstride + coff;
       if (b >= 0) {
         for (int z = lane; z < nz; z += 32) cp_async4(dst + z, img + b + z);
       } else {
@@ -255,20 +265,20 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
         for (int a0 = 0; a0 < L1.nax; a0 += 128) {
           const int nact = min(L1.nax - a0, 128);
           switch ((nact + 31) >> 5) {
-            case 1: gather_pass<NPA, 1, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
-            case 2: gather_pass<NPA, 2, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
-            case 3: gather_pass<NPA, 3, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
-            default: gather_pass<NPA, 4, true>(E, e0, e1, c0, cols, nz, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            case 1: GATHER(1, true, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            case 2: GATHER(2, true, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            case 3: GATHER(3, true, L1, L2, a0, nact, lane, row1, row2, xb); break;
+            default: GATHER(4, true, L1, L2, a0, nact, lane, row1, row2, xb); break;
           }
         }
       } else {
         for (int a0 = 0; a0 < L1.nax; a0 += 128) {
           const int nact = min(L1.nax - a0, 128);
           switch ((nact + 31) >> 5) {
-            case 1: gather_pass<NPA, 1, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
-            case 2: gather_pass<NPA, 2, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
-            case 3: gather_pass<NPA, 3, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
-            default: gather_pass<NPA, 4, false>(E, e0, e1, c0, cols, nz, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            case 1: GATHER(1, false, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            case 2: GATHER(2, false, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            case 3: GATHER(3, false, L1, L1, a0, nact, lane, row1, row1, xb); break;
+            default: GATHER(4, false, L1, L1, a0, nact, lane, row1, row1, xb); break;
           }
         }
       }
@@ -542,7 +552,7 @@ cudaError_t launch_path(K kernel, int nitems, int smem_bytes, cudaStream_t st, A
 template <int EPI>
 cudaError_t launch_forward_paths_epi(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* image,
                                      float* out, cudaStream_t st, const FwdEpilogue& ep) {
-  const int sm = path_smem_fwd(pp.K, p.nz, pp.max_lines, pp.max_acc, pp.npa_max).total;
+  const int sm = path_smem_fwd(pp.K, p.nz, pp.zpad, pp.max_lines, pp.max_acc, pp.npa_max).total;
   switch (p.uniform_npa) {
     case 1: return launch_path(forward_paths_kernel<1, EPI>, n, sm, st, p, pp, list, image, out, ep);
     case 2: return launch_path(forward_paths_kernel<2, EPI>, n, sm, st, p, pp, list, image, out, ep);

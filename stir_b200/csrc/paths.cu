@@ -325,8 +325,10 @@ struct FixedCols {
   }
 };
 
-// planes [zp, zp + 128) of one column: elements [k0, k1) of the path in column order
-template <typename Cols>
+// planes [zp, zp + 128) of one column: elements [k0, k1) of the path in column order.  HIT: every window of
+// every (element, line) meets the image (checked at set-up, PathParams::zpad >= 0), so no window test is needed
+// (an inactive line's data are all zero)
+template <typename Cols, bool HIT>
 __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int k0, int k1, const int4* lz,
                                             const int2* members, const float* dl, int zp, int nz, int lane, int b,
                                             const Cols& acc) {
@@ -346,7 +348,7 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
         const int4 L = lz[l];  // (z sign, z offset, window length, data offset)
         int zt = L.x * zr + L.y;
         // a window that misses the image (or an inactive line) reads the zero padding [0, F)
-        if (!(zt < nz && zt + L.z >= 0)) zt = zp + 128 + nz;
+        if (!HIT && !(zt < nz && zt + L.z >= 0)) zt = zp + 128 + nz;
         const float* q = dl + (L.w + zp + lane - zt);
 #pragma unroll
         for (int j = 0; j < 4; ++j) sum[j] += acc.term(v * q[32 * j]);
@@ -417,7 +419,12 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
     const int yi = (swap ? x : y) * sy - p.min_y;
     const int b = (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * nz : -1;
     const int k0 = __ldg(cs + ci), k1 = __ldg(cs + ci + 1);
-    for (int zp = 0; zp < nz; zp += 128) back_column<Cols>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+    for (int zp = 0; zp < nz; zp += 128) {
+      if (pp.zpad >= 0)
+        back_column<Cols, true>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+      else
+        back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+    }
   }
 }
 

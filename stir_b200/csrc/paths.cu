@@ -344,7 +344,7 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
       const float v = __shfl_sync(0xffffffffu, mine.v, i);
       const int zr = static_cast<int>(mz & 0xffffu);
       const int2 mem = members[mz >> 16];  // (first line, number of lines) of the element's basic bin
-      for (int l = mem.x; l < mem.x + mem.y; ++l) {
+      auto line = [&](int l) {
         const int4 L = lz[l];  // (z sign, z offset, window length, data offset)
         int zt = L.x * zr + L.y;
         // a window that misses the image (or an inactive line) reads the zero padding [0, F)
@@ -352,7 +352,11 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
         const float* q = dl + (L.w + zp + lane - zt);
 #pragma unroll
         for (int j = 0; j < 4; ++j) sum[j] += acc.term(v * q[32 * j]);
-      }
+      };
+      // a basic bin's lines are usually its two z orientations
+      if (mem.y > 0) line(mem.x);
+      if (mem.y > 1) line(mem.x + 1);
+      for (int l = mem.x + 2; l < mem.x + mem.y; ++l) line(l);
     }
   }
   if (b < 0) return;

@@ -348,6 +348,61 @@ int b200rt_batch_get_config(const b200rt_batch* b, b200rt_batch_config* out);
 /* cancelled singularities of one frame in the last batched sub-iteration it took part in; synchronises */
 int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out);
 
+/* ---- Gibbs penalties on device-resident images ---------------------------
+ * GibbsQuadraticPenalty and GibbsRelativeDifferencePenalty (src/include/stir/recon_buildblock/GibbsPenalty.h,
+ * GibbsPenalty.inl, GibbsQuadraticPenalty.h, GibbsRelativeDifferencePenalty.h) and their CUDA versions
+ * CudaGibbsQuadraticPenalty / CudaGibbsRelativeDifferencePenalty (CUDA/CudaGibbsPenalty.h, .cuh), which copy
+ * every image to and from the GPU per call: here the penalty is set up once (b200rt_gibbs_create replaces
+ * set_up: weights, kappa, image size) and every operation reads and writes device images.  Each voxel's sum is
+ * taken in the reference's types and order (GibbsPenalty.inl); scalars are reduced in a fixed order. */
+#define B200RT_GIBBS_QUADRATIC 1
+#define B200RT_GIBBS_RELATIVE_DIFFERENCE 2
+#define B200RT_LAYOUT_DEVICE 0 /* [y][x][z], z fastest: the layout of the *_dev projector entry points */
+#define B200RT_LAYOUT_STIR 1   /* [z][y][x], x fastest: STIR's Array<3,float> order */
+
+typedef struct b200rt_gibbs_params {
+  int32_t potential;          /* B200RT_GIBBS_*                                                    */
+  float penalisation_factor;  /* beta                                                               */
+  float gamma;                /* Relative Difference "gamma value" (STIR default 2)                 */
+  float epsilon;              /* Relative Difference "epsilon value" (STIR default 1e-7)            */
+  int32_t nz, ny, nx;         /* image size                                                         */
+  int32_t layout;             /* B200RT_LAYOUT_*                                                    */
+  float voxel_size_z, voxel_size_y, voxel_size_x; /* mm, for the default weights                    */
+  int32_t only_2D;            /* default weights in the plane only (1x3x3)                          */
+  int32_t weights_z, weights_y, weights_x; /* sizes of `weights`, 1..7 each (0 with weights NULL)   */
+  const float* weights;       /* host [z][y][x], indices -(size/2)..size-1-size/2; NULL: default    */
+                              /* weights, x voxel size / distance (compute_default_weights)         */
+  const float* kappa_dev;     /* kappa image on the device in `layout`, or NULL (kappa = 1)         */
+} b200rt_gibbs_params;
+
+typedef struct b200rt_gibbs b200rt_gibbs;
+
+/* set_up: validates the parameters, copies the weights; on failure *out = NULL and b200rt_last_error(NULL)
+ * says why. */
+int b200rt_gibbs_create(const b200rt_gibbs_params* params, int device, b200rt_gibbs** out);
+void b200rt_gibbs_destroy(b200rt_gibbs* g);
+const char* b200rt_gibbs_last_error(const b200rt_gibbs* g);
+/* get_weights: sizes[3] = (z, y, x); w receives sizes[0]*sizes[1]*sizes[2] floats (may be NULL) */
+int b200rt_gibbs_get_weights(const b200rt_gibbs* g, float* w, int32_t sizes[3]);
+/* set_kappa_sptr: a device image in the penalty's layout, or NULL */
+int b200rt_gibbs_set_kappa(b200rt_gibbs* g, const float* kappa_dev);
+/* compute_value (GibbsPenalty.inl compute_value): beta sum_r sum_dr w_dr phi(x_r, x_r+dr) kappa_r kappa_r+dr, FP64;
+ * synchronises and writes *value (host). */
+int b200rt_gibbs_value_dev(b200rt_gibbs* g, const float* image_dev, double* value, void* stream);
+/* compute_gradient: 2 beta sum_dr w_dr phi_10(x_r, x_r+dr) kappa kappa */
+int b200rt_gibbs_gradient_dev(b200rt_gibbs* g, const float* image_dev, float* gradient_dev, void* stream);
+/* compute_gradient_times_input: <gradient at image_dev, input_dev>, FP64; synchronises and writes *value (host). */
+int b200rt_gibbs_gradient_times_input_dev(b200rt_gibbs* g, const float* input_dev, const float* image_dev,
+                                          double* value, void* stream);
+/* compute_Hessian_diagonal: 2 beta sum_dr w_dr phi_20(x_r, x_r+dr) kappa kappa */
+int b200rt_gibbs_hessian_diagonal_dev(b200rt_gibbs* g, const float* image_dev, float* out_dev, void* stream);
+/* accumulate_Hessian_times_input: output += 2 beta sum_dr w_dr (phi_20 in_r + phi_11 in_r+dr) kappa kappa */
+int b200rt_gibbs_accumulate_hessian_times_input_dev(b200rt_gibbs* g, const float* image_dev, const float* input_dev,
+                                                    float* output_dev, void* stream);
+/* compute_Hessian of the voxel (z, y, x) (0-based indices): out_dev is overwritten with the voxel's Hessian row */
+int b200rt_gibbs_hessian_dev(b200rt_gibbs* g, const float* image_dev, int z, int y, int x, float* out_dev,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,8 @@ def _load():
         "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
         "or_ossps_denominator_f32": (_I, [_P, _P, _P, _I, _P]),
         "or_prior_hessian_times_input_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+        "or_gibbs_f32": (_D, [_I, _I, _F, _F, _F, _P, _I, _I, _I, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+        "or_gibbs_default_weights": (_I, [_F, _F, _F, _I, _P]),
         "or_prior_curvature_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _I, _I, _I, _F, _F, _F, _P]),
         "or_ossps_update_f32": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P,
                                      _F, _F, _F, _I]),
@@ -290,6 +292,36 @@ def prior_curvature(prior: _abi.Prior, shape, voxel_size, kappa=None):
     if lib().or_prior_curvature_f32(ctypes.byref(prior), _ptr(k), nz, ny, nx, *map(float, voxel_size), _ptr(c)) != 0:
         raise RuntimeError("oracle curvature failed")
     return c
+
+
+GIBBS_OPS = {"value": 0, "gradient": 1, "gradient_times_input": 2, "hessian_diagonal": 3,
+             "hessian_times_input": 4, "hessian": 5}
+
+
+def gibbs_default_weights(voxel_size, only_2D=False):
+    """GibbsPenalty::compute_default_weights: [wz][3][3] floats, x voxel size / distance."""
+    w = np.zeros(27, np.float32)
+    wz = lib().or_gibbs_default_weights(*map(float, voxel_size), int(bool(only_2D)), _ptr(w))
+    return w[:wz * 9].reshape(wz, 3, 3).copy()
+
+
+def gibbs(op, potential, beta, weights, image, input_image=None, kappa=None, gamma=2.0, epsilon=1e-7, voxel=(0, 0, 0),
+          out=None):
+    """GibbsPenalty<float, potential> (potential 1 Quadratic, 2 Relative Difference) on [z][y][x] images.
+
+    op: "value" and "gradient_times_input" return a float; "gradient", "hessian_diagonal" and "hessian"
+    (of voxel `voxel`) return an image; "hessian_times_input" returns out + H input."""
+    image = np.ascontiguousarray(image, np.float32)
+    nz, ny, nx = image.shape
+    w = np.ascontiguousarray(weights, np.float32)
+    assert w.ndim == 3
+    k = None if kappa is None else np.ascontiguousarray(kappa, np.float32)
+    inp = None if input_image is None else np.ascontiguousarray(input_image, np.float32)
+    o = np.zeros(image.shape, np.float32) if out is None else np.ascontiguousarray(out, np.float32).copy()
+    code = GIBBS_OPS[op]
+    v = lib().or_gibbs_f32(code, potential, float(beta), float(gamma), float(epsilon), _ptr(w), *w.shape, _ptr(k),
+                           _ptr(image), _ptr(inp), nz, ny, nx, *map(int, voxel), _ptr(o))
+    return v if code in (0, 2) else o
 
 
 def ray_trace(start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity=1 << 14):

@@ -1674,6 +1674,175 @@ double or_prior_value_f32(const b200rt_prior* p, const float* img, const float* 
   return prior_value(*p, img, kappa, nz, ny, nx, vz, vy, vx);
 }
 
+/* ---- Gibbs penalties: GibbsPenalty<float, Potential> (GibbsPenalty.inl) ---------------------------------------
+   Potentials as in QuadraticPotential (GibbsQuadraticPenalty.h:50-80) and RelativeDifferencePotential
+   (GibbsRelativeDifferencePenalty.h:60-120): each expression is evaluated in the types the reference gives it
+   (float operands, double literals 0.5 / 1.0 promote that operation to double, results converted back to
+   float where the reference assigns to an elemT).  fabs of a float is taken in float. */
+extern "C++" {
+struct GibbsQuadraticPotential {
+  double value(float c, float n) const {
+    const float diff = c - n;
+    return static_cast<double>(diff * diff) / 4.0;
+  }
+  double d10(float c, float n) const { return static_cast<double>(c - n) / 2.0; }
+  double d20(float, float) const { return 0.5; }
+  double d11(float, float) const { return -0.5; }
+};
+
+struct GibbsRDPotential {
+  float gamma, epsilon;
+  double value(float c, float n) const {
+    const float diff = c - n;
+    const float add = c + n;
+    const float num = static_cast<float>(0.5 * static_cast<double>(diff * diff));
+    const float den = static_cast<float>(1.0 / static_cast<double>(add + gamma * std::fabs(diff) + epsilon));
+    return static_cast<double>(num * den);
+  }
+  double d10(float c, float n) const {
+    const float diff = c - n;
+    const float factor = c + n + gamma * std::fabs(diff) + epsilon;
+    const float num = static_cast<float>(0.5 * static_cast<double>(diff) * static_cast<double>(factor + 2 * n + epsilon));
+    const float den = static_cast<float>(1.0 / static_cast<double>(factor * factor));
+    return static_cast<double>(num * den);
+  }
+  double d20(float c, float n) const {
+    const float num = 2 * n + epsilon;
+    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * std::fabs(c - n) + epsilon));
+    return static_cast<double>(num * num * den * den * den);
+  }
+  double d11(float c, float n) const {
+    const float num = -(2 * c + epsilon) * (2 * n + epsilon);
+    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * std::fabs(c - n) + epsilon));
+    return static_cast<double>(num * den * den * den);
+  }
+};
+
+/* weights [wz][wy][wx] with index ranges [-(w/2), w - 1 - w/2] (GibbsPenalty.inl post_processing: an even size
+   behaves as if a zero were appended) */
+struct GibbsWeights {
+  const float* w;
+  int wz, wy, wx;
+  int lo(int s) const { return -(s / 2); }
+  int hi(int s) const { return s - 1 - s / 2; }
+  float at(int dz, int dy, int dx) const {
+    return w[(static_cast<int64_t>(dz - lo(wz)) * wy + (dy - lo(wy))) * wx + (dx - lo(wx))];
+  }
+};
+
+template <typename Pot>
+double gibbs_run(int op, const Pot& pot, float beta, const GibbsWeights& W, const float* kappa, const float* x,
+                 const float* in, int nz, int ny, int nx, int vz, int vy, int vx, float* out) {
+  auto at = [&](int z, int y, int xx) { return (static_cast<int64_t>(z) * ny + y) * nx + xx; };
+  double total = 0.0;
+  if (op == 5) {  // compute_Hessian of one voxel (GibbsPenalty.inl compute_Hessian)
+    std::fill(out, out + static_cast<int64_t>(nz) * ny * nx, 0.f);
+    if (beta == 0) return 0.0;
+    const int z = vz, y = vy, xx = vx;
+    const int min_dz = std::max(W.lo(W.wz), -z), max_dz = std::min(W.hi(W.wz), nz - 1 - z);
+    const int min_dy = std::max(W.lo(W.wy), -y), max_dy = std::min(W.hi(W.wy), ny - 1 - y);
+    const int min_dx = std::max(W.lo(W.wx), -xx), max_dx = std::min(W.hi(W.wx), nx - 1 - xx);
+    const int64_t j = at(z, y, xx);
+    for (int dz = min_dz; dz <= max_dz; ++dz)
+      for (int dy = min_dy; dy <= max_dy; ++dy)
+        for (int dx = min_dx; dx <= max_dx; ++dx) {
+          float current = 0.0f;
+          if (dz == 0 && dy == 0 && dx == 0) {
+            for (int ddz = min_dz; ddz <= max_dz; ++ddz)
+              for (int ddy = min_dy; ddy <= max_dy; ++ddy)
+                for (int ddx = min_dx; ddx <= max_dx; ++ddx) {
+                  const int64_t k = at(z + ddz, y + ddy, xx + ddx);
+                  float dc = static_cast<float>(W.at(ddz, ddy, ddx) * 2 * pot.d20(x[j], x[k]));
+                  if (kappa) dc *= kappa[j] * kappa[k];
+                  current += dc;
+                }
+          } else {
+            const int64_t k = at(z + dz, y + dy, xx + dx);
+            current = static_cast<float>(W.at(dz, dy, dx) * 2 * pot.d11(x[j], x[k]));
+            if (kappa) current *= kappa[j] * kappa[k];
+          }
+          out[at(z + dz, y + dy, xx + dx)] = current * beta;
+        }
+    return 0.0;
+  }
+  if (beta == 0) {
+    if (op == 1 || op == 3) std::fill(out, out + static_cast<int64_t>(nz) * ny * nx, 0.f);
+    return 0.0;
+  }
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int xx = 0; xx < nx; ++xx) {
+        const int min_dz = std::max(W.lo(W.wz), -z), max_dz = std::min(W.hi(W.wz), nz - 1 - z);
+        const int min_dy = std::max(W.lo(W.wy), -y), max_dy = std::min(W.hi(W.wy), ny - 1 - y);
+        const int min_dx = std::max(W.lo(W.wx), -xx), max_dx = std::min(W.hi(W.wx), nx - 1 - xx);
+        const int64_t j = at(z, y, xx);
+        const float c = x[j];
+        if (op == 4) {  // accumulate_Hessian_times_input: float sums, the centre included
+          float result = 0;
+          for (int dz = min_dz; dz <= max_dz; ++dz)
+            for (int dy = min_dy; dy <= max_dy; ++dy)
+              for (int dx = min_dx; dx <= max_dx; ++dx) {
+                const int64_t k = at(z + dz, y + dy, xx + dx);
+                float current = W.at(dz, dy, dx);
+                if (dz == 0 && dy == 0 && dx == 0)
+                  current = static_cast<float>(current * (pot.d20(c, x[k]) * in[j]));
+                else
+                  current = static_cast<float>(current * (pot.d20(c, x[k]) * in[j] + pot.d11(c, x[k]) * in[k]));
+                if (kappa) current *= kappa[j] * kappa[k];
+                result += current;
+              }
+          out[j] += 2 * result * beta;
+          continue;
+        }
+        double sum = 0.0;
+        for (int dz = min_dz; dz <= max_dz; ++dz)
+          for (int dy = min_dy; dy <= max_dy; ++dy)
+            for (int dx = min_dx; dx <= max_dx; ++dx) {
+              if (dz == 0 && dy == 0 && dx == 0) continue;
+              const int64_t k = at(z + dz, y + dy, xx + dx);
+              const float n = x[k];
+              const double f = op == 0 ? pot.value(c, n) : (op == 3 ? pot.d20(c, n) : pot.d10(c, n));
+              double current = W.at(dz, dy, dx) * f;
+              if (kappa) current *= kappa[j] * kappa[k];
+              sum += current;
+            }
+        if (op == 0)
+          total += sum;
+        else if (op == 1 || op == 3)
+          out[j] = 2 * static_cast<float>(sum * beta);
+        else
+          total += 2 * sum * in[j];
+      }
+  return total * beta;
+}
+}  // extern "C++"
+
+double or_gibbs_f32(int op, int potential, float beta, float gamma, float epsilon, const float* weights, int wz, int wy,
+                    int wx, const float* kappa, const float* image, const float* input, int nz, int ny, int nx, int vz,
+                    int vy, int vx, float* out) {
+  const GibbsWeights W{weights, wz, wy, wx};
+  if (potential == 1) return gibbs_run(op, GibbsQuadraticPotential{}, beta, W, kappa, image, input, nz, ny, nx, vz, vy, vx, out);
+  return gibbs_run(op, GibbsRDPotential{gamma, epsilon}, beta, W, kappa, image, input, nz, ny, nx, vz, vy, vx, out);
+}
+
+/* GibbsPenalty::compute_default_weights (GibbsPenalty.inl): x voxel size / distance over a 3x3x3 neighbourhood
+   (1x3x3 with only_2D), centre 0; w holds wz*9 floats, wz returned */
+int or_gibbs_default_weights(float vz, float vy, float vx, int only_2D, float* w) {
+  const int z0 = only_2D ? 0 : -1, z1 = only_2D ? 0 : 1;
+  int i = 0;
+  for (int z = z0; z <= z1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        if (z == 0 && y == 0 && x == 0) {
+          w[i++] = 0.f;
+          continue;
+        }
+        const float a = x * vx, b = y * vy, c = z * vz;
+        w[i++] = vx / std::sqrt(a * a + b * b + c * c);
+      }
+  return z1 - z0 + 1;
+}
+
 int64_t or_ray_trace(const float start[3], const float stop[3], const float vox[3], float norm_const, int32_t* coords,
                      float* values, int64_t cap) {
   Row<float> r;

@@ -102,6 +102,16 @@ int or_prior_gradient_f32(const b200rt_prior* prior, const float* image, const f
 double or_prior_value_f32(const b200rt_prior* prior, const float* image, const float* kappa, int nz, int ny, int nx,
                           float vz, float vy, float vx);
 
+/* GibbsPenalty<float, potential> (GibbsPenalty.inl): potential 1 Quadratic, 2 Relative Difference;
+   op 0 value, 1 gradient, 2 gradient times input, 3 Hessian diagonal, 4 accumulate Hessian times input (out +=),
+   5 Hessian of voxel (vz, vy, vx) into out.  Images [z][y][x]; weights [wz][wy][wx]; kappa may be NULL.
+   Returns the value (op 0, 2), else 0. */
+double or_gibbs_f32(int op, int potential, float beta, float gamma, float epsilon, const float* weights, int wz, int wy,
+                    int wx, const float* kappa, const float* image, const float* input, int nz, int ny, int nx, int vz,
+                    int vy, int vx, float* out);
+/* default weights (x voxel size / distance), 27 or 9 (only_2D) floats; returns the z size */
+int or_gibbs_default_weights(float vz, float vy, float vx, int only_2D, float* w);
+
 /* Siddon tracer of one segment (RayTraceVoxelsOnCartesianGrid.cxx:51-269): appends to the
    arrays; returns the number of elements or -1 if capacity is exceeded. */
 int64_t or_ray_trace(const float start_zyx[3], const float stop_zyx[3], const float voxel_size_zyx[3],

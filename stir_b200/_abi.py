@@ -119,6 +119,36 @@ class BatchConfig(ctypes.Structure):
     ]
 
 
+GIBBS_QUADRATIC = 1
+GIBBS_RELATIVE_DIFFERENCE = 2
+LAYOUT_DEVICE = 0  # [y][x][z]
+LAYOUT_STIR = 1    # [z][y][x]
+
+
+class GibbsParams(ctypes.Structure):
+    """b200rt_gibbs_params"""
+
+    _fields_ = [
+        ("potential", ctypes.c_int32),
+        ("penalisation_factor", ctypes.c_float),
+        ("gamma", ctypes.c_float),
+        ("epsilon", ctypes.c_float),
+        ("nz", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("nx", ctypes.c_int32),
+        ("layout", ctypes.c_int32),
+        ("voxel_size_z", ctypes.c_float),
+        ("voxel_size_y", ctypes.c_float),
+        ("voxel_size_x", ctypes.c_float),
+        ("only_2D", ctypes.c_int32),
+        ("weights_z", ctypes.c_int32),
+        ("weights_y", ctypes.c_int32),
+        ("weights_x", ctypes.c_int32),
+        ("weights", ctypes.c_void_p),
+        ("kappa_dev", ctypes.c_void_p),
+    ]
+
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "libstir_b200.so")
 
@@ -170,6 +200,17 @@ EXPORTS = [
     ("b200rt_batch_set_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
     ("b200rt_batch_get_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
     ("b200rt_batch_get_num_cancelled", _I, [_P, _I, ctypes.POINTER(_I64)]),
+    ("b200rt_gibbs_create", _I, [ctypes.POINTER(GibbsParams), _I, ctypes.POINTER(_P)]),
+    ("b200rt_gibbs_destroy", None, [_P]),
+    ("b200rt_gibbs_last_error", ctypes.c_char_p, [_P]),
+    ("b200rt_gibbs_get_weights", _I, [_P, _P, ctypes.POINTER(ctypes.c_int32)]),
+    ("b200rt_gibbs_set_kappa", _I, [_P, _P]),
+    ("b200rt_gibbs_value_dev", _I, [_P, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    ("b200rt_gibbs_gradient_dev", _I, [_P, _P, _P, _P]),
+    ("b200rt_gibbs_gradient_times_input_dev", _I, [_P, _P, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    ("b200rt_gibbs_hessian_diagonal_dev", _I, [_P, _P, _P, _P]),
+    ("b200rt_gibbs_accumulate_hessian_times_input_dev", _I, [_P, _P, _P, _P, _P]),
+    ("b200rt_gibbs_hessian_dev", _I, [_P, _P, _I, _I, _I, _P, _P]),
 ]
 
 _lib = None
@@ -199,9 +240,14 @@ class B200Error(RuntimeError):
     pass
 
 
-def check(status: int, handle=None, what: str = "", batch=None):
+def check(status: int, handle=None, what: str = "", batch=None, gibbs=None):
     if status != OK:
         lib = load_library()
-        msg = lib.b200rt_batch_last_error(batch) if batch is not None else lib.b200rt_last_error(handle)
+        if gibbs is not None:
+            msg = lib.b200rt_gibbs_last_error(gibbs)
+        elif batch is not None:
+            msg = lib.b200rt_batch_last_error(batch)
+        else:
+            msg = lib.b200rt_last_error(handle)
         msg = msg.decode() if msg else ""
         raise B200Error(f"{what} failed with status {status}: {msg}")

@@ -128,6 +128,17 @@ struct b200rt_projector {
   // staging for the host API
   DevBuf<float> st_img_a, st_img_b, st_pd_a, st_pd_b;
   cudaStream_t stream = nullptr;
+  // host API pipelining: path items grouped by the views they write, so that the copies of one group of
+  // views overlap the projection of the next; copies on a second stream
+  std::vector<int> h_item_out_view;  // the view of every line of the item (-1: lines of several views)
+  bool paths_view_split = false;
+  struct ViewGroups {
+    std::unique_ptr<DevBuf<int>> list;  // the subset's items, group by group
+    std::vector<int> off, v0;           // group g: items [off[g], off[g+1]), views [v0[g], v0[g+1])
+  };
+  std::map<std::pair<int, int>, ViewGroups> view_groups;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> copy_events;
 
   long long bin_key(int view, int seg, int tang, int tof) const {
     const Geometry& g = *geo;
@@ -291,7 +302,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   std::vector<int> chunks;
   std::vector<PathLineDev> plines;
   std::vector<PathItemDev> items;
-  std::vector<int> item_view;
+  std::vector<int> item_view, item_out_view;
   int max_lines = 1, max_acc = 1;
   for (int gi = 0; gi < ngroups; ++gi) {
     const Group& G = groups[gi];
@@ -336,6 +347,10 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
       max_acc = std::max(max_acc, path_parts(it.num_lines) * nax_sum);
       items.push_back(it);
       item_view.push_back(bviews[vi]);
+      int ov = lines[plines[it.first_line].line].view;
+      for (int l = it.first_line; l < it.first_line + it.num_lines; ++l)
+        if (lines[plines[l].line].view != ov) ov = -1;
+      item_out_view.push_back(ov);
     }
   }
   if (elems.size() >= (size_t(1) << 31) || chunks.size() >= (size_t(1) << 31) || col_starts.size() >= (size_t(1) << 31))
@@ -377,6 +392,8 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   pp.max_acc = max_acc;
   pp.zpad = zpad;
   h.h_item_view = item_view;
+  h.h_item_out_view = item_out_view;
+  h.paths_view_split = std::find(item_out_view.begin(), item_out_view.end(), -1) == item_out_view.end();
   h.h_path_items = items;
   h.use_paths = true;
 }
@@ -872,6 +889,71 @@ cudaError_t projdata_layout(const Geometry& g, const float* in, float* out, bool
   return cudaSuccess;
 }
 
+// projection data layout change of the views [v0, v1) only (STIR order <-> device layout)
+cudaError_t projdata_layout_views(const Geometry& g, const float* in, float* out, bool to_dev, int v0, int v1,
+                                  cudaStream_t st) {
+  const int64_t nt = g.num_tang(), nvt = static_cast<int64_t>(g.num_views()) * nt;
+  const int64_t c0 = v0 * nt, nc = (v1 - v0) * nt;
+  for (int k = 0; k < g.num_tof(); ++k)
+    for (int s = -g.S(); s <= g.S(); ++s) {
+      const int64_t so = k * g.tof_stride() + g.stir_segment_offset(s) + c0;
+      const int64_t dv = k * g.tof_stride() + g.dev_segment_offset(s) + c0 * g.nax(s);
+      const int nax = g.nax(s);
+      const cudaError_t e = to_dev ? launch_transpose(in + so, out + dv, nax, nc, nvt, nax, st)
+                                   : launch_transpose(in + dv, out + so, static_cast<int>(nc), nax, nax, nvt, st);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+// copy of the views [v0, v1) of projection data in STIR order (rows of views x tangential positions for every
+// timing bin, segment and axial position): one strided copy
+cudaError_t copy_views(const Geometry& g, float* dst, const float* src, int v0, int v1, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+  const size_t nt = static_cast<size_t>(g.num_tang()), nvt = nt * static_cast<size_t>(g.num_views());
+  const size_t rows = static_cast<size_t>(g.projdata_size()) / nvt;
+  return cudaMemcpy2DAsync(dst + nt * v0, sizeof(float) * nvt, src + nt * v0, sizeof(float) * nvt,
+                           sizeof(float) * nt * (v1 - v0), rows, kind, st);
+}
+
+constexpr int kHostViewGroups = 8;
+
+// the subset's path items ordered by the group of views they write (kHostViewGroups equal view ranges)
+const b200rt_projector::ViewGroups& view_groups(b200rt_projector& h, int subset, int nsub) {
+  const auto key = std::make_pair(subset, nsub);
+  auto it = h.view_groups.find(key);
+  if (it != h.view_groups.end()) return it->second;
+  const int nv = h.geo->num_views();
+  const int G = std::min(kHostViewGroups, nv);
+  b200rt_projector::ViewGroups vg;
+  for (int gi = 0; gi <= G; ++gi) vg.v0.push_back(static_cast<int>(static_cast<int64_t>(nv) * gi / G));
+  std::vector<std::vector<int>> per(G);
+  for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i) {
+    if (h.h_item_view[i] % nsub != subset) continue;
+    const int gi = static_cast<int>(std::upper_bound(vg.v0.begin(), vg.v0.end(), h.h_item_out_view[i]) - vg.v0.begin()) - 1;
+    per[gi].push_back(i);
+  }
+  std::vector<int> list;
+  for (int gi = 0; gi < G; ++gi) {
+    vg.off.push_back(static_cast<int>(list.size()));
+    list.insert(list.end(), per[gi].begin(), per[gi].end());
+  }
+  vg.off.push_back(static_cast<int>(list.size()));
+  vg.list = std::make_unique<DevBuf<int>>();
+  vg.list->upload(list, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "view groups");
+  return h.view_groups.emplace(key, std::move(vg)).first->second;
+}
+
+void ensure_copy_stream(b200rt_projector& h) {
+  if (!h.copy_stream) ck(cudaStreamCreateWithFlags(&h.copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  while (h.copy_events.size() < kHostViewGroups + 1) {
+    cudaEvent_t e = nullptr;
+    ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    h.copy_events.push_back(e);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -946,6 +1028,12 @@ void b200rt_destroy(b200rt_projector* h) {
     h->st_img_b.release();
     h->st_pd_a.release();
     h->st_pd_b.release();
+    h->view_groups.clear();
+    if (h->copy_stream) {
+      cudaStreamSynchronize(h->copy_stream);
+      cudaStreamDestroy(h->copy_stream);
+    }
+    for (cudaEvent_t e : h->copy_events) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
   }
   delete h;
@@ -1083,6 +1171,27 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
     ck(cudaMemcpyAsync(h->st_img_a.p, image_host, sizeof(float) * g.image_size(), cudaMemcpyHostToDevice, st), "H2D");
     ck(launch_image_to_dev(h->st_img_a.p, h->st_img_b.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
     ck(cudaMemsetAsync(h->st_pd_b.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+    if (h->use_paths && h->paths_view_split) {
+      // group by group of views: projection, layout change, then the group's copy to the host on the copy
+      // stream while the next group is projected
+      const b200rt_projector::ViewGroups& vg = view_groups(*h, subset_num, num_subsets);
+      ensure_copy_stream(*h);
+      for (size_t gi = 0; gi + 1 < vg.v0.size(); ++gi) {
+        const int n = vg.off[gi + 1] - vg.off[gi];
+        if (n > 0)
+          ck(launch_forward_paths(h->params, h->pparams, vg.list->p + vg.off[gi], n, h->st_img_b.p, h->st_pd_b.p, st,
+                                  nullptr),
+             "forward projection");
+        ck(projdata_layout_views(g, h->st_pd_b.p, h->st_pd_a.p, false, vg.v0[gi], vg.v0[gi + 1], st), "layout");
+        ck(cudaEventRecord(h->copy_events[gi], st), "cudaEventRecord");
+        ck(cudaStreamWaitEvent(h->copy_stream, h->copy_events[gi], 0), "cudaStreamWaitEvent");
+        ck(copy_views(g, projdata_host, h->st_pd_a.p, vg.v0[gi], vg.v0[gi + 1], cudaMemcpyDeviceToHost, h->copy_stream),
+           "D2H");
+      }
+      ck(cudaStreamSynchronize(h->copy_stream), "forward projection");
+      ck(cudaStreamSynchronize(st), "forward projection");
+      return B200RT_OK;
+    }
     forward_subset(*h, h->st_img_b.p, h->st_pd_b.p, subset_num, num_subsets, st);
     ck(projdata_layout(g, h->st_pd_b.p, h->st_pd_a.p, false, st), "layout");
     ck(cudaMemcpyAsync(projdata_host, h->st_pd_a.p, sizeof(float) * g.projdata_size(), cudaMemcpyDeviceToHost, st), "D2H");
@@ -1107,9 +1216,35 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
     h->st_img_b.alloc(g.image_size());
     h->st_pd_a.alloc(g.projdata_size());
     h->st_pd_b.alloc(g.projdata_size());
-    ck(cudaMemcpyAsync(h->st_pd_a.p, projdata_host, sizeof(float) * g.projdata_size(), cudaMemcpyHostToDevice, st), "H2D");
-    ck(projdata_layout(g, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
-    back_project_into(*h, h->st_pd_b.p, h->st_img_b.p, subset_num, num_subsets, mode, 0, st);
+    if (h->use_paths && h->paths_view_split && mode == B200RT_BACKPROJECT_ATOMIC) {
+      // group by group of views: the copy stream brings the groups' data in order, the projection stream
+      // changes each group's layout and back-projects its items as soon as its data are in
+      const b200rt_projector::ViewGroups& vg = view_groups(*h, subset_num, num_subsets);
+      ensure_copy_stream(*h);
+      const size_t G = vg.v0.size() - 1;
+      ck(cudaEventRecord(h->copy_events[G], st), "cudaEventRecord");  // staging buffers free
+      ck(cudaStreamWaitEvent(h->copy_stream, h->copy_events[G], 0), "cudaStreamWaitEvent");
+      for (size_t gi = 0; gi < G; ++gi) {
+        ck(copy_views(g, h->st_pd_a.p, projdata_host, vg.v0[gi], vg.v0[gi + 1], cudaMemcpyHostToDevice, h->copy_stream),
+           "H2D");
+        ck(cudaEventRecord(h->copy_events[gi], h->copy_stream), "cudaEventRecord");
+      }
+      ck(cudaMemsetAsync(h->st_img_b.p, 0, sizeof(float) * g.image_size(), st), "memset");
+      for (size_t gi = 0; gi < G; ++gi) {
+        ck(cudaStreamWaitEvent(st, h->copy_events[gi], 0), "cudaStreamWaitEvent");
+        ck(projdata_layout_views(g, h->st_pd_a.p, h->st_pd_b.p, true, vg.v0[gi], vg.v0[gi + 1], st), "layout");
+        const int n = vg.off[gi + 1] - vg.off[gi];
+        if (n > 0)
+          ck(launch_back_paths_atomic(h->params, h->pparams, vg.list->p + vg.off[gi], n, h->st_pd_b.p, h->st_img_b.p,
+                                      st, 0),
+             "back projection");
+      }
+    } else {
+      ck(cudaMemcpyAsync(h->st_pd_a.p, projdata_host, sizeof(float) * g.projdata_size(), cudaMemcpyHostToDevice, st),
+         "H2D");
+      ck(projdata_layout(g, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
+      back_project_into(*h, h->st_pd_b.p, h->st_img_b.p, subset_num, num_subsets, mode, 0, st);
+    }
     ck(launch_image_from_dev(h->st_img_b.p, h->st_img_a.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");
     ck(cudaMemcpyAsync(image_host, h->st_img_a.p, sizeof(float) * g.image_size(), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "back projection");
@@ -2128,6 +2263,194 @@ int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out) {
     return B200RT_OK;
   } catch (const std::exception& e) {
     return bfail(b, status_of(e), e.what());
+  }
+}
+
+}  // extern "C"
+
+/* ---- Gibbs penalties ---------------------------------------------------- */
+struct b200rt_gibbs {
+  int device = 0;
+  GibbsDev d{};
+  std::vector<float> host_w;
+  DevBuf<double> partial, result;
+  std::string err;
+};
+
+namespace {
+
+int gfail(b200rt_gibbs* g, int code, const std::string& msg) {
+  if (g) g->err = msg;
+  return code;
+}
+
+int create_fail(int code, const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_create_error = msg;
+  return code;
+}
+
+// one penalty operation: validates the pointers, runs on `stream`; scalar results are copied to *value
+int gibbs_op(b200rt_gibbs* g, int op, const float* x, const float* in, float* out, double* value, void* stream) {
+  if (!g || !x) return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if ((op == 0 || op == 2) && !value) return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "null value pointer");
+  if ((op == 1 || op == 3 || op == 4) && !out) return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "null output");
+  if ((op == 2 || op == 4) && !in) return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "null input image");
+  try {
+    DeviceGuard dg(g->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = static_cast<int64_t>(g->d.nz) * g->d.ny * g->d.nx;
+    if (g->d.beta == 0) {  // GibbsPenalty.inl: a zero penalisation factor gives 0, a zero gradient / diagonal
+      if (op == 1 || op == 3) ck(cudaMemsetAsync(out, 0, sizeof(float) * n, st), "memset");
+      if (value) *value = 0.0;
+      return B200RT_OK;
+    }
+    if (op == 0 || op == 2) {
+      g->partial.alloc(static_cast<size_t>(gibbs_num_partials(g->d)));
+      g->result.alloc(1);
+    }
+    ck(launch_gibbs(g->d, op, x, in, out, g->partial.p, g->result.p, st), "Gibbs penalty");
+    if (op == 0 || op == 2) {
+      ck(cudaMemcpyAsync(value, g->result.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+      ck(cudaStreamSynchronize(st), "Gibbs penalty");
+    }
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return gfail(g, status_of(e), e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200rt_gibbs_create(const b200rt_gibbs_params* p, int device, b200rt_gibbs** out) {
+  if (!out) return B200RT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!p) return create_fail(B200RT_ERR_INVALID_ARGUMENT, "null parameters");
+  if (p->potential != B200RT_GIBBS_QUADRATIC && p->potential != B200RT_GIBBS_RELATIVE_DIFFERENCE)
+    return create_fail(B200RT_ERR_INVALID_ARGUMENT, "unknown Gibbs potential");
+  if (p->nz < 1 || p->ny < 1 || p->nx < 1) return create_fail(B200RT_ERR_INVALID_ARGUMENT, "empty image");
+  if (p->layout != B200RT_LAYOUT_DEVICE && p->layout != B200RT_LAYOUT_STIR)
+    return create_fail(B200RT_ERR_INVALID_ARGUMENT, "unknown image layout");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return create_fail(B200RT_ERR_INVALID_ARGUMENT, "invalid CUDA device");
+  auto g = std::make_unique<b200rt_gibbs>();
+  g->device = device;
+  GibbsDev& d = g->d;
+  d.potential = p->potential;
+  d.beta = p->penalisation_factor;
+  d.gamma = p->gamma;
+  d.epsilon = p->epsilon;
+  d.nz = p->nz;
+  d.ny = p->ny;
+  d.nx = p->nx;
+  d.layout = p->layout;
+  if (p->layout == B200RT_LAYOUT_DEVICE) {
+    d.sz = 1;
+    d.sx = p->nz;
+    d.sy = static_cast<int64_t>(p->nz) * p->nx;
+  } else {
+    d.sx = 1;
+    d.sy = p->nx;
+    d.sz = static_cast<int64_t>(p->nx) * p->ny;
+  }
+  d.kappa = p->kappa_dev;
+  if (p->weights) {
+    const int wz = p->weights_z, wy = p->weights_y, wx = p->weights_x;
+    if (wz < 1 || wy < 1 || wx < 1 || wz > 7 || wy > 7 || wx > 7)
+      return create_fail(B200RT_ERR_INVALID_ARGUMENT, "weights sizes must be 1..7");
+    d.wz = wz;
+    d.wy = wy;
+    d.wx = wx;
+    g->host_w.assign(p->weights, p->weights + wz * wy * wx);
+  } else {
+    // compute_default_weights (GibbsPenalty.inl): x voxel size / Euclidean distance, centre 0
+    if (!(p->voxel_size_x > 0 && p->voxel_size_y > 0 && p->voxel_size_z > 0))
+      return create_fail(B200RT_ERR_INVALID_ARGUMENT, "default weights need positive voxel sizes");
+    d.wz = p->only_2D ? 1 : 3;
+    d.wy = d.wx = 3;
+    const float vz = p->voxel_size_z, vy = p->voxel_size_y, vx = p->voxel_size_x;
+    for (int z = -(d.wz / 2); z <= d.wz / 2; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+          float v = 0.f;
+          if (!(z == 0 && y == 0 && x == 0)) {
+            const float a = static_cast<float>(x) * vx, b = static_cast<float>(y) * vy, c = static_cast<float>(z) * vz;
+            v = vx / std::sqrt(a * a + b * b + c * c);
+          }
+          g->host_w.push_back(v);
+        }
+  }
+  std::copy(g->host_w.begin(), g->host_w.end(), d.w);
+  *out = g.release();
+  return B200RT_OK;
+}
+
+void b200rt_gibbs_destroy(b200rt_gibbs* g) {
+  if (!g) return;
+  {
+    DeviceGuard dg(g->device);
+    g->partial.release();
+    g->result.release();
+  }
+  delete g;
+}
+
+const char* b200rt_gibbs_last_error(const b200rt_gibbs* g) { return g ? g->err.c_str() : "null penalty"; }
+
+int b200rt_gibbs_get_weights(const b200rt_gibbs* g, float* w, int32_t sizes[3]) {
+  if (!g || !sizes) return B200RT_ERR_INVALID_ARGUMENT;
+  sizes[0] = g->d.wz;
+  sizes[1] = g->d.wy;
+  sizes[2] = g->d.wx;
+  if (w) std::copy(g->host_w.begin(), g->host_w.end(), w);
+  return B200RT_OK;
+}
+
+int b200rt_gibbs_set_kappa(b200rt_gibbs* g, const float* kappa_dev) {
+  if (!g) return B200RT_ERR_INVALID_ARGUMENT;
+  g->d.kappa = kappa_dev;
+  return B200RT_OK;
+}
+
+int b200rt_gibbs_value_dev(b200rt_gibbs* g, const float* image_dev, double* value, void* stream) {
+  return gibbs_op(g, 0, image_dev, nullptr, nullptr, value, stream);
+}
+
+int b200rt_gibbs_gradient_dev(b200rt_gibbs* g, const float* image_dev, float* gradient_dev, void* stream) {
+  return gibbs_op(g, 1, image_dev, nullptr, gradient_dev, nullptr, stream);
+}
+
+int b200rt_gibbs_gradient_times_input_dev(b200rt_gibbs* g, const float* input_dev, const float* image_dev,
+                                          double* value, void* stream) {
+  return gibbs_op(g, 2, image_dev, input_dev, nullptr, value, stream);
+}
+
+int b200rt_gibbs_hessian_diagonal_dev(b200rt_gibbs* g, const float* image_dev, float* out_dev, void* stream) {
+  return gibbs_op(g, 3, image_dev, nullptr, out_dev, nullptr, stream);
+}
+
+int b200rt_gibbs_accumulate_hessian_times_input_dev(b200rt_gibbs* g, const float* image_dev, const float* input_dev,
+                                                    float* output_dev, void* stream) {
+  return gibbs_op(g, 4, image_dev, input_dev, output_dev, nullptr, stream);
+}
+
+int b200rt_gibbs_hessian_dev(b200rt_gibbs* g, const float* image_dev, int z, int y, int x, float* out_dev,
+                             void* stream) {
+  if (!g || !image_dev || !out_dev) return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (z < 0 || z >= g->d.nz || y < 0 || y >= g->d.ny || x < 0 || x >= g->d.nx)
+    return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "voxel outside the image");
+  try {
+    DeviceGuard dg(g->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = static_cast<int64_t>(g->d.nz) * g->d.ny * g->d.nx;
+    ck(cudaMemsetAsync(out_dev, 0, sizeof(float) * n, st), "memset");
+    if (g->d.beta != 0) ck(launch_gibbs_hessian_voxel(g->d, image_dev, z, y, x, out_dev, st), "Gibbs Hessian");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return gfail(g, status_of(e), e.what());
   }
 }
 

@@ -1,0 +1,250 @@
+// Gibbs penalties on device-resident images: GibbsPenalty<float, Potential>
+// (src/include/stir/recon_buildblock/GibbsPenalty.inl) with the Quadratic potential (GibbsQuadraticPenalty.h:50-80)
+// or the Relative Difference potential (GibbsRelativeDifferencePenalty.h:60-120), i.e. the operations of
+// GibbsQuadraticPenalty / GibbsRelativeDifferencePenalty and of their CUDA versions
+// (src/include/stir/recon_buildblock/CUDA/CudaGibbsPenalty.cuh), without the host copies.
+//
+// One thread per voxel, in memory order, for either image layout; the neighbourhood (weights of any size up to
+// 7x7x7, kernel parameters) is walked in STIR's order (dz, dy, dx) and every sum is taken in the type and order of
+// GibbsPenalty.inl (double for the value, gradient and Hessian diagonal, float for the Hessian times an input), so
+// each voxel's result is that of the host loop.  Scalars (value, gradient times input) are summed per block in a
+// fixed order and the block sums reduced in a fixed order: deterministic.  Compiled with -fmad=false, so float and
+// double expressions round as the host build evaluates them.
+#include "internal.hpp"
+
+namespace b200 {
+
+namespace {
+
+constexpr int kGibbsThreads = 256;
+
+struct QuadPot {
+  __device__ __forceinline__ double value(float c, float n) const {
+    const float diff = c - n;
+    return static_cast<double>(diff * diff) / 4.0;
+  }
+  __device__ __forceinline__ double d10(float c, float n) const { return static_cast<double>(c - n) / 2.0; }
+  __device__ __forceinline__ double d20(float, float) const { return 0.5; }
+  __device__ __forceinline__ double d11(float, float) const { return -0.5; }
+};
+
+// float operands; the double literals 0.5 and 1.0 make those operations double, and the results assigned to
+// float variables are rounded to float, as in the reference's expressions
+struct RDPot {
+  float gamma, epsilon;
+  __device__ __forceinline__ double value(float c, float n) const {
+    const float diff = c - n;
+    const float add = c + n;
+    const float num = static_cast<float>(0.5 * static_cast<double>(diff * diff));
+    const float den = static_cast<float>(1.0 / static_cast<double>(add + gamma * fabsf(diff) + epsilon));
+    return static_cast<double>(num * den);
+  }
+  __device__ __forceinline__ double d10(float c, float n) const {
+    const float diff = c - n;
+    const float factor = c + n + gamma * fabsf(diff) + epsilon;
+    const float num = static_cast<float>(0.5 * static_cast<double>(diff) * static_cast<double>(factor + 2 * n + epsilon));
+    const float den = static_cast<float>(1.0 / static_cast<double>(factor * factor));
+    return static_cast<double>(num * den);
+  }
+  __device__ __forceinline__ double d20(float c, float n) const {
+    const float num = 2 * n + epsilon;
+    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * fabsf(c - n) + epsilon));
+    return static_cast<double>(num * num * den * den * den);
+  }
+  __device__ __forceinline__ double d11(float c, float n) const {
+    const float num = -(2 * c + epsilon) * (2 * n + epsilon);
+    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * fabsf(c - n) + epsilon));
+    return static_cast<double>(num * den * den * den);
+  }
+};
+
+// the voxel (z, y, x) of memory index i
+__device__ __forceinline__ void gibbs_coords(const GibbsDev& g, int64_t i, int& z, int& y, int& x) {
+  if (g.layout == 0) {  // [y][x][z]
+    z = static_cast<int>(i % g.nz);
+    const int64_t t = i / g.nz;
+    x = static_cast<int>(t % g.nx);
+    y = static_cast<int>(t / g.nx);
+  } else {  // [z][y][x]
+    x = static_cast<int>(i % g.nx);
+    const int64_t t = i / g.nx;
+    y = static_cast<int>(t % g.ny);
+    z = static_cast<int>(t / g.ny);
+  }
+}
+
+struct Range {
+  int z0, z1, y0, y1, x0, x1;
+};
+__device__ __forceinline__ Range gibbs_range(const GibbsDev& g, int z, int y, int x) {
+  Range r;
+  r.z0 = max(-(g.wz / 2), -z);
+  r.z1 = min(g.wz - 1 - g.wz / 2, g.nz - 1 - z);
+  r.y0 = max(-(g.wy / 2), -y);
+  r.y1 = min(g.wy - 1 - g.wy / 2, g.ny - 1 - y);
+  r.x0 = max(-(g.wx / 2), -x);
+  r.x1 = min(g.wx - 1 - g.wx / 2, g.nx - 1 - x);
+  return r;
+}
+__device__ __forceinline__ float gibbs_w(const GibbsDev& g, int dz, int dy, int dx) {
+  return g.w[((dz + g.wz / 2) * g.wy + (dy + g.wy / 2)) * g.wx + (dx + g.wx / 2)];
+}
+
+// fixed-order block sum of one double per thread; thread 0 gets the total
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[kGibbsThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kGibbsThreads / 32; ++w) t += red[w];
+  return t;
+}
+
+// OP: 0 value, 1 gradient, 2 gradient times input, 3 Hessian diagonal, 4 accumulate Hessian times input
+template <typename Pot, int OP>
+__global__ void __launch_bounds__(kGibbsThreads) gibbs_kernel(const GibbsDev g, const Pot pot,
+                                                              const float* __restrict__ x,
+                                                              const float* __restrict__ in, float* __restrict__ out,
+                                                              double* __restrict__ partial) {
+  const int64_t n = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+  const int64_t j = static_cast<int64_t>(blockIdx.x) * kGibbsThreads + threadIdx.x;
+  double acc = 0.0;
+  if (j < n) {
+    int z, y, xx;
+    gibbs_coords(g, j, z, y, xx);
+    const Range r = gibbs_range(g, z, y, xx);
+    const float c = __ldg(x + j);
+    const float kj = g.kappa ? __ldg(g.kappa + j) : 1.f;
+    if (OP == 4) {
+      // accumulate_Hessian_times_input: float sums, the centre included
+      const float inj = __ldg(in + j);
+      float result = 0.f;
+      for (int dz = r.z0; dz <= r.z1; ++dz)
+        for (int dy = r.y0; dy <= r.y1; ++dy)
+          for (int dx = r.x0; dx <= r.x1; ++dx) {
+            const int64_t k = j + dz * g.sz + dy * g.sy + dx * g.sx;
+            const float nk = __ldg(x + k);
+            float current = gibbs_w(g, dz, dy, dx);
+            if (dz == 0 && dy == 0 && dx == 0)
+              current = static_cast<float>(current * (pot.d20(c, nk) * inj));
+            else
+              current = static_cast<float>(current * (pot.d20(c, nk) * inj + pot.d11(c, nk) * __ldg(in + k)));
+            if (g.kappa) current *= kj * __ldg(g.kappa + k);
+            result += current;
+          }
+      out[j] += 2 * result * g.beta;
+      return;
+    }
+    double sum = 0.0;
+    for (int dz = r.z0; dz <= r.z1; ++dz)
+      for (int dy = r.y0; dy <= r.y1; ++dy)
+        for (int dx = r.x0; dx <= r.x1; ++dx) {
+          if (dz == 0 && dy == 0 && dx == 0) continue;
+          const int64_t k = j + dz * g.sz + dy * g.sy + dx * g.sx;
+          const float nk = __ldg(x + k);
+          const double f = OP == 0 ? pot.value(c, nk) : (OP == 3 ? pot.d20(c, nk) : pot.d10(c, nk));
+          double current = gibbs_w(g, dz, dy, dx) * f;
+          if (g.kappa) current *= kj * __ldg(g.kappa + k);
+          sum += current;
+        }
+    if (OP == 1 || OP == 3)
+      out[j] = 2 * static_cast<float>(sum * g.beta);
+    else if (OP == 0)
+      acc = sum;
+    else
+      acc = 2 * sum * __ldg(in + j);
+  }
+  if (OP == 0 || OP == 2) {
+    const double t = block_sum(acc);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  }
+}
+
+// compute_Hessian of voxel (z, y, x): out (zeroed by the caller) gets the voxel's row of the Hessian; one thread
+// per neighbour
+template <typename Pot>
+__global__ void gibbs_hessian_voxel_kernel(const GibbsDev g, const Pot pot, const float* __restrict__ x, int z, int y,
+                                           int xx, float* __restrict__ out) {
+  const Range r = gibbs_range(g, z, y, xx);
+  const int ny = r.y1 - r.y0 + 1, nx = r.x1 - r.x0 + 1;
+  const int t = threadIdx.x;
+  if (t >= (r.z1 - r.z0 + 1) * ny * nx) return;
+  const int dz = r.z0 + t / (ny * nx), dy = r.y0 + (t / nx) % ny, dx = r.x0 + t % nx;
+  const int64_t j = static_cast<int64_t>(z) * g.sz + static_cast<int64_t>(y) * g.sy + static_cast<int64_t>(xx) * g.sx;
+  const float c = x[j];
+  float current = 0.f;
+  if (dz == 0 && dy == 0 && dx == 0) {
+    for (int ddz = r.z0; ddz <= r.z1; ++ddz)
+      for (int ddy = r.y0; ddy <= r.y1; ++ddy)
+        for (int ddx = r.x0; ddx <= r.x1; ++ddx) {
+          const int64_t k = j + ddz * g.sz + ddy * g.sy + ddx * g.sx;
+          float dc = static_cast<float>(gibbs_w(g, ddz, ddy, ddx) * 2 * pot.d20(c, x[k]));
+          if (g.kappa) dc *= g.kappa[j] * g.kappa[k];
+          current += dc;
+        }
+  } else {
+    const int64_t k = j + dz * g.sz + dy * g.sy + dx * g.sx;
+    current = static_cast<float>(gibbs_w(g, dz, dy, dx) * 2 * pot.d11(c, x[k]));
+    if (g.kappa) current *= g.kappa[j] * g.kappa[k];
+  }
+  out[j + dz * g.sz + dy * g.sy + dx * g.sx] = current * g.beta;
+}
+
+__global__ void gibbs_reduce_kernel(const double* __restrict__ partial, int n, double beta, double* __restrict__ out) {
+  // fixed order: thread t sums t, t + 256, ...; then the block sum in a fixed order
+  __shared__ double s[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) v += partial[i];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < 256; ++i) t += s[i];
+    *out = t * beta;
+  }
+}
+
+template <typename Pot>
+cudaError_t gibbs_launch_pot(const GibbsDev& g, const Pot& pot, int op, const float* x, const float* in, float* out,
+                             double* partial, double* result, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+  const int64_t blocks = (n + kGibbsThreads - 1) / kGibbsThreads;
+  if (blocks > 2147483647LL) return cudaErrorInvalidValue;
+  const unsigned nb = static_cast<unsigned>(blocks);
+  switch (op) {
+    case 0: gibbs_kernel<Pot, 0><<<nb, kGibbsThreads, 0, st>>>(g, pot, x, in, out, partial); break;
+    case 1: gibbs_kernel<Pot, 1><<<nb, kGibbsThreads, 0, st>>>(g, pot, x, in, out, partial); break;
+    case 2: gibbs_kernel<Pot, 2><<<nb, kGibbsThreads, 0, st>>>(g, pot, x, in, out, partial); break;
+    case 3: gibbs_kernel<Pot, 3><<<nb, kGibbsThreads, 0, st>>>(g, pot, x, in, out, partial); break;
+    case 4: gibbs_kernel<Pot, 4><<<nb, kGibbsThreads, 0, st>>>(g, pot, x, in, out, partial); break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (op == 0 || op == 2) gibbs_reduce_kernel<<<1, 256, 0, st>>>(partial, static_cast<int>(blocks), g.beta, result);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int64_t gibbs_num_partials(const GibbsDev& g) {
+  return (static_cast<int64_t>(g.nz) * g.ny * g.nx + kGibbsThreads - 1) / kGibbsThreads;
+}
+
+cudaError_t launch_gibbs(const GibbsDev& g, int op, const float* x, const float* in, float* out, double* partial,
+                         double* result, cudaStream_t st) {
+  if (g.potential == 1) return gibbs_launch_pot(g, QuadPot{}, op, x, in, out, partial, result, st);
+  return gibbs_launch_pot(g, RDPot{g.gamma, g.epsilon}, op, x, in, out, partial, result, st);
+}
+
+cudaError_t launch_gibbs_hessian_voxel(const GibbsDev& g, const float* x, int z, int y, int xx, float* out,
+                                       cudaStream_t st) {
+  const int threads = ((g.wz * g.wy * g.wx + 31) / 32) * 32;
+  if (g.potential == 1)
+    gibbs_hessian_voxel_kernel<<<1, threads, 0, st>>>(g, QuadPot{}, x, z, y, xx, out);
+  else
+    gibbs_hessian_voxel_kernel<<<1, threads, 0, st>>>(g, RDPot{g.gamma, g.epsilon}, x, z, y, xx, out);
+  return cudaGetLastError();
+}
+
+}  // namespace b200

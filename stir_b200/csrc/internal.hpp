@@ -300,6 +300,29 @@ cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny,
 // per segment: STIR [ax][view*tang] <-> device [view*tang][ax]
 cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
+// Gibbs penalty (gibbs.cu): image size and layout (0: [y][x][z], 1: [z][y][x]) with the strides of z, y, x;
+// weights [wz][wy][wx] with index ranges [-(w/2), w - 1 - w/2]
+constexpr int kGibbsMaxWeights = 343;
+struct GibbsDev {
+  int potential;  // 1 Quadratic, 2 Relative Difference
+  float beta, gamma, epsilon;
+  int nz, ny, nx, layout;
+  int64_t sz, sy, sx;
+  int wz, wy, wx;
+  const float* kappa;
+  float w[kGibbsMaxWeights];
+};
+// op: 0 value (-> *result, device), 1 gradient, 2 gradient times input (-> *result), 3 Hessian diagonal,
+// 4 out += Hessian times input; partial holds gibbs_num_partials() doubles
+int64_t gibbs_num_partials(const GibbsDev& g);
+cudaError_t launch_gibbs(const GibbsDev& g, int op, const float* x, const float* in, float* out, double* partial,
+                         double* result, cudaStream_t st);
+cudaError_t launch_gibbs_hessian_voxel(const GibbsDev& g, const float* x, int z, int y, int xx, float* out,
+                                       cudaStream_t st);
+
+// out[c * ld_out + r] = in[r * ld_in + c], r < rows, c < cols
+cudaError_t launch_transpose(const float* in, float* out, int rows, int64_t cols, int64_t ld_in, int64_t ld_out,
+                             cudaStream_t st);
 
 // deterministic back projection: contributions accumulated as int64 multiples of 1/scale
 cudaError_t launch_back_fixed(const ProjParams& p, const int* bin_list, int nbins, const float* projdata,

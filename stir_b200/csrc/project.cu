@@ -352,9 +352,10 @@ __global__ void __launch_bounds__(kThreads, kMinCtasBack) back_batch_kernel(cons
     back_bin<NPA, FloatAcc>(st.p, st.pb, smem, st.f.ratio, FloatAcc{st.f.u}, 0);
 }
 
-// image [z][y][x] <-> [y][x][z]: a transpose of (nz) x (ny*nx)
-__global__ void transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows, int64_t cols) {
-  // in: rows x cols, out: cols x rows
+// out[c * ld_out + r] = in[r * ld_in + c] for r < rows, c < cols: the image [z][y][x] <-> [y][x][z] and
+// projection data [axial][view, tangential] <-> [view, tangential][axial] layout changes, whole or a column range
+__global__ void transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows, int64_t cols,
+                                 int64_t ld_in, int64_t ld_out) {
   __shared__ float tile[32][33];
   const int64_t c0 = static_cast<int64_t>(blockIdx.x) * 32;
   const int r0 = blockIdx.y * 32;
@@ -362,23 +363,18 @@ __global__ void transpose_kernel(const float* __restrict__ in, float* __restrict
   for (int i = ty; i < 32; i += 8) {
     const int r = r0 + i;
     const int64_t c = c0 + tx;
-    if (r < rows && c < cols) tile[i][tx] = in[static_cast<int64_t>(r) * cols + c];
+    if (r < rows && c < cols) tile[i][tx] = in[static_cast<int64_t>(r) * ld_in + c];
   }
   __syncthreads();
   for (int i = ty; i < 32; i += 8) {
     const int64_t c = c0 + i;
     const int r = r0 + tx;
-    if (r < rows && c < cols) out[c * rows + r] = tile[tx][i];
+    if (r < rows && c < cols) out[c * ld_out + r] = tile[tx][i];
   }
 }
 
 cudaError_t transpose(const float* in, float* out, int rows, int64_t cols, cudaStream_t st) {
-  if (rows <= 0 || cols <= 0) return cudaSuccess;
-  const int64_t gx = (cols + 31) / 32;
-  const int64_t gy = (rows + 31) / 32;
-  if (gy > 65535 || gx > 2147483647LL) return cudaErrorInvalidValue;
-  transpose_kernel<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), dim3(32, 8), 0, st>>>(in, out, rows, cols);
-  return cudaGetLastError();
+  return launch_transpose(in, out, rows, cols, cols, rows, st);
 }
 
 }  // namespace
@@ -507,6 +503,17 @@ cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64
 }
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st) {
   return transpose(dev, stir, static_cast<int>(nvt), nax, st);
+}
+
+cudaError_t launch_transpose(const float* in, float* out, int rows, int64_t cols, int64_t ld_in, int64_t ld_out,
+                             cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t gx = (cols + 31) / 32;
+  const int64_t gy = (rows + 31) / 32;
+  if (gy > 65535 || gx > 2147483647LL) return cudaErrorInvalidValue;
+  transpose_kernel<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy)), dim3(32, 8), 0, st>>>(in, out, rows,
+                                                                                                      cols, ld_in, ld_out);
+  return cudaGetLastError();
 }
 
 }  // namespace b200

@@ -198,3 +198,35 @@ def test_unrestricted_fov_matches_oracle(cuda_device, oracle_lib):
     y = rng.uniform(0, 1, proj.projdata_size).astype(np.float32)
     assert rel_l2(proj.forward_host(x), orc.forward(x)) < REL_L2
     assert rel_l2(proj.back_host(y), orc.back(y)) < REL_L2
+
+
+@pytest.mark.parametrize("which", ["small", "rpt"])
+@pytest.mark.parametrize("subset", [(0, 1), (1, 4)])
+def test_host_api_matches_device_api(which, subset, small, rpt):
+    """The host-buffer entry points project group by group of views with the copies overlapped: the
+    forward projection equals the device entry point's bit for bit, the back projection to float
+    rounding; with pageable (numpy) and with pinned host buffers."""
+    import ctypes
+    import torch
+    pdi, img, proj, orc = small if which == "small" else rpt
+    rng = np.random.default_rng(41)
+    x = rng.uniform(0, 1, img.shape).astype(np.float32)
+    y = rng.uniform(0, 1, proj.projdata_size).astype(np.float32)
+    xd = proj.image_to_device_layout(torch.from_numpy(x).cuda())
+    out = torch.zeros(proj.projdata_size, device="cuda")
+    fd = proj.projdata_from_device_layout(proj.forward_dev(xd, out, *subset)).cpu().numpy()
+    assert np.array_equal(proj.forward_host(x, *subset), fd)
+    yd = proj.projdata_to_device_layout(torch.from_numpy(y).cuda())
+    bd = proj.image_from_device_layout(proj.back_dev(yd, None, *subset)).cpu().numpy()
+    assert rel_l2(proj.back_host(y, *subset), bd) < 1e-6
+    # pinned buffers (asynchronous copies)
+    x_pin = torch.from_numpy(x).pin_memory()
+    f_pin = torch.full((proj.projdata_size,), -1.0).pin_memory()
+    _abi.check(proj.lib.b200rt_forward_project(proj.h, ctypes.c_void_p(x_pin.data_ptr()),
+                                               ctypes.c_void_p(f_pin.data_ptr()), *subset), proj.h, "forward")
+    assert np.array_equal(f_pin.numpy(), fd)
+    y_pin = torch.from_numpy(y).pin_memory()
+    b_pin = torch.full(img.shape, -1.0).pin_memory()
+    _abi.check(proj.lib.b200rt_back_project(proj.h, ctypes.c_void_p(y_pin.data_ptr()), ctypes.c_void_p(b_pin.data_ptr()),
+                                            *subset, _abi.BACKPROJECT_ATOMIC), proj.h, "back")
+    assert rel_l2(b_pin.numpy(), bd) < 1e-6

@@ -59,6 +59,12 @@ extern "C" {
 #define B200RT_ATTENUATION_FACTORS 0 /* projdata = undo of ones: 1 / exp(A mu), the multiplicative factors */
 #define B200RT_ATTENUATION_APPLY 1   /* projdata *= exp(A mu)   (apply: attenuation correction) */
 #define B200RT_ATTENUATION_UNDO 2    /* projdata /= exp(A mu)   (undo: attenuate) */
+/* normalisation chains (b200rt_normalisation_dev) */
+#define B200RT_NORM_FACTORS 0 /* projdata = undo of ones: the multiplicative factors of the chain */
+#define B200RT_NORM_APPLY 1   /* apply every term in order (correction)                        */
+#define B200RT_NORM_UNDO 2    /* undo every term in order (the model's multiplicative effect)   */
+#define B200RT_NORM_PROJDATA 1    /* BinNormalisationFromProjData: factors as projection data   */
+#define B200RT_NORM_ATTENUATION 2 /* BinNormalisationFromAttenuationImage: a mu image (1/mm)    */
 
 /* priors (src/recon_buildblock/QuadraticPrior.cxx, RelativeDifferencePrior.cxx) */
 #define B200RT_PRIOR_NONE 0
@@ -275,6 +281,23 @@ int b200rt_prior_gradient_dev(b200rt_projector* h, const b200rt_prior* prior, co
  * (src/recon_buildblock/BinNormalisationFromAttenuationImage.cxx:122-170); non-TOF only, as STIR. */
 int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* projdata_dev, int mode, void* stream);
 
+/* One term of a normalisation chain: B200RT_NORM_PROJDATA with factors in device layout (non_tof = 1: factors of
+ * the non-TOF data serving every timing bin, as BinNormalisationFromProjData allows), or B200RT_NORM_ATTENUATION
+ * with a device-layout mu image. */
+typedef struct b200rt_norm_term {
+  int32_t kind;          /* B200RT_NORM_PROJDATA or B200RT_NORM_ATTENUATION */
+  int32_t non_tof;       /* projection-data factors without timing bins    */
+  const float* data_dev; /* the factors or the mu image                    */
+} b200rt_norm_term;
+
+/* ChainedBinNormalisation (src/recon_buildblock/ChainedBinNormalisation.cxx:91-143) of num_terms terms
+ * (BinNormalisationFromProjData.cxx:131-150, BinNormalisationFromAttenuationImage.cxx:138-170) on
+ * device-resident projection data (all bins, device layout): mode B200RT_NORM_APPLY applies the terms in order,
+ * B200RT_NORM_UNDO undoes them in order (as ChainedBinNormalisation::undo), B200RT_NORM_FACTORS writes the undo
+ * of ones (the multiplicative factors m of the Poisson model).  Attenuation terms need non-TOF data, as STIR. */
+int b200rt_normalisation_dev(b200rt_projector* h, const b200rt_norm_term* terms, int num_terms, int mode,
+                             float* projdata_dev, void* stream);
+
 /* accumulate_Hessian_times_input of the prior (QuadraticPrior.cxx:603-688, RelativeDifferencePrior.cxx:535-621):
  * output += beta sum_k w_jk (f20(x_j, x_k) in_j + f11(x_j, x_k) in_k) (kappa_j kappa_k) at x = image_dev;
  * device layout images. */
@@ -347,6 +370,48 @@ int b200rt_batch_set_config(b200rt_batch* b, const b200rt_batch_config* config);
 int b200rt_batch_get_config(const b200rt_batch* b, b200rt_batch_config* out);
 /* cancelled singularities of one frame in the last batched sub-iteration it took part in; synchronises */
 int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out);
+
+/* ---- projection data streams (ProjDataFromStream) ------------------------
+ * The bytes of a projection data file (from its data offset on, e.g. an Interfile ".s"), copied to the device
+ * as they are, converted to or from the device layout on the GPU: the element addressing of
+ * ProjDataFromStream::get_offset (src/buildblock/ProjDataFromStream.cxx:415-500), with the stream's number type,
+ * byte order and scale factor.  Views and tangential positions are the projector's; the stream holds
+ * num_segments segments in the order segment_sequence gives (num_axial_poss each) and num_timing_poss timing
+ * positions (timing position numbers in timing_poss_sequence, or min..max when NULL).  Segments of the stream
+ * that the projector does not use are skipped (as STIR with "maximum absolute segment number to process"); a
+ * segment of the projector missing from the stream, or with other axial sizes, is an error. */
+#define B200RT_STORAGE_SEGMENT_VIEW_AXIAL_TANG 0 /* Segment_View_AxialPos_TangPos (Timing_ outermost with TOF) */
+#define B200RT_STORAGE_SEGMENT_AXIAL_VIEW_TANG 1 /* Segment_AxialPos_View_TangPos (Timing_ outermost with TOF) */
+#define B200RT_NUMBER_SCHAR 0  /* NumericType::SCHAR  */
+#define B200RT_NUMBER_UCHAR 1  /* NumericType::UCHAR  */
+#define B200RT_NUMBER_SHORT 2  /* NumericType::SHORT  */
+#define B200RT_NUMBER_USHORT 3 /* NumericType::USHORT */
+#define B200RT_NUMBER_INT 4    /* NumericType::INT    */
+#define B200RT_NUMBER_UINT 5   /* NumericType::UINT   */
+#define B200RT_NUMBER_FLOAT 6  /* NumericType::FLOAT  */
+#define B200RT_NUMBER_DOUBLE 7 /* NumericType::DOUBLE */
+
+typedef struct b200rt_stream_format {
+  int32_t storage_order;               /* B200RT_STORAGE_*                                            */
+  int32_t number_type;                 /* B200RT_NUMBER_*                                             */
+  int32_t swap_bytes;                  /* 1: the stream's byte order is not the host's                */
+  float scale_factor;                  /* read: value = stored * scale_factor; write: must be 1       */
+  int32_t num_segments;                /* segments in the stream                                      */
+  const int32_t* segment_sequence;     /* host: segment number of the stream's i-th segment           */
+  const int32_t* num_axial_poss;       /* host: axial positions of the stream's i-th segment          */
+  int32_t num_timing_poss;             /* timing positions in the stream (1: non-TOF)                 */
+  const int32_t* timing_poss_sequence; /* host: timing position number of the i-th, or NULL (min..max) */
+} b200rt_stream_format;
+
+/* bytes a stream of this format holds for the projector's views and tangential positions */
+int b200rt_stream_bytes(b200rt_projector* h, const b200rt_stream_format* fmt, int64_t* bytes);
+/* read: stream_dev (stream_bytes long, any alignment) -> projdata_dev (device layout, every bin written) */
+int b200rt_projdata_from_stream_dev(b200rt_projector* h, const void* stream_dev, int64_t stream_bytes,
+                                    const b200rt_stream_format* fmt, float* projdata_dev, void* stream);
+/* write (ProjDataFromStream::set_segment with a float or double stream): the projector's segments into their
+ * places in stream_dev; other bytes are left as they are */
+int b200rt_projdata_to_stream_dev(b200rt_projector* h, const float* projdata_dev, const b200rt_stream_format* fmt,
+                                  void* stream_dev, int64_t stream_bytes, void* stream);
 
 /* ---- Gibbs penalties on device-resident images ---------------------------
  * GibbsQuadraticPenalty and GibbsRelativeDifferencePenalty (src/include/stir/recon_buildblock/GibbsPenalty.h,

@@ -119,6 +119,44 @@ class BatchConfig(ctypes.Structure):
     ]
 
 
+NORM_FACTORS = 0
+NORM_APPLY = 1
+NORM_UNDO = 2
+NORM_PROJDATA = 1
+NORM_ATTENUATION = 2
+
+
+class NormTerm(ctypes.Structure):
+    """b200rt_norm_term"""
+
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("non_tof", ctypes.c_int32),
+        ("data_dev", ctypes.c_void_p),
+    ]
+
+
+STORAGE_SEGMENT_VIEW_AXIAL_TANG = 0
+STORAGE_SEGMENT_AXIAL_VIEW_TANG = 1
+NUMBER_TYPES = {"schar": 0, "uchar": 1, "short": 2, "ushort": 3, "int": 4, "uint": 5, "float": 6, "double": 7}
+
+
+class StreamFormat(ctypes.Structure):
+    """b200rt_stream_format"""
+
+    _fields_ = [
+        ("storage_order", ctypes.c_int32),
+        ("number_type", ctypes.c_int32),
+        ("swap_bytes", ctypes.c_int32),
+        ("scale_factor", ctypes.c_float),
+        ("num_segments", ctypes.c_int32),
+        ("segment_sequence", ctypes.POINTER(ctypes.c_int32)),
+        ("num_axial_poss", ctypes.POINTER(ctypes.c_int32)),
+        ("num_timing_poss", ctypes.c_int32),
+        ("timing_poss_sequence", ctypes.POINTER(ctypes.c_int32)),
+    ]
+
+
 GIBBS_QUADRATIC = 1
 GIBBS_RELATIVE_DIFFERENCE = 2
 LAYOUT_DEVICE = 0  # [y][x][z]
@@ -200,6 +238,10 @@ EXPORTS = [
     ("b200rt_batch_set_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
     ("b200rt_batch_get_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
     ("b200rt_batch_get_num_cancelled", _I, [_P, _I, ctypes.POINTER(_I64)]),
+    ("b200rt_normalisation_dev", _I, [_P, ctypes.POINTER(NormTerm), _I, _I, _P, _P]),
+    ("b200rt_stream_bytes", _I, [_P, ctypes.POINTER(StreamFormat), ctypes.POINTER(_I64)]),
+    ("b200rt_projdata_from_stream_dev", _I, [_P, _P, _I64, ctypes.POINTER(StreamFormat), _P, _P]),
+    ("b200rt_projdata_to_stream_dev", _I, [_P, _P, ctypes.POINTER(StreamFormat), _P, _I64, _P]),
     ("b200rt_gibbs_create", _I, [ctypes.POINTER(GibbsParams), _I, ctypes.POINTER(_P)]),
     ("b200rt_gibbs_destroy", None, [_P]),
     ("b200rt_gibbs_last_error", ctypes.c_char_p, [_P]),

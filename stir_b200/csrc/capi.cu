@@ -1524,6 +1524,53 @@ int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* proj
   }
 }
 
+int b200rt_normalisation_dev(b200rt_projector* h, const b200rt_norm_term* terms, int num_terms, int mode,
+                             float* projdata_dev, void* stream) {
+  if (!h || !projdata_dev || (num_terms > 0 && !terms) || num_terms < 0)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (mode < B200RT_NORM_FACTORS || mode > B200RT_NORM_UNDO)
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown normalisation mode");
+  const Geometry& g = *h->geo;
+  for (int t = 0; t < num_terms; ++t) {
+    if (!terms[t].data_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null normalisation data");
+    if (terms[t].kind == B200RT_NORM_ATTENUATION) {
+      if (g.num_tof() > 1)
+        return fail(h, B200RT_ERR_UNSUPPORTED,
+                    "BinNormalisationFromAttenuationImage limitation: currently can only handle non_TOF data.");
+    } else if (terms[t].kind != B200RT_NORM_PROJDATA) {
+      return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown normalisation kind");
+    }
+  }
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = g.projdata_size();
+    int step = mode;
+    if (mode == B200RT_NORM_FACTORS) {
+      ck(launch_fill(projdata_dev, n, 1.f, st), "fill");
+      step = B200RT_NORM_UNDO;
+    }
+    for (int t = 0; t < num_terms; ++t) {
+      if (terms[t].kind == B200RT_NORM_PROJDATA) {
+        const int64_t fstride = (terms[t].non_tof && g.num_tof() > 1) ? g.tof_stride() : 0;
+        ck(launch_norm_projdata(terms[t].data_dev, projdata_dev, n, fstride, step, st), "normalisation");
+      } else {
+        if (!h->ratio.p) {
+          h->ratio.alloc(n);
+          ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * n, st), "memset");
+        }
+        forward_subset(*h, terms[t].data_dev, h->ratio.p, 0, 1, st);
+        ck(launch_attenuation(h->ratio.p, projdata_dev, n,
+                              step == B200RT_NORM_APPLY ? B200RT_ATTENUATION_APPLY : B200RT_ATTENUATION_UNDO, st),
+           "attenuation");
+      }
+    }
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_ossps_denominator_dev(b200rt_projector* h, const float* y_dev, const float* norm_dev, float* denominator_dev,
                                  int back_projection_mode, void* stream) {
   if (!h || !y_dev || !denominator_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
@@ -2268,6 +2315,118 @@ int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out) {
 
 }  // extern "C"
 
+/* ---- projection data streams ------------------------------------------- */
+namespace {
+
+// the stream's segment groups for the projector's segments and timing positions; throws on a mismatch
+std::vector<StreamSegment> stream_plan(const Geometry& g, const b200rt_stream_format& f, int64_t& total_elems) {
+  if (f.storage_order != B200RT_STORAGE_SEGMENT_VIEW_AXIAL_TANG && f.storage_order != B200RT_STORAGE_SEGMENT_AXIAL_VIEW_TANG)
+    throw std::invalid_argument("unsupported storage order");
+  if (numeric_type_size(f.number_type) == 0) throw std::invalid_argument("unknown number type");
+  if (f.num_segments < 1 || !f.segment_sequence || !f.num_axial_poss)
+    throw std::invalid_argument("the stream needs its segment sequence and axial sizes");
+  if (f.num_timing_poss != g.num_tof())
+    throw std::invalid_argument("the stream's number of timing positions differs from the projector's");
+  const int64_t nvt = static_cast<int64_t>(g.num_views()) * g.num_tang();
+  int64_t size3d = 0;
+  for (int i = 0; i < f.num_segments; ++i) {
+    if (f.num_axial_poss[i] < 0) throw std::invalid_argument("negative axial size");
+    size3d += f.num_axial_poss[i] * nvt;
+  }
+  total_elems = size3d * f.num_timing_poss;
+  std::vector<StreamSegment> plan;
+  for (int k = 0; k < g.num_tof(); ++k) {
+    int ti = k;  // the stream's index of timing position min_tof + k
+    if (f.timing_poss_sequence) {
+      ti = -1;
+      for (int i = 0; i < f.num_timing_poss; ++i)
+        if (f.timing_poss_sequence[i] == g.min_tof() + k) ti = i;
+      if (ti < 0) throw std::invalid_argument("a timing position of the projector is missing from the stream");
+    }
+    for (int s = -g.S(); s <= g.S(); ++s) {
+      int64_t off = 0;
+      int idx = -1;
+      for (int i = 0; i < f.num_segments && idx < 0; ++i) {
+        if (f.segment_sequence[i] == s)
+          idx = i;
+        else
+          off += f.num_axial_poss[i] * nvt;
+      }
+      if (idx < 0) throw std::invalid_argument("segment " + std::to_string(s) + " is missing from the stream");
+      if (f.num_axial_poss[idx] != g.nax(s))
+        throw std::invalid_argument("segment " + std::to_string(s) + " has another number of axial positions");
+      StreamSegment ss{};
+      ss.order = f.storage_order == B200RT_STORAGE_SEGMENT_AXIAL_VIEW_TANG ? kStorageSegmentAxialViewTang
+                                                                           : kStorageSegmentViewAxialTang;
+      ss.type = f.number_type;
+      ss.swap = f.swap_bytes ? 1 : 0;
+      ss.scale = f.scale_factor;
+      ss.nax = g.nax(s);
+      ss.nv = g.num_views();
+      ss.nt = g.num_tang();
+      ss.stream_elem = ti * size3d + off;
+      ss.dev_off = k * g.tof_stride() + g.dev_segment_offset(s);
+      plan.push_back(ss);
+    }
+  }
+  return plan;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200rt_stream_bytes(b200rt_projector* h, const b200rt_stream_format* fmt, int64_t* bytes) {
+  if (!h || !fmt || !bytes) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    int64_t n = 0;
+    stream_plan(*h->geo, *fmt, n);
+    *bytes = n * numeric_type_size(fmt->number_type);
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_projdata_from_stream_dev(b200rt_projector* h, const void* stream_dev, int64_t stream_bytes,
+                                    const b200rt_stream_format* fmt, float* projdata_dev, void* stream) {
+  if (!h || !stream_dev || !fmt || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    int64_t n = 0;
+    const std::vector<StreamSegment> plan = stream_plan(*h->geo, *fmt, n);
+    if (stream_bytes < n * numeric_type_size(fmt->number_type))
+      return fail(h, B200RT_ERR_INVALID_ARGUMENT, "the stream is shorter than its format says");
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (const StreamSegment& ss : plan) ck(launch_stream_segment(ss, true, stream_dev, projdata_dev, st), "stream read");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_projdata_to_stream_dev(b200rt_projector* h, const float* projdata_dev, const b200rt_stream_format* fmt,
+                                  void* stream_dev, int64_t stream_bytes, void* stream) {
+  if (!h || !stream_dev || !fmt || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (fmt->number_type != B200RT_NUMBER_FLOAT && fmt->number_type != B200RT_NUMBER_DOUBLE)
+    return fail(h, B200RT_ERR_UNSUPPORTED, "streams are written as float or double");
+  if (fmt->scale_factor != 1.f) return fail(h, B200RT_ERR_UNSUPPORTED, "streams are written with scale factor 1");
+  try {
+    int64_t n = 0;
+    const std::vector<StreamSegment> plan = stream_plan(*h->geo, *fmt, n);
+    if (stream_bytes < n * numeric_type_size(fmt->number_type))
+      return fail(h, B200RT_ERR_INVALID_ARGUMENT, "the stream is shorter than its format says");
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (const StreamSegment& ss : plan) ck(launch_stream_segment(ss, false, projdata_dev, stream_dev, st), "stream write");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+}  // extern "C"
+
 /* ---- Gibbs penalties ---------------------------------------------------- */
 struct b200rt_gibbs {
   int device = 0;
@@ -2331,6 +2490,8 @@ int b200rt_gibbs_create(const b200rt_gibbs_params* p, int device, b200rt_gibbs**
   if (p->potential != B200RT_GIBBS_QUADRATIC && p->potential != B200RT_GIBBS_RELATIVE_DIFFERENCE)
     return create_fail(B200RT_ERR_INVALID_ARGUMENT, "unknown Gibbs potential");
   if (p->nz < 1 || p->ny < 1 || p->nx < 1) return create_fail(B200RT_ERR_INVALID_ARGUMENT, "empty image");
+  if (static_cast<int64_t>(p->nz) * p->ny * p->nx >= (int64_t(1) << 31))
+    return create_fail(B200RT_ERR_TOO_LARGE, "image of 2^31 voxels or more");
   if (p->layout != B200RT_LAYOUT_DEVICE && p->layout != B200RT_LAYOUT_STIR)
     return create_fail(B200RT_ERR_INVALID_ARGUMENT, "unknown image layout");
   int ndev = 0;

@@ -28,48 +28,54 @@ struct QuadPot {
   __device__ __forceinline__ double d11(float, float) const { return -0.5; }
 };
 
-// float operands; the double literals 0.5 and 1.0 make those operations double, and the results assigned to
-// float variables are rounded to float, as in the reference's expressions
+// The reference evaluates with float operands, the double literals 0.5 and 1.0 making those operations double
+// and the results assigned to floats rounded back.  Each such double step equals a float step here:
+//  - (float)(1.0 / (double)v) is the correctly rounded float reciprocal of v (division of two floats rounded first
+//    to 53 bits, then to 24: double rounding is innocuous when 53 >= 2*24 + 2, Figueroa 1995), __frcp_rn(v);
+//  - (float)(0.5 * (double)a * (double)b) with float a, b is (0.5f * a) * b: 0.5 a is exact, the double product of
+//    two floats is exact, so one rounding to float remains, as in the float product;
+//  - (float)(0.5 * (double)(d * d)) is 0.5f * (d * d) (exact scaling).
+// so every value is bit-identical to the reference's expression without double divisions.
 struct RDPot {
   float gamma, epsilon;
   __device__ __forceinline__ double value(float c, float n) const {
     const float diff = c - n;
     const float add = c + n;
-    const float num = static_cast<float>(0.5 * static_cast<double>(diff * diff));
-    const float den = static_cast<float>(1.0 / static_cast<double>(add + gamma * fabsf(diff) + epsilon));
+    const float num = 0.5f * (diff * diff);
+    const float den = __frcp_rn(add + gamma * fabsf(diff) + epsilon);
     return static_cast<double>(num * den);
   }
   __device__ __forceinline__ double d10(float c, float n) const {
     const float diff = c - n;
     const float factor = c + n + gamma * fabsf(diff) + epsilon;
-    const float num = static_cast<float>(0.5 * static_cast<double>(diff) * static_cast<double>(factor + 2 * n + epsilon));
-    const float den = static_cast<float>(1.0 / static_cast<double>(factor * factor));
+    const float num = (0.5f * diff) * (factor + 2 * n + epsilon);
+    const float den = __frcp_rn(factor * factor);
     return static_cast<double>(num * den);
   }
   __device__ __forceinline__ double d20(float c, float n) const {
     const float num = 2 * n + epsilon;
-    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * fabsf(c - n) + epsilon));
+    const float den = __frcp_rn(c + n + gamma * fabsf(c - n) + epsilon);
     return static_cast<double>(num * num * den * den * den);
   }
   __device__ __forceinline__ double d11(float c, float n) const {
     const float num = -(2 * c + epsilon) * (2 * n + epsilon);
-    const float den = static_cast<float>(1.0 / static_cast<double>(c + n + gamma * fabsf(c - n) + epsilon));
+    const float den = __frcp_rn(c + n + gamma * fabsf(c - n) + epsilon);
     return static_cast<double>(num * den * den * den);
   }
 };
 
 // the voxel (z, y, x) of memory index i
-__device__ __forceinline__ void gibbs_coords(const GibbsDev& g, int64_t i, int& z, int& y, int& x) {
+__device__ __forceinline__ void gibbs_coords(const GibbsDev& g, int i, int& z, int& y, int& x) {
   if (g.layout == 0) {  // [y][x][z]
-    z = static_cast<int>(i % g.nz);
-    const int64_t t = i / g.nz;
-    x = static_cast<int>(t % g.nx);
-    y = static_cast<int>(t / g.nx);
+    z = i % g.nz;
+    const int t = i / g.nz;
+    x = t % g.nx;
+    y = t / g.nx;
   } else {  // [z][y][x]
-    x = static_cast<int>(i % g.nx);
-    const int64_t t = i / g.nx;
-    y = static_cast<int>(t % g.ny);
-    z = static_cast<int>(t / g.ny);
+    x = i % g.nx;
+    const int t = i / g.nx;
+    y = t % g.ny;
+    z = t / g.ny;
   }
 }
 
@@ -102,54 +108,80 @@ __device__ __forceinline__ double block_sum(double v) {
   return t;
 }
 
-// OP: 0 value, 1 gradient, 2 gradient times input, 3 Hessian diagonal, 4 accumulate Hessian times input
+// one neighbour's term of the per-voxel sums, in the reference's types
+template <typename Pot, int OP>
+__device__ __forceinline__ void gibbs_term(const Pot& pot, float w, float c, float nk, float kk, float inj, float ink,
+                                           bool centre, const float* kappa, double& sum, float& result) {
+  if (OP == 4) {
+    float current = w;
+    if (centre)
+      current = static_cast<float>(current * (pot.d20(c, nk) * inj));
+    else
+      current = static_cast<float>(current * (pot.d20(c, nk) * inj + pot.d11(c, nk) * ink));
+    if (kappa) current *= kk;
+    result += current;
+  } else {
+    if (centre) return;
+    const double f = OP == 0 ? pot.value(c, nk) : (OP == 3 ? pot.d20(c, nk) : pot.d10(c, nk));
+    double current = w * f;
+    if (kappa) current *= kk;
+    sum += current;
+  }
+}
+
+// OP: 0 value, 1 gradient, 2 gradient times input, 3 Hessian diagonal, 4 accumulate Hessian times input.
+// Voxels whose whole neighbourhood lies in the image take an unrolled path when the weights are 3x3x3 or 1x3x3
+// (the default weights and STIR's usual explicit ones), with the same order of terms as the general loop.
 template <typename Pot, int OP>
 __global__ void __launch_bounds__(kGibbsThreads) gibbs_kernel(const GibbsDev g, const Pot pot,
                                                               const float* __restrict__ x,
                                                               const float* __restrict__ in, float* __restrict__ out,
                                                               double* __restrict__ partial) {
-  const int64_t n = static_cast<int64_t>(g.nz) * g.ny * g.nx;
-  const int64_t j = static_cast<int64_t>(blockIdx.x) * kGibbsThreads + threadIdx.x;
+  const int n = g.nz * g.ny * g.nx;  // < 2^31, checked at set-up
+  const int j = blockIdx.x * kGibbsThreads + threadIdx.x;
   double acc = 0.0;
   if (j < n) {
     int z, y, xx;
     gibbs_coords(g, j, z, y, xx);
-    const Range r = gibbs_range(g, z, y, xx);
+    const int sz = static_cast<int>(g.sz), sy = static_cast<int>(g.sy), sx = static_cast<int>(g.sx);
     const float c = __ldg(x + j);
     const float kj = g.kappa ? __ldg(g.kappa + j) : 1.f;
-    if (OP == 4) {
-      // accumulate_Hessian_times_input: float sums, the centre included
-      const float inj = __ldg(in + j);
-      float result = 0.f;
+    const float inj = (OP == 4) ? __ldg(in + j) : 0.f;
+    double sum = 0.0;
+    float result = 0.f;
+    const bool in3 = y >= 1 && y + 1 < g.ny && xx >= 1 && xx + 1 < g.nx;
+    if (g.wy == 3 && g.wx == 3 && g.wz == 3 && in3 && z >= 1 && z + 1 < g.nz) {
+#pragma unroll
+      for (int t = 0; t < 27; ++t) {
+        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+        const int k = j + dz * sz + dy * sy + dx * sx;
+        const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
+        gibbs_term<Pot, OP>(pot, g.w[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 13, g.kappa,
+                            sum, result);
+      }
+    } else if (g.wy == 3 && g.wx == 3 && g.wz == 1 && in3) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const int dy = t / 3 - 1, dx = t % 3 - 1;
+        const int k = j + dy * sy + dx * sx;
+        const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
+        gibbs_term<Pot, OP>(pot, g.w[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 4, g.kappa,
+                            sum, result);
+      }
+    } else {
+      const Range r = gibbs_range(g, z, y, xx);
       for (int dz = r.z0; dz <= r.z1; ++dz)
         for (int dy = r.y0; dy <= r.y1; ++dy)
           for (int dx = r.x0; dx <= r.x1; ++dx) {
-            const int64_t k = j + dz * g.sz + dy * g.sy + dx * g.sx;
-            const float nk = __ldg(x + k);
-            float current = gibbs_w(g, dz, dy, dx);
-            if (dz == 0 && dy == 0 && dx == 0)
-              current = static_cast<float>(current * (pot.d20(c, nk) * inj));
-            else
-              current = static_cast<float>(current * (pot.d20(c, nk) * inj + pot.d11(c, nk) * __ldg(in + k)));
-            if (g.kappa) current *= kj * __ldg(g.kappa + k);
-            result += current;
+            const int k = j + dz * sz + dy * sy + dx * sx;
+            const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
+            gibbs_term<Pot, OP>(pot, gibbs_w(g, dz, dy, dx), c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f,
+                                dz == 0 && dy == 0 && dx == 0, g.kappa, sum, result);
           }
-      out[j] += 2 * result * g.beta;
-      return;
     }
-    double sum = 0.0;
-    for (int dz = r.z0; dz <= r.z1; ++dz)
-      for (int dy = r.y0; dy <= r.y1; ++dy)
-        for (int dx = r.x0; dx <= r.x1; ++dx) {
-          if (dz == 0 && dy == 0 && dx == 0) continue;
-          const int64_t k = j + dz * g.sz + dy * g.sy + dx * g.sx;
-          const float nk = __ldg(x + k);
-          const double f = OP == 0 ? pot.value(c, nk) : (OP == 3 ? pot.d20(c, nk) : pot.d10(c, nk));
-          double current = gibbs_w(g, dz, dy, dx) * f;
-          if (g.kappa) current *= kj * __ldg(g.kappa + k);
-          sum += current;
-        }
-    if (OP == 1 || OP == 3)
+    if (OP == 4)
+      out[j] += 2 * result * g.beta;
+    else if (OP == 1 || OP == 3)
       out[j] = 2 * static_cast<float>(sum * g.beta);
     else if (OP == 0)
       acc = sum;

@@ -300,6 +300,20 @@ cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny,
 // per segment: STIR [ax][view*tang] <-> device [view*tang][ax]
 cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
+// Projection data streams (stream.cu): NumericType codes and storage orders as b200rt_stream_format
+constexpr int kNumSChar = 0, kNumUChar = 1, kNumShort = 2, kNumUShort = 3, kNumInt = 4, kNumUInt = 5, kNumFloat = 6,
+              kNumDouble = 7;
+constexpr int kStorageSegmentViewAxialTang = 0, kStorageSegmentAxialViewTang = 1;
+// one segment of one timing position: its first element in the stream, its first float in the device layout
+struct StreamSegment {
+  int order, type, swap;
+  float scale;
+  int nax, nv, nt;
+  int64_t stream_elem, dev_off;
+};
+int numeric_type_size(int type);  // 0 for an unknown type
+cudaError_t launch_stream_segment(const StreamSegment& s, bool to_dev, const void* in, void* out, cudaStream_t st);
+
 // Gibbs penalty (gibbs.cu): image size and layout (0: [y][x][z], 1: [z][y][x]) with the strides of z, y, x;
 // weights [wz][wy][wx] with index ranges [-(w/2), w - 1 - w/2]
 constexpr int kGibbsMaxWeights = 343;
@@ -342,6 +356,8 @@ cudaError_t launch_hessian_ratio(float* fp, const float* y, const float* norm, c
 cudaError_t launch_ossps_update(float* x, float* den, const float* g, float* pg, const float* sens, const b200rt_prior* prior,
                                 const float prior_weights[27], int ny, int nx, int nz, int num_subsets, int first,
                                 float relax, float upper, float* partial, float* minpos, cudaStream_t st);
+cudaError_t launch_norm_projdata(const float* factors, float* projdata, int64_t n, int64_t fstride, int mode,
+                                 cudaStream_t st);
 cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int64_t n, int mode, cudaStream_t st);
 cudaError_t launch_fixed_to_float(const unsigned long long* acc, const double* scale, float* image, int64_t n,
                                   cudaStream_t st);

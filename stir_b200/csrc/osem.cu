@@ -362,6 +362,30 @@ __global__ void attenuation_kernel(const float* __restrict__ line_integrals, flo
   }
 }
 
+// BinNormalisationFromProjData (BinNormalisationFromProjData.cxx:131-150): apply multiplies by the factors, undo
+// divides by them (no guard, as the viewgram division); factors of non-TOF data serve every timing bin (period
+// fstride), factors = undo of ones
+__global__ void norm_projdata_kernel(const float* __restrict__ f, float* __restrict__ pd, int64_t n, int64_t fstride,
+                                     int mode) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float v = f[fstride > 0 ? i % fstride : i];
+    if (mode == B200RT_NORM_FACTORS)
+      pd[i] = 1.F / v;
+    else if (mode == B200RT_NORM_APPLY)
+      pd[i] *= v;
+    else
+      pd[i] /= v;
+  }
+}
+
+cudaError_t launch_norm_projdata(const float* factors, float* projdata, int64_t n, int64_t fstride, int mode,
+                                 cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  norm_projdata_kernel<<<update_num_blocks(n), 256, 0, st>>>(factors, projdata, n, fstride, mode);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_attenuation(const float* line_integrals, float* projdata, int64_t n, int mode, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   attenuation_kernel<<<update_num_blocks(n), 256, 0, st>>>(line_integrals, projdata, n, mode);

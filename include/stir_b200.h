@@ -371,6 +371,42 @@ int b200rt_batch_get_config(const b200rt_batch* b, b200rt_batch_config* out);
 /* cancelled singularities of one frame in the last batched sub-iteration it took part in; synchronises */
 int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out);
 
+/* ---- list-mode objective (PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByBin) ----
+ * Events as STIR's cached BinAndCorr records (the bin with its value, the additive term), in a device array.
+ * Each event's row is the cached basic row with the event's symmetry operation and axial shift; an event belongs
+ * to subset s of n when its basic bin's view mod n is s (LM_distributable_computation,
+ * src/include/stir/recon_buildblock/distributable.txx:36-140).  Events whose bin lies outside the projector's data
+ * are skipped and counted (b200rt_listmode_num_invalid); events of value 0 are skipped as STIR does. */
+typedef struct b200rt_lm_event {
+  int32_t segment, view, axial_pos, tangential_pos, timing_pos; /* Bin (timing_pos 0 for non-TOF)      */
+  float value;                                                  /* the bin value: counts (usually 1)   */
+  float corr;                                                   /* the additive term (used if has_add)  */
+} b200rt_lm_event;
+
+/* actual_compute_subset_gradient_without_penalty (…ListModeDataWithProjMatrixByBin.cxx:900-955) with
+ * LM_gradient_and_value<true,false> (:750-785): gradient (+)= sum_e A_e^T (y_e / (A_e x + c_e)) over the subset's
+ * events; accumulate = 0 zeroes gradient_dev first; subset_sensitivity_dev != NULL subtracts it afterwards
+ * (add_sensitivity = false), NULL leaves the sum (add_sensitivity = true). */
+int b200rt_listmode_gradient_dev(b200rt_projector* h, const b200rt_lm_event* events_dev, int64_t num_events,
+                                 const float* image_dev, int subset_num, int num_subsets, int has_add,
+                                 const float* subset_sensitivity_dev, int accumulate, float* gradient_dev,
+                                 void* stream);
+/* actual_compute_objective_function_without_penalty (:866-898) with LM_gradient_and_value<false,true>:
+ * -sum_e y_e log(A_e x + c_e), a cancelled event (y > 1e4 (A x + c)) giving -y log(y / 1e4); FP64, fixed order.
+ * The reference's inner product with the sensitivity (:895-898) discards its result, so it is not part of the
+ * value.  Synchronises and writes *value. */
+int b200rt_listmode_value_dev(b200rt_projector* h, const b200rt_lm_event* events_dev, int64_t num_events,
+                              const float* image_dev, int subset_num, int num_subsets, int has_add, double* value,
+                              void* stream);
+/* actual_accumulate_sub_Hessian_times_input_without_penalty (:957-1000) with LM_Hessian (:787-820):
+ * output += sum_e A_e^T (-y_e / (A_e x + c_e)^2 A_e rhs), skipping cancelled events and A_e rhs = 0. */
+int b200rt_listmode_hessian_times_input_dev(b200rt_projector* h, const b200rt_lm_event* events_dev,
+                                            int64_t num_events, const float* image_dev, const float* rhs_dev,
+                                            int subset_num, int num_subsets, int has_add, float* output_dev,
+                                            void* stream);
+/* events skipped as outside the projection data since the last call of this function; synchronises */
+int b200rt_listmode_num_invalid(b200rt_projector* h, int64_t* count);
+
 /* ---- projection data streams (ProjDataFromStream) ------------------------
  * The bytes of a projection data file (from its data offset on, e.g. an Interfile ".s"), copied to the device
  * as they are, converted to or from the device layout on the GPU: the element addressing of
@@ -394,7 +430,7 @@ int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out);
 typedef struct b200rt_stream_format {
   int32_t storage_order;               /* B200RT_STORAGE_*                                            */
   int32_t number_type;                 /* B200RT_NUMBER_*                                             */
-  int32_t swap_bytes;                  /* 1: the stream's byte order is not the host's                */
+  int32_t swap_bytes;                  /* 1: the stream is big-endian (the GPU's order is little)      */
   float scale_factor;                  /* read: value = stored * scale_factor; write: must be 1       */
   int32_t num_segments;                /* segments in the stream                                      */
   const int32_t* segment_sequence;     /* host: segment number of the stream's i-th segment           */

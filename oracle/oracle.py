@@ -356,3 +356,35 @@ def ref_ray_trace(start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity=1 <<
         _ref.ref_ray_trace.restype = _I64
         _ref.ref_ray_trace.argtypes = [_P, _P, _P, _F, _P, _P, _I64]
     return _trace(_ref.ref_ray_trace, start_zyx, stop_zyx, voxel_size_zyx, norm_const, capacity)
+
+
+# ---- projection data streams: ProjDataFromStream::get_offset (src/buildblock/ProjDataFromStream.cxx:415-500) ----
+NUMPY_TYPES = {"schar": "i1", "uchar": "u1", "short": "i2", "ushort": "u2", "int": "i4", "uint": "u4", "float": "f4",
+               "double": "f8"}
+
+
+def projdata_from_stream(raw, geometry: _abi.Geometry, storage_order, number_type, big_endian, scale_factor,
+                         segment_sequence, num_axial_poss, num_timing_poss=1, timing_poss_sequence=None,
+                         min_timing_pos_num=0):
+    """The projector's bins in ProjDataInMemory order (segments 0, +1, -1, ..., then axial, view, tangential;
+    timing positions outermost) read from the bytes of a stream, element by element as get_offset addresses them."""
+    dt = np.dtype(NUMPY_TYPES[number_type]).newbyteorder(">" if big_endian else "<")
+    data = np.frombuffer(bytes(raw), dtype=dt)
+    nv, nt, S = geometry.num_views, geometry.num_tangential_poss, geometry.max_segment_num
+    size3d = sum(num_axial_poss) * nv * nt
+    ntof = num_timing_poss
+    order = [0] + [s for k in range(1, S + 1) for s in (k, -k)]
+    out = []
+    for k in range(ntof):
+        ti = k if timing_poss_sequence is None else list(timing_poss_sequence).index(min_timing_pos_num + k)
+        for s in order:
+            i = list(segment_sequence).index(s)
+            nax = num_axial_poss[i]
+            off = ti * size3d + sum(num_axial_poss[:i]) * nv * nt
+            seg = data[off:off + nax * nv * nt].astype(np.float64)
+            if storage_order == _abi.STORAGE_SEGMENT_AXIAL_VIEW_TANG:
+                seg = seg.reshape(nax, nv, nt)
+            else:
+                seg = seg.reshape(nv, nax, nt).transpose(1, 0, 2)
+            out.append((seg.astype(np.float32) * np.float32(scale_factor)).astype(np.float32).ravel())
+    return np.concatenate(out)

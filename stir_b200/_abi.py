@@ -136,6 +136,20 @@ class NormTerm(ctypes.Structure):
     ]
 
 
+class LmEvent(ctypes.Structure):
+    """b200rt_lm_event"""
+
+    _fields_ = [
+        ("segment", ctypes.c_int32),
+        ("view", ctypes.c_int32),
+        ("axial_pos", ctypes.c_int32),
+        ("tangential_pos", ctypes.c_int32),
+        ("timing_pos", ctypes.c_int32),
+        ("value", ctypes.c_float),
+        ("corr", ctypes.c_float),
+    ]
+
+
 STORAGE_SEGMENT_VIEW_AXIAL_TANG = 0
 STORAGE_SEGMENT_AXIAL_VIEW_TANG = 1
 NUMBER_TYPES = {"schar": 0, "uchar": 1, "short": 2, "ushort": 3, "int": 4, "uint": 5, "float": 6, "double": 7}
@@ -239,6 +253,10 @@ EXPORTS = [
     ("b200rt_batch_get_config", _I, [_P, ctypes.POINTER(BatchConfig)]),
     ("b200rt_batch_get_num_cancelled", _I, [_P, _I, ctypes.POINTER(_I64)]),
     ("b200rt_normalisation_dev", _I, [_P, ctypes.POINTER(NormTerm), _I, _I, _P, _P]),
+    ("b200rt_listmode_gradient_dev", _I, [_P, _P, _I64, _P, _I, _I, _I, _P, _I, _P, _P]),
+    ("b200rt_listmode_value_dev", _I, [_P, _P, _I64, _P, _I, _I, _I, ctypes.POINTER(ctypes.c_double), _P]),
+    ("b200rt_listmode_hessian_times_input_dev", _I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _P]),
+    ("b200rt_listmode_num_invalid", _I, [_P, ctypes.POINTER(_I64)]),
     ("b200rt_stream_bytes", _I, [_P, ctypes.POINTER(StreamFormat), ctypes.POINTER(_I64)]),
     ("b200rt_projdata_from_stream_dev", _I, [_P, _P, _I64, ctypes.POINTER(StreamFormat), _P, _P]),
     ("b200rt_projdata_to_stream_dev", _I, [_P, _P, ctypes.POINTER(StreamFormat), _P, _I64, _P]),

@@ -139,6 +139,11 @@ struct b200rt_projector {
   std::map<std::pair<int, int>, ViewGroups> view_groups;
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> copy_events;
+  // list mode: the related lines on the host, (tof, seg, view, tang) -> (basic bin, line, basic view)
+  std::vector<LineDev> h_lines;
+  DevBuf<int4> lm_table;
+  DevBuf<double> lm_partial, lm_sum;
+  DevBuf<unsigned> lm_invalid;
 
   long long bin_key(int view, int seg, int tang, int tof) const {
     const Geometry& g = *geo;
@@ -651,6 +656,7 @@ void setup_projector(b200rt_projector& h) {
   }
   h.bins.upload(h.h_bins, h.stream);
   h.lines.upload(lines, h.stream);
+  h.h_lines = lines;
   std::vector<SegDev> sd(2 * g.S() + 1);
   for (int s = -g.S(); s <= g.S(); ++s) {
     sd[s + g.S()].dev_offset = g.dev_segment_offset(s);
@@ -1029,6 +1035,10 @@ void b200rt_destroy(b200rt_projector* h) {
     h->st_pd_a.release();
     h->st_pd_b.release();
     h->view_groups.clear();
+    h->lm_table.release();
+    h->lm_partial.release();
+    h->lm_sum.release();
+    h->lm_invalid.release();
     if (h->copy_stream) {
       cudaStreamSynchronize(h->copy_stream);
       cudaStreamDestroy(h->copy_stream);
@@ -2310,6 +2320,128 @@ int b200rt_batch_get_num_cancelled(b200rt_batch* b, int frame, int64_t* out) {
     return B200RT_OK;
   } catch (const std::exception& e) {
     return bfail(b, status_of(e), e.what());
+  }
+}
+
+}  // extern "C"
+
+/* ---- list mode ---------------------------------------------------------- */
+namespace {
+
+void ensure_lm_table(b200rt_projector& h) {
+  if (h.lm_table.p) return;
+  const Geometry& g = *h.geo;
+  const int nseg = 2 * g.S() + 1, nv = g.num_views(), nt = g.num_tang(), ntof = g.num_tof();
+  std::vector<int4> table(static_cast<size_t>(ntof) * nseg * nv * nt, make_int4(-1, -1, -1, 0));
+  for (int b = 0; b < static_cast<int>(h.h_bins.size()); ++b) {
+    const ProjBinDev& pb = h.h_bins[b];
+    for (int l = 0; l < pb.num_lines; ++l) {
+      const LineDev& L = h.h_lines[pb.first_line + l];
+      const int tang = L.tang_sign * pb.tang;
+      if (tang < g.min_tang() || tang > g.max_tang()) continue;
+      const size_t k = ((static_cast<size_t>(pb.tof - g.min_tof()) * nseg + (L.seg + g.S())) * nv + L.view) * nt +
+                       (tang - g.min_tang());
+      table[k] = make_int4(b, l, h.h_bin_view[b], 0);
+    }
+  }
+  h.lm_table.upload(table, h.stream);
+  h.lm_invalid.alloc(1);
+  ck(cudaMemsetAsync(h.lm_invalid.p, 0, sizeof(unsigned), h.stream), "memset");
+  ck(cudaStreamSynchronize(h.stream), "list-mode table");
+}
+
+int lm_check(b200rt_projector* h, const b200rt_lm_event* ev, int64_t n, const float* x, int subset, int nsub) {
+  if (!h || (!ev && n > 0) || !x || n < 0) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  return check_subset(h, subset, nsub);
+}
+
+}  // namespace
+
+static_assert(sizeof(b200rt_lm_event) == sizeof(LmEventDev), "list-mode event layouts agree");
+
+extern "C" {
+
+int b200rt_listmode_gradient_dev(b200rt_projector* h, const b200rt_lm_event* events_dev, int64_t num_events,
+                                 const float* image_dev, int subset_num, int num_subsets, int has_add,
+                                 const float* subset_sensitivity_dev, int accumulate, float* gradient_dev,
+                                 void* stream) {
+  if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
+  if (!gradient_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    ensure_lm_table(*h);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t ni = h->geo->image_size();
+    if (!accumulate) ck(cudaMemsetAsync(gradient_dev, 0, sizeof(float) * ni, st), "memset");
+    if (num_events > 0)
+      ck(launch_listmode(h->params, h->lm_table.p, reinterpret_cast<const LmEventDev*>(events_dev), num_events, 0,
+                         image_dev, nullptr, subset_num, num_subsets, has_add, gradient_dev, nullptr, h->lm_invalid.p,
+                         st),
+         "list-mode gradient");
+    if (subset_sensitivity_dev) ck(launch_subtract(gradient_dev, subset_sensitivity_dev, ni, st), "subtract");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_listmode_value_dev(b200rt_projector* h, const b200rt_lm_event* events_dev, int64_t num_events,
+                              const float* image_dev, int subset_num, int num_subsets, int has_add, double* value,
+                              void* stream) {
+  if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
+  if (!value) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    ensure_lm_table(*h);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nb = listmode_num_blocks(num_events);
+    h->lm_partial.alloc(std::max<size_t>(h->lm_partial.n, static_cast<size_t>(nb)));
+    h->lm_sum.alloc(1);
+    ck(launch_listmode(h->params, h->lm_table.p, reinterpret_cast<const LmEventDev*>(events_dev), num_events, 1,
+                       image_dev, nullptr, subset_num, num_subsets, has_add, nullptr, h->lm_partial.p, h->lm_invalid.p,
+                       st),
+       "list-mode value");
+    ck(launch_reduce_sum(h->lm_partial.p, nb, h->lm_sum.p, st), "list-mode value");
+    ck(cudaMemcpyAsync(value, h->lm_sum.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "list-mode value");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_listmode_hessian_times_input_dev(b200rt_projector* h, const b200rt_lm_event* events_dev,
+                                            int64_t num_events, const float* image_dev, const float* rhs_dev,
+                                            int subset_num, int num_subsets, int has_add, float* output_dev,
+                                            void* stream) {
+  if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
+  if (!rhs_dev || !output_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    ensure_lm_table(*h);
+    if (num_events > 0)
+      ck(launch_listmode(h->params, h->lm_table.p, reinterpret_cast<const LmEventDev*>(events_dev), num_events, 2,
+                         image_dev, rhs_dev, subset_num, num_subsets, has_add, output_dev, nullptr, h->lm_invalid.p,
+                         static_cast<cudaStream_t>(stream)),
+         "list-mode Hessian");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_listmode_num_invalid(b200rt_projector* h, int64_t* count) {
+  if (!h || !count) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    ensure_lm_table(*h);
+    unsigned v = 0;
+    ck(cudaMemcpy(&v, h->lm_invalid.p, sizeof(unsigned), cudaMemcpyDeviceToHost), "D2H");
+    ck(cudaMemset(h->lm_invalid.p, 0, sizeof(unsigned)), "memset");
+    *count = v;
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
   }
 }
 

@@ -300,6 +300,19 @@ cudaError_t launch_image_from_dev(const float* dev, float* stir, int nz, int ny,
 // per segment: STIR [ax][view*tang] <-> device [view*tang][ax]
 cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64_t nvt, cudaStream_t st);
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st);
+// List-mode events (listmode.cu), the layout of b200rt_lm_event; table[(tof, seg, view, tang)] = (basic bin, line
+// of the bin, basic view, 0) or x = -1 for a bin no line covers
+struct LmEventDev {
+  int seg, view, axial, tang, tof;
+  float value, corr;
+};
+int listmode_num_blocks(int64_t n);
+cudaError_t launch_subtract(float* out, const float* s, int64_t n, cudaStream_t st);  // out -= s
+// op 0: out += gradient terms, 1: per-block value partials (listmode_num_blocks of them), 2: out += Hessian times rhs
+cudaError_t launch_listmode(const ProjParams& p, const int4* table, const LmEventDev* events, int64_t n, int op,
+                            const float* x, const float* rhs, int subset, int nsub, int has_add, float* out,
+                            double* partial, unsigned* invalid, cudaStream_t st);
+
 // Projection data streams (stream.cu): NumericType codes and storage orders as b200rt_stream_format
 constexpr int kNumSChar = 0, kNumUChar = 1, kNumShort = 2, kNumUShort = 3, kNumInt = 4, kNumUInt = 5, kNumFloat = 6,
               kNumDouble = 7;

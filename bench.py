@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched dynamic OSEM measurement")
     ap.add_argument("--batch-iterations", type=int, default=2, help="full OSEM iterations per dynamic frame")
+    ap.add_argument("--no-extras", action="store_true", help="skip the list-mode and Gibbs penalty measurements")
     return ap.parse_args()
 
 
@@ -140,6 +141,98 @@ class CpuBaseline:
                 "sample": f"forward+back of subset {self.sub} of {self.nsub} ({self.nbins} LORs) of the clinical "
                           f"workload with a warm row cache (cache fill {self.cache_fill_s:.2f} s), {self.nthreads} "
                           "OpenMP threads; restated CPU path, not the STIR binary"}
+
+
+LM_EVENTS = 10_000_000
+
+
+def random_lm_bins(pdi, n, rng, views=None):
+    """n events on uniformly drawn bins (segment, view, axial, tangential, timing 0) of the geometry, optionally
+    restricted to `views`."""
+    S = pdi.max_segment_num
+    seg = rng.integers(-S, S + 1, n)
+    nax = np.array([pdi.get_num_axial_poss(int(s)) for s in range(-S, S + 1)])
+    ax = (rng.random(n) * nax[seg + S]).astype(np.int64)
+    view = rng.integers(0, pdi.num_views, n) if views is None else np.asarray(views)[rng.integers(0, len(views), n)]
+    tang = rng.integers(pdi.min_tangential_pos_num, pdi.min_tangential_pos_num + pdi.num_tangential_poss, n)
+    return np.stack([seg, view, ax, tang, np.zeros(n, np.int64)], 1).astype(np.int32)
+
+
+def time_dev(fn, warm=3, reps=5):
+    """mean device time of fn() in ms over reps calls (CUDA events on the current stream, after warm calls)"""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def listmode_and_priors(proj, pdi, img, xd, cpu_ref):
+    """The list-mode sub-gradient (events/s) and the Gibbs Relative Difference penalty gradient (voxels/s) on the
+    clinical geometry, with single-thread oracle baselines on bounded samples (cpu_ref: the CpuBaseline whose row
+    cache already holds subset 0 of 42, or None)."""
+    import torch
+    from stir_b200 import _abi, gibbs
+    from stir_b200.listmode import PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByBin as LM
+    from stir_b200.listmode import pack_events
+    out = {}
+    rng = np.random.default_rng(5)
+    bins = random_lm_bins(pdi, LM_EVENTS, rng)
+    obj = LM(proj, pack_events(bins, None, np.full(LM_EVENTS, 0.1, np.float32), proj.device), has_add=True)
+    g = proj.empty_image(zero=False)
+    ms = time_dev(lambda: obj.compute_sub_gradient_without_penalty(xd, 0, out=g))
+    lm = {"metric": "list-mode sub-gradient events/s", "value": LM_EVENTS / (ms / 1e3), "unit": "events/s",
+          "events": LM_EVENTS, "ms": ms, "gpu_launches": 2,
+          "workload": "10M events on uniformly drawn bins of the clinical geometry (seed 5), value 1, additive 0.1, "
+                      "one subset; one warp per event: forward, ratio, back projection"}
+    if cpu_ref is not None:
+        from stir_b200.subsets import views_in_subset
+        views = views_in_subset(cpu_ref.geo, cpu_ref.sub, cpu_ref.nsub, cpu_ref.orc.symmetries_used)
+        sample = random_lm_bins(pdi, 40000, np.random.default_rng(6), views)
+        x_host = cpu_ref.x
+        t0 = time.perf_counter()
+        cpu_ref.orc.listmode("gradient", sample, np.ones(len(sample), np.float32), x_host,
+                             corr=np.full(len(sample), 0.1, np.float32), has_add=True)
+        dt = time.perf_counter() - t0
+        lm["cpu_baseline"] = {"value": len(sample) / dt, "unit": "events/s", "cores": 1, "kind": "port",
+                              "sample": f"{len(sample)} events on the bins of subset 0 of 42 (warm row cache), the "
+                                        "oracle's sequential LM_gradient_and_value loop"}
+    out["listmode"] = lm
+    del obj
+    # Gibbs Relative Difference penalty gradient on the image
+    shape = (img.nz, img.ny, img.nx)
+    vox = img.voxel_size
+    p = gibbs.GibbsRelativeDifferencePenalty(penalisation_factor=0.1, gamma=2.0, epsilon=1e-7, device=proj.device)
+    p.set_up(shape, vox, _abi.LAYOUT_DEVICE)
+    gg = proj.empty_image(zero=False)
+    ms = time_dev(lambda: p.compute_gradient(xd, gg))
+    nvox = int(np.prod(shape))
+    hbm, peak_kind = peaks()
+    pr = {"metric": "Gibbs RDP gradient voxels/s", "value": nvox / (ms / 1e3), "unit": "voxels/s", "ms": ms,
+          "workload": "GibbsRelativeDifferencePenalty (gamma 2, epsilon 1e-7) gradient, 3x3x3 default weights, "
+                      "344x344x127 image in the device layout",
+          "roofline": {"bound": "issue", "hbm_bytes": 8 * nvox, "achieved_GBs": 8 * nvox / (ms / 1e3) / 1e9,
+                       "peak": hbm, "frac_hbm": 8 * nvox / (ms / 1e3) / 1e9 / hbm, "peak_kind": peak_kind}}
+    if cpu_ref is not None:
+        from oracle import oracle as O
+        slab = np.ascontiguousarray(cpu_ref.x[:16])
+        w = O.gibbs_default_weights(vox)
+        t0 = time.perf_counter()
+        O.gibbs("gradient", 2, 0.1, w, slab, gamma=2.0, epsilon=1e-7)
+        dt = time.perf_counter() - t0
+        pr["cpu_baseline"] = {"value": slab.size / dt, "unit": "voxels/s", "cores": 1, "kind": "port",
+                              "sample": "16 planes of the image, the oracle's GibbsPenalty::compute_gradient loop"}
+    out["gibbs_rdp_gradient"] = pr
+    del p
+    torch.cuda.empty_cache()
+    return out
 
 
 def dist_setup():
@@ -408,11 +501,13 @@ def b200_main(args):
             "frac_forward": fwd_bytes / (fwd_ms / 1e3) / 1e9 / hbm, "frac_back": back_bytes / (back_ms / 1e3) / 1e9 / hbm}
 
     cpu = None
+    cb = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             cb = CpuBaseline()
             cpu = cb.describe(cb.step())
         except Exception as e:  # the baseline is reported, never the measured product
+            cb = None
             cpu = {"value": None, "unit": "LORs/s", "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
     line = {"metric": METRIC, "value": value, "unit": "LORs/s", "n_gpus": ws, "steps": K, "warmup": max(args.warmup, 3),
@@ -428,6 +523,11 @@ def b200_main(args):
                     "d2h_bytes_per_step": pd_bytes + img_bytes},
             "clocks": clocks.summary(),
             "gpu_launches": 2 * K}
+    if not args.no_extras:
+        try:
+            line.update(listmode_and_priors(proj, pdi, img, xd, cb))
+        except Exception as e:  # reported, never hides the headline line
+            line["listmode"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_batch:
         proj.close()
         del pd, bk, flush, y, xd

@@ -61,6 +61,7 @@ def _load():
         "or_ray_trace": (_I64, [_P, _P, _P, _F, _P, _P, _I64]),
         "or_ossps_denominator_f32": (_I, [_P, _P, _P, _I, _P]),
         "or_prior_hessian_times_input_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+        "or_listmode_f32": (_D, [_P, _I, _P, _P, _P, _I64, _P, _P, _I, _I, _I, _P, ctypes.POINTER(_I64)]),
         "or_gibbs_f32": (_D, [_I, _I, _F, _F, _F, _P, _I, _I, _I, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
         "or_gibbs_default_weights": (_I, [_F, _F, _F, _I, _P]),
         "or_prior_curvature_f32": (_I, [ctypes.POINTER(_abi.Prior), _P, _I, _I, _I, _F, _F, _F, _P]),
@@ -245,6 +246,21 @@ class Oracle:
                                         int(zero_seg0_end_planes), nthreads or default_threads(), _ptr(g)) != 0:
             raise RuntimeError("oracle gradient failed")
         return g
+
+    def listmode(self, op, bins, values, image, corr=None, rhs=None, subset=0, nsub=1, has_add=False, out=None):
+        """List-mode objective over events: bins (n, 5) ints (segment, view, axial, tangential, timing), values (n,),
+        corr (n,) additive terms.  op "gradient" / "hessian" return out + the sum; "value" returns (value, invalid)."""
+        bins = np.ascontiguousarray(bins, np.int32).reshape(-1, 5)
+        values = np.ascontiguousarray(values, np.float32)
+        c = None if corr is None else np.ascontiguousarray(corr, np.float32)
+        img = np.ascontiguousarray(image, np.float32)
+        r = None if rhs is None else np.ascontiguousarray(rhs, np.float32)
+        o = np.zeros(img.shape, np.float32) if out is None else np.ascontiguousarray(out, np.float32).copy()
+        bad = ctypes.c_int64()
+        code = {"gradient": 0, "value": 1, "hessian": 2}[op]
+        v = lib().or_listmode_f32(self.h, code, _ptr(bins), _ptr(values), _ptr(c), bins.shape[0], _ptr(img), _ptr(r),
+                                  subset, nsub, int(bool(has_add)), _ptr(o), ctypes.byref(bad))
+        return (v, bad.value) if code == 1 else o
 
     def log_likelihood(self, image, y, additive=None, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False,
                        nthreads=None):

@@ -1674,6 +1674,54 @@ double or_prior_value_f32(const b200rt_prior* p, const float* img, const float* 
   return prior_value(*p, img, kappa, nz, ny, nx, vz, vy, vx);
 }
 
+/* ---- list mode: LM_gradient_and_value / LM_Hessian
+   (PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByBin.cxx:750-820) over the events in order,
+   with the subset rule of LM_distributable_computation (distributable.txx:36-140): the basic bin's view mod
+   num_subsets.  events: n x 5 ints (segment, view, axial, tangential, timing) with values and additive terms.
+   op 0: out += gradient terms; 1: returns the value; 2: out += Hessian times rhs.  Returns the value (op 1), else 0;
+   *invalid counts events outside the projection data. */
+double or_listmode_f32(or_handle* h, int op, const int32_t* bins, const float* values, const float* corr, int64_t n,
+                       const float* x, const float* rhs, int subset, int nsub, int has_add, float* out,
+                       int64_t* invalid) {
+  Handle<float>& H = *h->f;
+  const auto& g = H.g;
+  const float max_quotient = 10000.F;
+  double value = 0.0;
+  int64_t bad = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const float y = values[i];
+    if (y == 0.0f) continue;
+    Bin<float> b{bins[5 * i], bins[5 * i + 1], bins[5 * i + 2], bins[5 * i + 3], bins[5 * i + 4]};
+    if (b.seg < -g.S || b.seg > g.S || b.view < 0 || b.view >= g.num_views || b.tang < g.min_tang ||
+        b.tang > g.max_tang || b.tof < g.min_tof || b.tof > g.max_tof || b.ax < 0 || b.ax >= g.nax(b.seg)) {
+      ++bad;
+      continue;
+    }
+    if (nsub > 1) {
+      Bin<float> basic = b;
+      find_op_and_basic(g, basic);
+      if (subset != basic.view % nsub) continue;
+    }
+    const float fwd = H.fwd_bin(b, x) + (has_add ? corr[i] : 0.F);
+    const bool cancel = y > max_quotient * fwd;
+    if (op == 1) {
+      value -= cancel ? y * std::log(static_cast<double>(y / max_quotient)) : y * std::log(static_cast<double>(fwd));
+      continue;
+    }
+    if (op == 0) {
+      H.back_bin(b, y / fwd, out);
+      continue;
+    }
+    if (cancel) continue;
+    const float c = -y / (fwd * fwd);
+    const float r = H.fwd_bin(b, rhs);
+    if (r == 0) continue;
+    H.back_bin(b, c * r, out);
+  }
+  if (invalid) *invalid = bad;
+  return value;
+}
+
 /* ---- Gibbs penalties: GibbsPenalty<float, Potential> (GibbsPenalty.inl) ---------------------------------------
    Potentials as in QuadraticPotential (GibbsQuadraticPenalty.h:50-80) and RelativeDifferencePotential
    (GibbsRelativeDifferencePenalty.h:60-120): each expression is evaluated in the types the reference gives it

@@ -102,6 +102,13 @@ int or_prior_gradient_f32(const b200rt_prior* prior, const float* image, const f
 double or_prior_value_f32(const b200rt_prior* prior, const float* image, const float* kappa, int nz, int ny, int nx,
                           float vz, float vy, float vx);
 
+/* list-mode objective over events (n x 5 ints: segment, view, axial, tangential, timing; values; additive terms or
+   NULL): op 0 out += gradient terms, 1 returns the value, 2 out += Hessian times rhs; *invalid (may be NULL) gets
+   the number of events outside the projection data */
+double or_listmode_f32(or_handle* h, int op, const int32_t* bins, const float* values, const float* corr, int64_t n,
+                       const float* x, const float* rhs, int subset, int nsub, int has_add, float* out,
+                       int64_t* invalid);
+
 /* GibbsPenalty<float, potential> (GibbsPenalty.inl): potential 1 Quadratic, 2 Relative Difference;
    op 0 value, 1 gradient, 2 gradient times input, 3 Hessian diagonal, 4 accumulate Hessian times input (out +=),
    5 Hessian of voxel (vz, vy, vx) into out.  Images [z][y][x]; weights [wz][wy][wx]; kappa may be NULL.

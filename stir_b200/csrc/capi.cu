@@ -2677,6 +2677,7 @@ int b200rt_gibbs_create(const b200rt_gibbs_params* p, int device, b200rt_gibbs**
         }
   }
   std::copy(g->host_w.begin(), g->host_w.end(), d.w);
+  for (size_t i = 0; i < 27 && i < g->host_w.size(); ++i) d.wd[i] = static_cast<double>(g->host_w[i]);
   *out = g.release();
   return B200RT_OK;
 }

@@ -110,8 +110,8 @@ __device__ __forceinline__ double block_sum(double v) {
 
 // one neighbour's term of the per-voxel sums, in the reference's types
 template <typename Pot, int OP>
-__device__ __forceinline__ void gibbs_term(const Pot& pot, float w, float c, float nk, float kk, float inj, float ink,
-                                           bool centre, const float* kappa, double& sum, float& result) {
+__device__ __forceinline__ void gibbs_term(const Pot& pot, float w, double wd, float c, float nk, float kk, float inj,
+                                           float ink, bool centre, const float* kappa, double& sum, float& result) {
   if (OP == 4) {
     float current = w;
     if (centre)
@@ -123,7 +123,7 @@ __device__ __forceinline__ void gibbs_term(const Pot& pot, float w, float c, flo
   } else {
     if (centre) return;
     const double f = OP == 0 ? pot.value(c, nk) : (OP == 3 ? pot.d20(c, nk) : pot.d10(c, nk));
-    double current = w * f;
+    double current = wd * f;  // wd = (double)w: the product is the reference's w * f
     if (kappa) current *= kk;
     sum += current;
   }
@@ -156,8 +156,8 @@ __global__ void __launch_bounds__(kGibbsThreads) gibbs_kernel(const GibbsDev g, 
         const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
         const int k = j + dz * sz + dy * sy + dx * sx;
         const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
-        gibbs_term<Pot, OP>(pot, g.w[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 13, g.kappa,
-                            sum, result);
+        gibbs_term<Pot, OP>(pot, g.w[t], g.wd[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 13,
+                            g.kappa, sum, result);
       }
     } else if (g.wy == 3 && g.wx == 3 && g.wz == 1 && in3) {
 #pragma unroll
@@ -165,8 +165,8 @@ __global__ void __launch_bounds__(kGibbsThreads) gibbs_kernel(const GibbsDev g, 
         const int dy = t / 3 - 1, dx = t % 3 - 1;
         const int k = j + dy * sy + dx * sx;
         const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
-        gibbs_term<Pot, OP>(pot, g.w[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 4, g.kappa,
-                            sum, result);
+        gibbs_term<Pot, OP>(pot, g.w[t], g.wd[t], c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f, t == 4,
+                            g.kappa, sum, result);
       }
     } else {
       const Range r = gibbs_range(g, z, y, xx);
@@ -175,8 +175,9 @@ __global__ void __launch_bounds__(kGibbsThreads) gibbs_kernel(const GibbsDev g, 
           for (int dx = r.x0; dx <= r.x1; ++dx) {
             const int k = j + dz * sz + dy * sy + dx * sx;
             const float kk = g.kappa ? kj * __ldg(g.kappa + k) : 1.f;
-            gibbs_term<Pot, OP>(pot, gibbs_w(g, dz, dy, dx), c, __ldg(x + k), kk, inj, OP == 4 ? __ldg(in + k) : 0.f,
-                                dz == 0 && dy == 0 && dx == 0, g.kappa, sum, result);
+            const float w = gibbs_w(g, dz, dy, dx);
+            gibbs_term<Pot, OP>(pot, w, static_cast<double>(w), c, __ldg(x + k), kk, inj,
+                                OP == 4 ? __ldg(in + k) : 0.f, dz == 0 && dy == 0 && dx == 0, g.kappa, sum, result);
           }
     }
     if (OP == 4)

@@ -338,6 +338,7 @@ struct GibbsDev {
   int wz, wy, wx;
   const float* kappa;
   float w[kGibbsMaxWeights];
+  double wd[27];  // the first 27 weights as double (the unrolled 3x3x3 / 1x3x3 paths)
 };
 // op: 0 value (-> *result, device), 1 gradient, 2 gradient times input (-> *result), 3 Hessian diagonal,
 // 4 out += Hessian times input; partial holds gibbs_num_partials() doubles

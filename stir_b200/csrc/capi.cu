@@ -686,6 +686,8 @@ void setup_projector(b200rt_projector& h) {
   p.min_x = g.desc().min_x;
   p.max_row_len = max_len;
   p.uniform_npa = g.npa(0);
+  p.max_nax = 0;
+  for (int s = -g.S(); s <= g.S(); ++s) p.max_nax = std::max(p.max_nax, g.nax(s));
   for (int s = -g.S(); s <= g.S(); ++s)
     if (g.npa(s) != p.uniform_npa) p.uniform_npa = 0;
   if (static_cast<int64_t>(p.nz) * p.ny * p.nx >= (int64_t(1) << 31)) throw std::runtime_error("image too large");

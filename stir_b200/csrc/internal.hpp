@@ -80,7 +80,11 @@ struct ProjParams {
   int min_z, min_y, min_x;
   int max_row_len;
   int uniform_npa;  // planes per axial position if equal for all segments, else 0
+  int max_nax;      // most axial positions of any segment
 };
+// with at most this many axial positions per line the per-basic-bin kernels pack (line, axial position) pairs
+// into the lanes of a warp (project.cu)
+constexpr int kPackedMaxNax = 16;
 
 // What the forward projector does with each projected bin A x:
 //   kEpiNone:   store it;

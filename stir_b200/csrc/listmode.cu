@@ -36,6 +36,53 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+// sum over the row of img[voxel] * weight, each lane over elements lane, lane + 32, ... in order, four elements'
+// loads in flight at a time
+__device__ __forceinline__ float lm_forward(const ProjParams& p, const RowElem* __restrict__ row, int len,
+                                            const LineDev& L, int zadd, const float* __restrict__ img, int lane) {
+  float f = 0.f;
+  int k = lane;
+  for (; k + 96 < len; k += 128) {
+    const RowElem e0 = row[k], e1 = row[k + 32], e2 = row[k + 64], e3 = row[k + 96];
+    const int v0 = lm_voxel(p, e0, L, zadd), v1 = lm_voxel(p, e1, L, zadd), v2 = lm_voxel(p, e2, L, zadd),
+              v3 = lm_voxel(p, e3, L, zadd);
+    const float x0 = v0 >= 0 ? __ldg(img + v0) : 0.f, x1 = v1 >= 0 ? __ldg(img + v1) : 0.f;
+    const float x2 = v2 >= 0 ? __ldg(img + v2) : 0.f, x3 = v3 >= 0 ? __ldg(img + v3) : 0.f;
+    if (v0 >= 0) f += x0 * e0.v;
+    if (v1 >= 0) f += x1 * e1.v;
+    if (v2 >= 0) f += x2 * e2.v;
+    if (v3 >= 0) f += x3 * e3.v;
+  }
+  for (; k < len; k += 32) {
+    const RowElem e = row[k];
+    const int v = lm_voxel(p, e, L, zadd);
+    if (v >= 0) f += __ldg(img + v) * e.v;
+  }
+  return warp_sum(f);
+}
+
+__device__ __forceinline__ void lm_back(const ProjParams& p, const RowElem* __restrict__ row, int len, const LineDev& L,
+                                        int zadd, float data, float* __restrict__ out, int lane) {
+  int k = lane;
+  for (; k + 96 < len; k += 128) {
+    const RowElem e0 = row[k], e1 = row[k + 32], e2 = row[k + 64], e3 = row[k + 96];
+    const int v0 = lm_voxel(p, e0, L, zadd), v1 = lm_voxel(p, e1, L, zadd), v2 = lm_voxel(p, e2, L, zadd),
+              v3 = lm_voxel(p, e3, L, zadd);
+    if (v0 >= 0) atomicAdd(out + v0, e0.v * data);
+    if (v1 >= 0) atomicAdd(out + v1, e1.v * data);
+    if (v2 >= 0) atomicAdd(out + v2, e2.v * data);
+    if (v3 >= 0) atomicAdd(out + v3, e3.v * data);
+  }
+  for (; k < len; k += 32) {
+    const RowElem e = row[k];
+    const int v = lm_voxel(p, e, L, zadd);
+    if (v >= 0) atomicAdd(out + v, e.v * data);
+  }
+}
+
+// A warp takes 32 consecutive events at a time: each lane resolves one event (bin lookup, basic bin, line) so the
+// dependent loads of 32 events overlap, then the warp projects the events one after the other with the lane's
+// results broadcast by shuffles.
 template <int OP>  // 0 gradient, 1 value, 2 Hessian times rhs
 __global__ void __launch_bounds__(kLmThreads) listmode_kernel(const ProjParams p, const int4* __restrict__ table,
                                                              const LmEventDev* __restrict__ ev, int64_t n,
@@ -45,60 +92,67 @@ __global__ void __launch_bounds__(kLmThreads) listmode_kernel(const ProjParams p
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kLmWarps;
   double val = 0.0;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * kLmWarps + warp; i < n; i += nwarps) {
-    const LmEventDev e = ev[i];
-    if (e.value == 0.0f) continue;
-    const int s = e.seg + p.S, tofi = e.tof - p.min_tof, ti = e.tang - p.min_tang;
-    if (s < 0 || s > 2 * p.S || tofi < 0 || tofi >= p.num_tof || e.view < 0 || e.view >= p.num_views || ti < 0 ||
-        ti >= p.num_tang) {
-      if (lane == 0) atomicAdd(invalid, 1u);
-      continue;
-    }
-    const int4 t = table[((static_cast<int64_t>(tofi) * (2 * p.S + 1) + s) * p.num_views + e.view) * p.num_tang + ti];
-    const SegDev sd = p.segs[s];
-    if (t.x < 0 || e.axial < 0 || e.axial >= sd.nax) {
-      if (lane == 0) atomicAdd(invalid, 1u);
-      continue;
-    }
-    if (nsub > 1 && t.z % nsub != subset) continue;
-    const ProjBinDev pb = p.bins[t.x];
-    const LineDev L = p.lines[pb.first_line + t.y];
-    const int zadd = e.axial * sd.npa - p.min_z;
-    const RowElem* row = p.rows + pb.row_offset;
-    float f = 0.f;
-    for (int k = lane; k < pb.row_len; k += 32) {
-      const RowElem el = row[k];
-      const int v = lm_voxel(p, el, L, zadd);
-      if (v >= 0) f += __ldg(x + v) * el.v;
-    }
-    const float fwd = warp_sum(f) + (has_add ? e.corr : 0.f);
-    const float y = e.value;
-    const bool cancel = y > kMaxQuotient * fwd;
-    if (OP == 1) {
-      if (lane == 0) val -= cancel ? y * log(static_cast<double>(y / kMaxQuotient)) : y * log(static_cast<double>(fwd));
-      continue;
-    }
-    if (OP == 2 && cancel) continue;
-    float data;
-    if (OP == 0) {
-      data = y / fwd;
-    } else {
-      const float c = -y / (fwd * fwd);
-      float r = 0.f;
-      for (int k = lane; k < pb.row_len; k += 32) {
-        const RowElem el = row[k];
-        const int v = lm_voxel(p, el, L, zadd);
-        if (v >= 0) r += __ldg(rhs + v) * el.v;
+  for (int64_t base = (static_cast<int64_t>(blockIdx.x) * kLmWarps + warp) * 32; base < n; base += nwarps * 32) {
+    // this lane's event: 0 = skip, 1 = project (row, line, z offset), invalid ones counted
+    int state = 0, row_len = 0, line_bits = 0, zadd = 0;
+    int64_t row_off = 0;
+    float y = 0.f, corr = 0.f;
+    if (base + lane < n) {
+      const LmEventDev e = ev[base + lane];
+      if (e.value != 0.0f) {
+        const int s = e.seg + p.S, tofi = e.tof - p.min_tof, ti = e.tang - p.min_tang;
+        bool ok = s >= 0 && s <= 2 * p.S && tofi >= 0 && tofi < p.num_tof && e.view >= 0 && e.view < p.num_views &&
+                  ti >= 0 && ti < p.num_tang;
+        int4 t = make_int4(-1, 0, 0, 0);
+        if (ok) t = table[((static_cast<int64_t>(tofi) * (2 * p.S + 1) + s) * p.num_views + e.view) * p.num_tang + ti];
+        SegDev sd{};
+        if (ok) sd = p.segs[s];
+        ok = ok && t.x >= 0 && e.axial >= 0 && e.axial < sd.nax;
+        if (!ok) {
+          atomicAdd(invalid, 1u);
+        } else if (nsub <= 1 || t.z % nsub == subset) {
+          const ProjBinDev pb = p.bins[t.x];
+          const LineDev L = p.lines[pb.first_line + t.y];
+          state = 1;
+          row_off = pb.row_offset;
+          row_len = pb.row_len;
+          line_bits = (static_cast<int>(static_cast<uint8_t>(L.flags)) << 16) | static_cast<uint16_t>(L.q);
+          zadd = e.axial * sd.npa - p.min_z;
+          y = e.value;
+          corr = has_add ? e.corr : 0.f;
+        }
       }
-      r = warp_sum(r);
-      if (r == 0.f) continue;
-      data = c * r;
     }
-    if (data == 0.f) continue;
-    for (int k = lane; k < pb.row_len; k += 32) {
-      const RowElem el = row[k];
-      const int v = lm_voxel(p, el, L, zadd);
-      if (v >= 0) atomicAdd(out + v, el.v * data);
+    for (int j = 0; j < 32; ++j) {
+      if (!__shfl_sync(0xffffffffu, state, j)) continue;
+      const int64_t off = __shfl_sync(0xffffffffu, row_off, j);
+      const int len = __shfl_sync(0xffffffffu, row_len, j);
+      const int lb = __shfl_sync(0xffffffffu, line_bits, j);
+      const int za = __shfl_sync(0xffffffffu, zadd, j);
+      const float yj = __shfl_sync(0xffffffffu, y, j);
+      const float cj = __shfl_sync(0xffffffffu, corr, j);
+      LineDev L;
+      L.flags = static_cast<int8_t>(lb >> 16);
+      L.q = static_cast<int16_t>(lb & 0xffff);
+      const RowElem* row = p.rows + off;
+      const float fwd = lm_forward(p, row, len, L, za, x, lane) + cj;
+      const bool cancel = yj > kMaxQuotient * fwd;
+      if (OP == 1) {
+        if (lane == 0)
+          val -= cancel ? yj * log(static_cast<double>(yj / kMaxQuotient)) : yj * log(static_cast<double>(fwd));
+        continue;
+      }
+      if (OP == 2 && cancel) continue;
+      float data;
+      if (OP == 0) {
+        data = yj / fwd;
+      } else {
+        const float r = lm_forward(p, row, len, L, za, rhs, lane);
+        if (r == 0.f) continue;
+        data = (-yj / (fwd * fwd)) * r;
+      }
+      if (data == 0.f) continue;
+      lm_back(p, row, len, L, za, data, out, lane);
     }
   }
   if (OP == 1) {
@@ -130,7 +184,7 @@ cudaError_t launch_subtract(float* out, const float* s, int64_t n, cudaStream_t 
 }
 
 int listmode_num_blocks(int64_t n) {
-  const int64_t want = (n + kLmWarps - 1) / kLmWarps;
+  const int64_t want = (n + 32 * kLmWarps - 1) / (32 * kLmWarps);
   return static_cast<int>(want < 1 ? 1 : (want > 148 * 16 ? 148 * 16 : want));
 }
 

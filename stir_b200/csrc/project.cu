@@ -286,6 +286,148 @@ __global__ void __launch_bounds__(kThreads, kMinCtasBack) back_atomic_kernel(Pro
   back_bin<NPA, Acc>(p, pb, smem, pd, img, zero_ends);
 }
 
+// ---- packed kernels: few axial positions per line ----------------------------
+// With at most 16 axial positions per line (small scanners, and TOF data, where every timing bin of a basic bin
+// has its own row) the kernels above leave most lanes idle.  Here a warp takes a whole basic bin and its lanes
+// are (related line, axial position) pairs, 32 / nax lines at a time; the warp reads the row 32 elements at a
+// time (coalesced) and shuffles each element to every lane, which applies its own line's symmetry operation.
+// Each lane sums its bin's elements in row order, as the kernels above do, so the sums are the same.
+constexpr int kPackedWarps = 8;
+
+struct PackedLane {
+  bool act;
+  int swap, sx, sy, zq, q, zoff;  // zoff = npa * a - min_z
+  int a;
+  LineSetup s;
+  LineDev L;
+};
+
+__device__ __forceinline__ PackedLane packed_lane(const ProjParams& p, const ProjBinDev& pb, int l0, int G, int nax,
+                                                  int lane) {
+  PackedLane t{};
+  const int gi = lane / nax;
+  const int l = l0 + gi;
+  t.a = lane - gi * nax;
+  t.act = gi < G && l < pb.num_lines;
+  if (t.act) {
+    t.L = p.lines[pb.first_line + l];
+    t.act = setup_line(p, pb, t.L, t.s);
+  }
+  if (t.act) {
+    t.swap = t.L.flags & 1;
+    t.sx = (t.L.flags & 2) ? -1 : 1;
+    t.sy = (t.L.flags & 4) ? -1 : 1;
+    t.zq = (t.L.flags & 8) ? 1 : 0;
+    t.q = t.L.q;
+    t.zoff = t.a * t.s.npa - p.min_z;
+  }
+  return t;
+}
+
+// the image index of element (zyx) for this lane's line and axial position, or -1 outside [0, nz)
+__device__ __forceinline__ int packed_voxel(const ProjParams& p, const PackedLane& t, uint32_t zyx) {
+  int z, y, x;
+  unpack_zyx(zyx, z, y, x);
+  const int xt = (t.swap ? y : x) * t.sx;
+  const int yt = (t.swap ? x : y) * t.sy;
+  const int zz = (t.zq ? t.q - z : z) + t.zoff;
+  if (zz < 0 || zz >= p.nz) return -1;
+  return ((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz + zz;
+}
+
+// nax of the basic bin's lines (a basic bin's related lines all have segments +-s)
+__device__ __forceinline__ int packed_nax(const ProjParams& p, const ProjBinDev& pb) {
+  return p.segs[p.lines[pb.first_line].seg + p.S].nax;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                                          int nbins, const float* __restrict__ img,
+                                                                          float* __restrict__ out, FwdEpilogue ep) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kPackedWarps + warp;
+  if (bi >= nbins) return;  // whole warps only: no block-wide synchronisation below
+  const ProjBinDev pb = p.bins[bin_list[bi]];
+  const RowElem* row = p.rows + pb.row_offset;
+  const int nax = packed_nax(p, pb);
+  const int G = 32 / nax;
+  double ll = 0.0;
+  unsigned ncancel = 0;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
+    const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    float acc = 0.f;
+    for (int k0 = 0; k0 < pb.row_len; k0 += 32) {
+      RowElem mine{0u, 0.f};
+      if (k0 + lane < pb.row_len) mine = row[k0 + lane];
+      const int cnt = min(32, pb.row_len - k0);
+      int k = 0;
+      for (; k + 4 <= cnt; k += 4) {
+        uint32_t zyx[4];
+        float w[4], xv[4];
+        int v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          zyx[u] = __shfl_sync(0xffffffffu, mine.zyx, k + u);
+          w[u] = __shfl_sync(0xffffffffu, mine.v, k + u);
+          v[u] = t.act ? packed_voxel(p, t, zyx[u]) : -1;
+          xv[u] = v[u] >= 0 ? __ldg(img + v[u]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (v[u] >= 0) acc += xv[u] * w[u];
+      }
+      for (; k < cnt; ++k) {
+        const uint32_t zyx = __shfl_sync(0xffffffffu, mine.zyx, k);
+        const float w = __shfl_sync(0xffffffffu, mine.v, k);
+        const int v = t.act ? packed_voxel(p, t, zyx) : -1;
+        if (v >= 0) acc += __ldg(img + v) * w;
+      }
+    }
+    if (t.act) forward_store<EPI>(p, t.L.seg, t.L.view, t.s.tofi, t.s.nax, t.s.out_base + t.a, t.a, acc, out, ep, ll, ncancel);
+  }
+  if (EPI == kEpiRatio || EPI == kEpiGradient) {
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
+  }
+  if (EPI == kEpiLoglik) {
+    // one partial per basic bin (as the one-CTA-per-bin kernel), reduced in a fixed order by the caller
+    for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
+    if (lane == 0) ep.partials[bi] = ll;
+  }
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kPackedWarps * 32) back_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                                       int nbins, const float* __restrict__ pd, Acc img,
+                                                                       int zero_ends) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kPackedWarps + warp;
+  if (bi >= nbins) return;
+  const ProjBinDev pb = p.bins[bin_list[bi]];
+  const RowElem* row = p.rows + pb.row_offset;
+  const int nax = packed_nax(p, pb);
+  const int G = 32 / nax;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
+    PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    float d = 0.f;
+    if (t.act && !(zero_ends && t.L.seg == 0 && (t.a == 0 || t.a == t.s.nax - 1)))
+      d = pd ? __ldg(pd + t.s.out_base + t.a) : 1.f;  // pd == nullptr back-projects ones
+    t.act = t.act && d != 0.f;  // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
+    if (!__any_sync(0xffffffffu, t.act)) continue;
+    for (int k0 = 0; k0 < pb.row_len; k0 += 32) {
+      RowElem mine{0u, 0.f};
+      if (k0 + lane < pb.row_len) mine = row[k0 + lane];
+      const int cnt = min(32, pb.row_len - k0);
+      for (int k = 0; k < cnt; ++k) {
+        const uint32_t zyx = __shfl_sync(0xffffffffu, mine.zyx, k);
+        const float w = __shfl_sync(0xffffffffu, mine.v, k);
+        const int v = t.act ? packed_voxel(p, t, zyx) : -1;
+        if (v >= 0) img.add(v, w * d);
+      }
+    }
+  }
+}
+
 // ---- batched (several reconstructions in one launch) ------------------------
 // A persistent grid takes work items (frame, basic bin) from a queue in list order: the list is
 // frame-major, so at any time the CTAs work on one or two frames and their images stay in L2.
@@ -404,6 +546,11 @@ static cudaError_t launch_proj(K kernel, const ProjParams& p, int nbins, cudaStr
 template <int EPI>
 static cudaError_t launch_forward_epi(const ProjParams& p, const int* list, int nbins, const float* image, float* out,
                                       const FwdEpilogue& ep, cudaStream_t st) {
+  if (p.max_nax <= kPackedMaxNax) {
+    forward_packed_kernel<EPI><<<(nbins + kPackedWarps - 1) / kPackedWarps, kPackedWarps * 32, 0, st>>>(
+        p, list, nbins, image, out, ep);
+    return cudaGetLastError();
+  }
   switch (p.uniform_npa) {
     case 1: return launch_proj(forward_kernel<1, EPI>, p, nbins, st, list, image, out, ep);
     case 2: return launch_proj(forward_kernel<2, EPI>, p, nbins, st, list, image, out, ep);
@@ -425,6 +572,11 @@ template <typename Acc>
 static cudaError_t launch_back_acc(const ProjParams& p, const int* bin_list, int nbins, const float* projdata, Acc acc,
                                    cudaStream_t st, int zero_ends) {
   if (nbins <= 0) return cudaSuccess;
+  if (p.max_nax <= kPackedMaxNax) {
+    back_packed_kernel<Acc><<<(nbins + kPackedWarps - 1) / kPackedWarps, kPackedWarps * 32, 0, st>>>(
+        p, bin_list, nbins, projdata, acc, zero_ends);
+    return cudaGetLastError();
+  }
   switch (p.uniform_npa) {
     case 1: return launch_proj(back_atomic_kernel<1, Acc>, p, nbins, st, bin_list, projdata, acc, zero_ends);
     case 2: return launch_proj(back_atomic_kernel<2, Acc>, p, nbins, st, bin_list, projdata, acc, zero_ends);

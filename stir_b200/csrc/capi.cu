@@ -924,7 +924,7 @@ cudaError_t copy_views(const Geometry& g, float* dst, const float* src, int v0, 
                            sizeof(float) * nt * (v1 - v0), rows, kind, st);
 }
 
-constexpr int kHostViewGroups = 8;
+constexpr int kHostViewGroups = 16;
 
 // the subset's path items ordered by the group of views they write (kHostViewGroups equal view ranges)
 const b200rt_projector::ViewGroups& view_groups(b200rt_projector& h, int subset, int nsub) {

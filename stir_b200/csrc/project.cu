@@ -340,47 +340,75 @@ __device__ __forceinline__ int packed_nax(const ProjParams& p, const ProjBinDev&
   return p.segs[p.lines[pb.first_line].seg + p.S].nax;
 }
 
+// The transformed elements of a batch of 32, per line of the group being projected: xs[g][k] = (image index of
+// element k under line g without its z, z after the line's z operation - min_z); lane k computes element k for
+// every line, so each transform is done once instead of once per axial position.
+constexpr int kPackedMaxLines = 16;  // lines per basic bin handled per pass (32 / nax, at most the bin's lines)
+struct PackedStage {
+  int2 xs[kPackedMaxLines][33];  // padded: the lanes of different lines read the same k without bank conflicts
+  float w[32];
+};
+
 template <int EPI>
 __global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                                           int nbins, const float* __restrict__ img,
                                                                           float* __restrict__ out, FwdEpilogue ep) {
+  __shared__ PackedStage stage[kPackedWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bi = blockIdx.x * kPackedWarps + warp;
   if (bi >= nbins) return;  // whole warps only: no block-wide synchronisation below
+  PackedStage& S = stage[warp];
   const ProjBinDev pb = p.bins[bin_list[bi]];
   const RowElem* row = p.rows + pb.row_offset;
   const int nax = packed_nax(p, pb);
-  const int G = 32 / nax;
+  const int G = min(32 / nax, kPackedMaxLines);
+  const int gi = lane / nax;
   double ll = 0.0;
   unsigned ncancel = 0;
   for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
     const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    const int ng = min(G, pb.num_lines - l0);
     float acc = 0.f;
     for (int k0 = 0; k0 < pb.row_len; k0 += 32) {
-      RowElem mine{0u, 0.f};
-      if (k0 + lane < pb.row_len) mine = row[k0 + lane];
       const int cnt = min(32, pb.row_len - k0);
-      int k = 0;
-      for (; k + 4 <= cnt; k += 4) {
-        uint32_t zyx[4];
-        float w[4], xv[4];
-        int v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          zyx[u] = __shfl_sync(0xffffffffu, mine.zyx, k + u);
-          w[u] = __shfl_sync(0xffffffffu, mine.v, k + u);
-          v[u] = t.act ? packed_voxel(p, t, zyx[u]) : -1;
-          xv[u] = v[u] >= 0 ? __ldg(img + v[u]) : 0.f;
+      __syncwarp();
+      if (lane < cnt) {
+        const RowElem e = row[k0 + lane];
+        int z, y, x;
+        unpack_zyx(e.zyx, z, y, x);
+        S.w[lane] = e.v;
+        for (int g = 0; g < ng; ++g) {
+          const LineDev L = p.lines[pb.first_line + l0 + g];
+          const int swap = L.flags & 1;
+          const int xt = (swap ? y : x) * ((L.flags & 2) ? -1 : 1);
+          const int yt = (swap ? x : y) * ((L.flags & 4) ? -1 : 1);
+          const int zt = ((L.flags & 8) ? static_cast<int>(L.q) - z : z) - p.min_z;
+          S.xs[g][lane] = make_int2(((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz, zt);
         }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (v[u] >= 0) acc += xv[u] * w[u];
       }
-      for (; k < cnt; ++k) {
-        const uint32_t zyx = __shfl_sync(0xffffffffu, mine.zyx, k);
-        const float w = __shfl_sync(0xffffffffu, mine.v, k);
-        const int v = t.act ? packed_voxel(p, t, zyx) : -1;
-        if (v >= 0) acc += __ldg(img + v) * w;
+      __syncwarp();
+      if (t.act) {
+        const int zoff = t.a * t.s.npa;
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+          int v[4];
+          float xv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int2 X = S.xs[gi][k + u];
+            const int zz = X.y + zoff;
+            v[u] = (zz >= 0 && zz < p.nz) ? X.x + zz : -1;
+            xv[u] = v[u] >= 0 ? __ldg(img + v[u]) : 0.f;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (v[u] >= 0) acc += xv[u] * S.w[k + u];
+        }
+        for (; k < cnt; ++k) {
+          const int2 X = S.xs[gi][k];
+          const int zz = X.y + zoff;
+          if (zz >= 0 && zz < p.nz) acc += __ldg(img + X.x + zz) * S.w[k];
+        }
       }
     }
     if (t.act) forward_store<EPI>(p, t.L.seg, t.L.view, t.s.tofi, t.s.nax, t.s.out_base + t.a, t.a, acc, out, ep, ll, ncancel);
@@ -400,30 +428,49 @@ template <typename Acc>
 __global__ void __launch_bounds__(kPackedWarps * 32) back_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
                                                                        int nbins, const float* __restrict__ pd, Acc img,
                                                                        int zero_ends) {
+  __shared__ PackedStage stage[kPackedWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bi = blockIdx.x * kPackedWarps + warp;
   if (bi >= nbins) return;
+  PackedStage& S = stage[warp];
   const ProjBinDev pb = p.bins[bin_list[bi]];
   const RowElem* row = p.rows + pb.row_offset;
   const int nax = packed_nax(p, pb);
-  const int G = 32 / nax;
+  const int G = min(32 / nax, kPackedMaxLines);
+  const int gi = lane / nax;
   for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
     PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    const int ng = min(G, pb.num_lines - l0);
     float d = 0.f;
     if (t.act && !(zero_ends && t.L.seg == 0 && (t.a == 0 || t.a == t.s.nax - 1)))
       d = pd ? __ldg(pd + t.s.out_base + t.a) : 1.f;  // pd == nullptr back-projects ones
     t.act = t.act && d != 0.f;  // zero bins are skipped (ProjMatrixElemsForOneBin.cxx:339-340)
     if (!__any_sync(0xffffffffu, t.act)) continue;
+    const int zoff = t.a * t.s.npa;
     for (int k0 = 0; k0 < pb.row_len; k0 += 32) {
-      RowElem mine{0u, 0.f};
-      if (k0 + lane < pb.row_len) mine = row[k0 + lane];
       const int cnt = min(32, pb.row_len - k0);
-      for (int k = 0; k < cnt; ++k) {
-        const uint32_t zyx = __shfl_sync(0xffffffffu, mine.zyx, k);
-        const float w = __shfl_sync(0xffffffffu, mine.v, k);
-        const int v = t.act ? packed_voxel(p, t, zyx) : -1;
-        if (v >= 0) img.add(v, w * d);
+      __syncwarp();
+      if (lane < cnt) {
+        const RowElem e = row[k0 + lane];
+        int z, y, x;
+        unpack_zyx(e.zyx, z, y, x);
+        S.w[lane] = e.v;
+        for (int g = 0; g < ng; ++g) {
+          const LineDev L = p.lines[pb.first_line + l0 + g];
+          const int swap = L.flags & 1;
+          const int xt = (swap ? y : x) * ((L.flags & 2) ? -1 : 1);
+          const int yt = (swap ? x : y) * ((L.flags & 4) ? -1 : 1);
+          const int zt = ((L.flags & 8) ? static_cast<int>(L.q) - z : z) - p.min_z;
+          S.xs[g][lane] = make_int2(((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz, zt);
+        }
       }
+      __syncwarp();
+      if (t.act)
+        for (int k = 0; k < cnt; ++k) {
+          const int2 X = S.xs[gi][k];
+          const int zz = X.y + zoff;
+          if (zz >= 0 && zz < p.nz) img.add(X.x + zz, S.w[k] * d);
+        }
     }
   }
 }

@@ -924,7 +924,7 @@ cudaError_t copy_views(const Geometry& g, float* dst, const float* src, int v0, 
                            sizeof(float) * nt * (v1 - v0), rows, kind, st);
 }
 
-constexpr int kHostViewGroups = 16;
+constexpr int kHostViewGroups = 8;
 
 // the subset's path items ordered by the group of views they write (kHostViewGroups equal view ranges)
 const b200rt_projector::ViewGroups& view_groups(b200rt_projector& h, int subset, int nsub) {
@@ -1839,6 +1839,7 @@ struct b200rt_batch {
   DevBuf<b200::ProjParams> d_geoms;
   DevBuf<b200::PathParams> d_pgeoms;
   bool paths = false;  // every frame's projector has path items: the column-staged batched kernels
+  bool packed = false;  // otherwise, every segment of every frame has few axial positions: the packed kernels
   int smem_f = 0, smem_b = 0;
   DevBuf<b200::BatchFrameDev> d_frames;
   DevBuf<unsigned int> counters;  // work-queue heads of the forward and back launches
@@ -1888,6 +1889,8 @@ void batch_finalize(b200rt_batch& b) {
   b.d_geoms.upload(gp, st);
   b.paths = true;
   for (auto* h : b.geoms) b.paths = b.paths && h->use_paths;
+  b.packed = !b.paths;
+  for (auto* h : b.geoms) b.packed = b.packed && h->params.max_nax <= b200::kPackedMaxNax;
   if (b.paths) {
     std::vector<b200::PathParams> pg;
     b.smem_f = b.smem_b = 0;
@@ -1939,6 +1942,9 @@ void batch_finalize(b200rt_batch& b) {
   if (b.paths) {
     b.max_fwd = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
     b.max_back = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
+  } else if (b.packed) {
+    b.max_fwd = b200::batch_packed_max_ctas_per_sm(true);
+    b.max_back = b200::batch_packed_max_ctas_per_sm(false);
   } else {
     b.max_fwd = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
     b.max_back = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
@@ -2033,6 +2039,9 @@ cudaError_t batch_launch(b200rt_batch& b, int dir, const BatchItem* items, int n
                                                        n, b.counters.p, grid, st)
                     : b200::launch_back_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.smem_b, b.d_frames.p, items, n,
                                                     b.counters.p + 1, grid, st);
+  if (b.packed)
+    return dir == 0 ? b200::launch_forward_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
+                    : b200::launch_back_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);
   return dir == 0 ? b200::launch_forward_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p, grid, st)
                   : b200::launch_back_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p + 1, grid,
                                             st);

@@ -293,6 +293,12 @@ cudaError_t launch_forward_batch(const ProjParams* geoms, int npa, size_t smem_b
 cudaError_t launch_back_batch(const ProjParams* geoms, int npa, size_t smem_bytes, const BatchFrameDev* frames,
                               const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st);
 // resident CTAs per SM of the batched kernels (0 on error); also sets their shared-memory limit
+// batched packed kernels (frames whose segments have at most kPackedMaxNax axial positions): one item per warp
+cudaError_t launch_forward_batch_packed(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                        int nitems, unsigned* counter, int grid, cudaStream_t st);
+cudaError_t launch_back_batch_packed(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                     int nitems, unsigned* counter, int grid, cudaStream_t st);
+int batch_packed_max_ctas_per_sm(bool forward);
 int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward);
 // dynamic shared memory of the projection kernels for a row length bound
 size_t proj_smem_bytes(int max_row_len);

@@ -36,22 +36,28 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
-// sum over the row of img[voxel] * weight, each lane over elements lane, lane + 32, ... in order, four elements'
-// loads in flight at a time
+// sum over the row of img[voxel] * weight, each lane over elements lane, lane + 32, ... in order, kLmBatch
+// elements' loads in flight at a time
+constexpr int kLmBatch = 4;
+
 __device__ __forceinline__ float lm_forward(const ProjParams& p, const RowElem* __restrict__ row, int len,
                                             const LineDev& L, int zadd, const float* __restrict__ img, int lane) {
   float f = 0.f;
   int k = lane;
-  for (; k + 96 < len; k += 128) {
-    const RowElem e0 = row[k], e1 = row[k + 32], e2 = row[k + 64], e3 = row[k + 96];
-    const int v0 = lm_voxel(p, e0, L, zadd), v1 = lm_voxel(p, e1, L, zadd), v2 = lm_voxel(p, e2, L, zadd),
-              v3 = lm_voxel(p, e3, L, zadd);
-    const float x0 = v0 >= 0 ? __ldg(img + v0) : 0.f, x1 = v1 >= 0 ? __ldg(img + v1) : 0.f;
-    const float x2 = v2 >= 0 ? __ldg(img + v2) : 0.f, x3 = v3 >= 0 ? __ldg(img + v3) : 0.f;
-    if (v0 >= 0) f += x0 * e0.v;
-    if (v1 >= 0) f += x1 * e1.v;
-    if (v2 >= 0) f += x2 * e2.v;
-    if (v3 >= 0) f += x3 * e3.v;
+  for (; k + 32 * (kLmBatch - 1) < len; k += 32 * kLmBatch) {
+    RowElem e[kLmBatch];
+    int v[kLmBatch];
+    float xv[kLmBatch];
+#pragma unroll
+    for (int u = 0; u < kLmBatch; ++u) e[u] = row[k + 32 * u];
+#pragma unroll
+    for (int u = 0; u < kLmBatch; ++u) {
+      v[u] = lm_voxel(p, e[u], L, zadd);
+      xv[u] = v[u] >= 0 ? __ldg(img + v[u]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kLmBatch; ++u)
+      if (v[u] >= 0) f += xv[u] * e[u].v;
   }
   for (; k < len; k += 32) {
     const RowElem e = row[k];
@@ -64,14 +70,15 @@ __device__ __forceinline__ float lm_forward(const ProjParams& p, const RowElem* 
 __device__ __forceinline__ void lm_back(const ProjParams& p, const RowElem* __restrict__ row, int len, const LineDev& L,
                                         int zadd, float data, float* __restrict__ out, int lane) {
   int k = lane;
-  for (; k + 96 < len; k += 128) {
-    const RowElem e0 = row[k], e1 = row[k + 32], e2 = row[k + 64], e3 = row[k + 96];
-    const int v0 = lm_voxel(p, e0, L, zadd), v1 = lm_voxel(p, e1, L, zadd), v2 = lm_voxel(p, e2, L, zadd),
-              v3 = lm_voxel(p, e3, L, zadd);
-    if (v0 >= 0) atomicAdd(out + v0, e0.v * data);
-    if (v1 >= 0) atomicAdd(out + v1, e1.v * data);
-    if (v2 >= 0) atomicAdd(out + v2, e2.v * data);
-    if (v3 >= 0) atomicAdd(out + v3, e3.v * data);
+  for (; k + 32 * (kLmBatch - 1) < len; k += 32 * kLmBatch) {
+    RowElem e[kLmBatch];
+#pragma unroll
+    for (int u = 0; u < kLmBatch; ++u) e[u] = row[k + 32 * u];
+#pragma unroll
+    for (int u = 0; u < kLmBatch; ++u) {
+      const int v = lm_voxel(p, e[u], L, zadd);
+      if (v >= 0) atomicAdd(out + v, e[u].v * data);
+    }
   }
   for (; k < len; k += 32) {
     const RowElem e = row[k];

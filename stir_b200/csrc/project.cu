@@ -349,22 +349,15 @@ struct PackedStage {
   float w[32];
 };
 
+// one basic bin by one warp (the lanes are (line, axial position) pairs); S is the warp's staging table
 template <int EPI>
-__global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                                          int nbins, const float* __restrict__ img,
-                                                                          float* __restrict__ out, FwdEpilogue ep) {
-  __shared__ PackedStage stage[kPackedWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int bi = blockIdx.x * kPackedWarps + warp;
-  if (bi >= nbins) return;  // whole warps only: no block-wide synchronisation below
-  PackedStage& S = stage[warp];
-  const ProjBinDev pb = p.bins[bin_list[bi]];
+__device__ __forceinline__ void forward_packed_bin(const ProjParams& p, const ProjBinDev& pb, PackedStage& S,
+                                                   const float* __restrict__ img, float* __restrict__ out,
+                                                   const FwdEpilogue& ep, double& ll, unsigned& ncancel, int lane) {
   const RowElem* row = p.rows + pb.row_offset;
   const int nax = packed_nax(p, pb);
   const int G = min(32 / nax, kPackedMaxLines);
   const int gi = lane / nax;
-  double ll = 0.0;
-  unsigned ncancel = 0;
   for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
     const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
     const int ng = min(G, pb.num_lines - l0);
@@ -413,6 +406,20 @@ __global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjP
     }
     if (t.act) forward_store<EPI>(p, t.L.seg, t.L.view, t.s.tofi, t.s.nax, t.s.out_base + t.a, t.a, acc, out, ep, ll, ncancel);
   }
+  __syncwarp();  // the staging table is free for the warp's next bin
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                                          int nbins, const float* __restrict__ img,
+                                                                          float* __restrict__ out, FwdEpilogue ep) {
+  __shared__ PackedStage stage[kPackedWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kPackedWarps + warp;
+  if (bi >= nbins) return;  // whole warps only: no block-wide synchronisation below
+  double ll = 0.0;
+  unsigned ncancel = 0;
+  forward_packed_bin<EPI>(p, p.bins[bin_list[bi]], stage[warp], img, out, ep, ll, ncancel, lane);
   if (EPI == kEpiRatio || EPI == kEpiGradient) {
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
@@ -425,15 +432,8 @@ __global__ void __launch_bounds__(kPackedWarps * 32) forward_packed_kernel(ProjP
 }
 
 template <typename Acc>
-__global__ void __launch_bounds__(kPackedWarps * 32) back_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
-                                                                       int nbins, const float* __restrict__ pd, Acc img,
-                                                                       int zero_ends) {
-  __shared__ PackedStage stage[kPackedWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int bi = blockIdx.x * kPackedWarps + warp;
-  if (bi >= nbins) return;
-  PackedStage& S = stage[warp];
-  const ProjBinDev pb = p.bins[bin_list[bi]];
+__device__ __forceinline__ void back_packed_bin(const ProjParams& p, const ProjBinDev& pb, PackedStage& S,
+                                                const float* __restrict__ pd, const Acc& img, int zero_ends, int lane) {
   const RowElem* row = p.rows + pb.row_offset;
   const int nax = packed_nax(p, pb);
   const int G = min(32 / nax, kPackedMaxLines);
@@ -473,6 +473,18 @@ __global__ void __launch_bounds__(kPackedWarps * 32) back_packed_kernel(ProjPara
         }
     }
   }
+  __syncwarp();
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kPackedWarps * 32) back_packed_kernel(ProjParams p, const int* __restrict__ bin_list,
+                                                                       int nbins, const float* __restrict__ pd, Acc img,
+                                                                       int zero_ends) {
+  __shared__ PackedStage stage[kPackedWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kPackedWarps + warp;
+  if (bi >= nbins) return;
+  back_packed_bin<Acc>(p, p.bins[bin_list[bi]], stage[warp], pd, img, zero_ends, lane);
 }
 
 // ---- batched (several reconstructions in one launch) ------------------------
@@ -570,6 +582,67 @@ cudaError_t transpose(const float* in, float* out, int rows, int64_t cols, cudaS
 
 size_t proj_smem_bytes(int max_row_len) {
   return sizeof(XElem) * kWarps * kChunk + sizeof(RowElem) * static_cast<size_t>(max_row_len > 0 ? max_row_len : 1);
+}
+
+// Batched packed kernels: a persistent grid whose warps take (frame, basic bin) items from the queue one at a time
+// and project them as forward_packed_bin / back_packed_bin; each warp stages its item's frame, geometry and bin.
+struct WarpStage {
+  ProjParams p;
+  BatchFrameDev f;
+  ProjBinDev pb;
+};
+
+__device__ __forceinline__ bool next_item_warp(unsigned* counter, const BatchItem* __restrict__ items, int nitems,
+                                               const ProjParams* __restrict__ geoms,
+                                               const BatchFrameDev* __restrict__ frames, WarpStage& st, int lane) {
+  __syncwarp();  // the warp has finished with the previous item
+  int it = 0;
+  if (lane == 0) it = static_cast<int>(atomicAdd(counter, 1u));
+  it = __shfl_sync(0xffffffffu, it, 0);
+  if (it >= nitems) return false;
+  const BatchItem wi = items[it];
+  const int g = frames[wi.frame].geom;
+  constexpr int nf = sizeof(BatchFrameDev) / 4, np = sizeof(ProjParams) / 4, nb = sizeof(ProjBinDev) / 4;
+  for (int t = lane; t < nf + np + nb; t += 32) {
+    if (t < nf)
+      reinterpret_cast<uint32_t*>(&st.f)[t] = reinterpret_cast<const uint32_t*>(frames + wi.frame)[t];
+    else if (t < nf + np)
+      reinterpret_cast<uint32_t*>(&st.p)[t - nf] = reinterpret_cast<const uint32_t*>(geoms + g)[t - nf];
+    else
+      reinterpret_cast<uint32_t*>(&st.pb)[t - nf - np] =
+          reinterpret_cast<const uint32_t*>(geoms[g].bins + wi.bin)[t - nf - np];
+  }
+  __syncwarp();
+  return true;
+}
+
+__global__ void __launch_bounds__(kPackedWarps * 32) forward_batch_packed_kernel(const ProjParams* __restrict__ geoms,
+                                                                                const BatchFrameDev* __restrict__ frames,
+                                                                                const BatchItem* __restrict__ items,
+                                                                                int nitems, unsigned* counter) {
+  __shared__ WarpStage wst[kPackedWarps];
+  __shared__ PackedStage stage[kPackedWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpStage& st = wst[warp];
+  while (next_item_warp(counter, items, nitems, geoms, frames, st, lane)) {
+    double ll = 0.0;
+    unsigned ncancel = 0;
+    forward_packed_bin<kEpiRatio>(st.p, st.pb, stage[warp], st.f.x, st.f.ratio, st.f.ep, ll, ncancel, lane);
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
+  }
+}
+
+__global__ void __launch_bounds__(kPackedWarps * 32) back_batch_packed_kernel(const ProjParams* __restrict__ geoms,
+                                                                             const BatchFrameDev* __restrict__ frames,
+                                                                             const BatchItem* __restrict__ items,
+                                                                             int nitems, unsigned* counter) {
+  __shared__ WarpStage wst[kPackedWarps];
+  __shared__ PackedStage stage[kPackedWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpStage& st = wst[warp];
+  while (next_item_warp(counter, items, nitems, geoms, frames, st, lane))
+    back_packed_bin<FloatAcc>(st.p, st.pb, stage[warp], st.f.ratio, FloatAcc{st.f.u}, 0, lane);
 }
 
 static size_t proj_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p.max_row_len); }
@@ -673,6 +746,28 @@ cudaError_t launch_back_batch(const ProjParams* geoms, int npa, size_t smem_byte
   else
     back_batch_kernel<0><<<grid, kThreads, smem_bytes, st>>>(geoms, frames, items, nitems, counter);
   return cudaGetLastError();
+}
+
+cudaError_t launch_forward_batch_packed(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                        int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  forward_batch_packed_kernel<<<grid, kPackedWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_batch_packed(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                     int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  back_batch_packed_kernel<<<grid, kPackedWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+int batch_packed_max_ctas_per_sm(bool forward) {
+  const void* fn = forward ? reinterpret_cast<const void*>(forward_batch_packed_kernel)
+                           : reinterpret_cast<const void*>(back_batch_packed_kernel);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kPackedWarps * 32, 0) != cudaSuccess) return 0;
+  return n;
 }
 
 int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward) {

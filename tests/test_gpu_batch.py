@@ -154,3 +154,40 @@ def test_batch_rejects_bad_frames(frames):
     with pytest.raises(_abi.B200Error):
         batch.set_config(order=5)
     batch.close()
+
+
+def test_batch_tof_frames_equal_frame_by_frame(cuda_device):
+    """TOF frames go through the per-basic-bin batched kernels (one CTA per timing bin of a basic bin); frame by
+    frame they go through the packed kernels: the reconstructions agree to the order of float additions."""
+    import torch
+    from stir_b200.batch import BatchedOSMAPOSL
+    from stir_b200.osmaposl import OSMAPOSLReconstruction
+    from stir_b200.projectors import RayTracingProjector
+    pdi, img = G.tof_small_3d_pet(num_tof_bins=7, timing_bin_ps=250.0, num_views=48)
+    proj = RayTracingProjector(pdi, img, device=cuda_device)
+    xt = phantoms.cylinder_with_spheres(proj.image, radius_mm=90.0, n_spheres=2, sphere_radius=(10.0, 10.0), seed=3)
+    ybar = proj.forward_dev(proj.image_to_device_layout(torch.from_numpy(np.ascontiguousarray(xt, np.float32)).cuda()))
+    bg = float(0.1 * ybar.mean())
+    rng = np.random.default_rng(8)
+    batch = BatchedOSMAPOSL()
+    runs = []
+    from stir_b200.osmaposl import QuadraticPrior
+    # a strong MAP-OSL prior (beta 0.5 here) multiplies float-rounding differences about tenfold per sub-iteration
+    # (the clamped one-step-late denominator), so the comparison uses beta 0.05, where they stay at 1e-7
+    for k, (nsub, n, prior) in enumerate([(3, 4, None), (2, 3, None), (7, 9, QuadraticPrior(0.05))]):
+        scale = (1e6 * (k + 1)) / float((ybar + bg).sum())
+        y = torch.from_numpy(rng.poisson(((ybar + bg) * scale).cpu().numpy()).astype(np.float32) / np.float32(scale)).cuda()
+        add = torch.full_like(y, bg)
+        ref = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n, prior=prior)
+        xr = proj.empty_image().fill_(1.0)
+        ref.reconstruct(xr)
+        rec = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n, prior=prior)
+        rec.sensitivities = ref.sensitivities
+        x = proj.empty_image().fill_(1.0)
+        batch.add(rec, x)
+        runs.append((x, xr))
+    batch.reconstruct(use_graph=True)
+    torch.cuda.synchronize()
+    for x, xr in runs:
+        assert rel_l2(x.cpu().numpy(), xr.cpu().numpy()) < BATCH_TOL
+    batch.close()

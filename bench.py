@@ -236,6 +236,64 @@ def listmode_and_priors(proj, pdi, img, xd, cpu_ref):
     return out
 
 
+def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5):
+    """The TOF configuration's reconstructions: `frames` noise realisations (seeds 0..), OSMAPOSL with a
+    QuadraticPrior (beta 0.5, 3x3x3 neighbourhood), 21 subsets x 3 iterations, batched in one graph against one
+    at a time.  With beta 0.5 the one-step-late update amplifies float-rounding differences, so the two differ by
+    far more than rounding after 63 sub-iterations (reported, not a parity check)."""
+    import torch
+    from stir_b200 import phantoms
+    from stir_b200.batch import BatchedOSMAPOSL
+    from stir_b200.osmaposl import OSMAPOSLReconstruction, QuadraticPrior
+    xt = phantoms.cylinder_with_spheres(proj.image, radius_mm=90.0, n_spheres=2, sphere_radius=(10.0, 10.0), seed=3)
+    ybar = proj.forward_dev(proj.image_to_device_layout(torch.from_numpy(np.ascontiguousarray(xt, np.float32)).cuda()))
+    bg = float(0.1 * ybar.mean())
+    data = []
+    for k in range(frames):
+        g = torch.Generator(device=ybar.device).manual_seed(k)
+        scale = 5e6 / float((ybar + bg).sum())
+        y = torch.poisson((ybar + bg) * scale, generator=g) / scale
+        data.append((y, torch.full_like(y, bg)))
+    n = nsub * iterations
+    objs = [OSMAPOSLReconstruction(proj, y, additive=a, num_subsets=nsub, num_subiterations=n,
+                                   prior=QuadraticPrior(beta)).set_up() for y, a in data]
+    xs = [proj.empty_image() for _ in objs]
+
+    def per_frame():
+        for r, x in zip(objs, xs):
+            x.fill_(1.0)
+            r.reconstruct(x)
+
+    per_frame()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    per_frame()
+    torch.cuda.synchronize()
+    t_pf = time.perf_counter() - t0
+    batch = BatchedOSMAPOSL()
+    bx = []
+    for (y, a), r0 in zip(data, objs):
+        r = OSMAPOSLReconstruction(proj, y, additive=a, num_subsets=nsub, num_subiterations=n, prior=QuadraticPrior(beta))
+        r.sensitivities = r0.sensitivities
+        x = proj.empty_image().fill_(1.0)
+        batch.add(r, x)
+        bx.append(x)
+    batch.reconstruct(use_graph=True)  # captures the graph
+    for x in bx:
+        x.fill_(1.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.reconstruct(use_graph=True)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    batch.close()
+    return {"metric": "batched TOF OSMAPOSL reconstructions/s", "value": frames / t_b, "unit": "reconstructions/s",
+            "per_frame_value": frames / t_pf, "speedup_vs_per_frame": t_pf / t_b, "frames": frames,
+            "subsets": nsub, "sub_iterations": n, "prior": f"QuadraticPrior beta {beta}",
+            "workload": "noise realisations (torch Poisson, seeds 0..3, 5e6 counts) of a cylinder with 2 spheres, "
+                        "additive background 10 %; wall clock with a device synchronisation on both sides"}
+
+
 def tof_workload(with_cpu, device):
     """TOF forward + back projection (per-basic-bin kernels with the TOF rows) on the 8-ring scanner with 33 timing
     bins of 50 ps and a 550 ps FWHM kernel (19.5M TOF bins), against the oracle on one subset."""
@@ -258,6 +316,7 @@ def tof_workload(with_cpu, device):
                "tof_bins_per_step": n, "forward_ms": fms, "back_ms": bms, "setup_s": setup_s, "gpu_launches": 2,
                "workload": "8 rings x 288 det (R 300 mm), span 1, 144 views x 64 tang, 33 timing bins of 50 ps, "
                            "Gaussian 550 ps FWHM (STIR truncation), image 64x64x15; per-basic-bin TOF kernels"}
+        res["batched"] = tof_batched_reconstructions(proj)
         if with_cpu:
             from oracle.oracle import Oracle
             orc = Oracle(proj.geometry)

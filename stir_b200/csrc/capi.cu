@@ -139,6 +139,14 @@ struct b200rt_projector {
   std::map<std::pair<int, int>, ViewGroups> view_groups;
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> copy_events;
+  // TOF by basic bin (the TOF-grouped packed kernels): non-TOF basic rows, per-element weights of every timing
+  // bin, one entry per basic bin, its view, and the subsets' lists of basic bins
+  DevBuf<RowElem> tof_basic_rows;
+  DevBuf<float> tof_w;
+  DevBuf<ProjBinDev> tof_basic;
+  std::vector<int> h_tof_basic_view;
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf<int>>> tof_group_lists;
+  std::map<std::pair<int, int>, int> tof_group_counts;
   // list mode: the related lines on the host, (tof, seg, view, tang) -> (basic bin, line, basic view)
   std::vector<LineDev> h_lines;
   DevBuf<int4> lm_table;
@@ -632,6 +640,31 @@ void setup_projector(b200rt_projector& h) {
     std::swap(h.rows.p, tof_rows.p);
     std::swap(h.rows.n, tof_rows.n);
     total = off[njobs];
+    int max_nax = 0;
+    for (int sg = -g.S(); sg <= g.S(); ++sg) max_nax = std::max(max_nax, g.nax(sg));
+    if (max_nax <= kPackedMaxNax) {
+      // keep the non-TOF rows (now in tof_rows) and the weights of every timing bin for the TOF-grouped kernels
+      std::swap(h.tof_basic_rows.p, tof_rows.p);
+      std::swap(h.tof_basic_rows.n, tof_rows.n);
+      h.tof_w.alloc(std::max<int64_t>(src, 1) * nt);
+      ck(launch_tof_weights(h.tof_basic_rows.p, d_jobs.p, njobs, tp, nt, h.tof_w.p, h.stream), "TOF weights");
+      std::vector<ProjBinDev> tb(nb);
+      h.h_tof_basic_view.resize(nb);
+      for (int b = 0; b < nb; ++b) {
+        const auto lg = group_lines(bbs[b].view, bbs[b].seg, bbs[b].tang == 0);
+        ProjBinDev pb{};
+        pb.row_offset = jobs[static_cast<size_t>(b) * nt].src_offset;
+        pb.row_len = static_cast<int32_t>(row_len[b]);
+        pb.tang = static_cast<int16_t>(bbs[b].tang);
+        pb.tof = static_cast<int16_t>(g.min_tof());
+        pb.first_line = lg.first;
+        pb.num_lines = lg.second;
+        tb[b] = pb;
+        h.h_tof_basic_view[b] = bbs[b].view;
+      }
+      h.tof_basic.upload(tb, h.stream);
+      ck(cudaStreamSynchronize(h.stream), "TOF weights");
+    }
     h.h_bins.resize(njobs);
     h.h_bin_view.resize(njobs);
     h.h_bin_seg.resize(njobs);
@@ -685,6 +718,9 @@ void setup_projector(b200rt_projector& h) {
   p.min_y = g.desc().min_y;
   p.min_x = g.desc().min_x;
   p.max_row_len = max_len;
+  p.tof_basic_rows = h.tof_basic_rows.p;
+  p.tof_w = h.tof_w.p;
+  p.tof_basic = h.tof_basic.p;
   p.uniform_npa = g.npa(0);
   p.max_nax = 0;
   for (int s = -g.S(); s <= g.S(); ++s) p.max_nax = std::max(p.max_nax, g.nax(s));
@@ -767,6 +803,27 @@ const int* path_list(b200rt_projector& h, int subset, int nsub, int& count) {
   return p;
 }
 
+// basic bins (TOF-grouped kernels) of a subset: those whose basic view v has v mod nsub == subset
+const int* tof_group_list(b200rt_projector& h, int subset, int nsub, int& count) {
+  const auto key = std::make_pair(subset, nsub);
+  auto it = h.tof_group_lists.find(key);
+  if (it != h.tof_group_lists.end()) {
+    count = h.tof_group_counts[key];
+    return it->second->p;
+  }
+  std::vector<int> list;
+  for (int b = 0; b < static_cast<int>(h.h_tof_basic_view.size()); ++b)
+    if (h.h_tof_basic_view[b] % nsub == subset) list.push_back(b);
+  auto buf = std::make_unique<DevBuf<int>>();
+  buf->upload(list, h.stream);
+  ck(cudaStreamSynchronize(h.stream), "TOF group list");
+  count = static_cast<int>(list.size());
+  h.tof_group_counts[key] = count;
+  const int* p = buf->p;
+  h.tof_group_lists[key] = std::move(buf);
+  return p;
+}
+
 // forward projection of one subset with the column-staged kernel where it applies (not for the
 // log-likelihood, whose per-CTA partial sums follow the basic bins), else the per-basic-bin kernel
 void forward_subset(b200rt_projector& h, const float* image, float* out, int subset, int nsub, cudaStream_t st,
@@ -775,6 +832,9 @@ void forward_subset(b200rt_projector& h, const float* image, float* out, int sub
   if (h.use_paths && (!ep || ep->mode != kEpiLoglik)) {
     const int* list = path_list(h, subset, nsub, n);
     ck(launch_forward_paths(h.params, h.pparams, list, n, image, out, st, ep), "forward projection");
+  } else if (h.params.tof_w && (!ep || ep->mode != kEpiLoglik)) {
+    const int* list = tof_group_list(h, subset, nsub, n);
+    ck(launch_forward_tof_grouped(h.params, list, n, image, out, st, ep), "forward projection");
   } else {
     const int* list = subset_list(h, subset, nsub, n);
     ck(launch_forward(h.params, list, n, image, out, st, ep), "forward projection");
@@ -835,11 +895,16 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
   const Geometry& g = *h.geo;
   const int64_t ni = g.image_size();
   int n = 0;
-  const int* list = h.use_paths ? path_list(h, subset, nsub, n) : subset_list(h, subset, nsub, n);
+  const bool grouped = !h.use_paths && h.params.tof_w;
+  const int* list = h.use_paths ? path_list(h, subset, nsub, n)
+                    : grouped   ? tof_group_list(h, subset, nsub, n)
+                                : subset_list(h, subset, nsub, n);
   if (mode == B200RT_BACKPROJECT_ATOMIC) {
     ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
     if (h.use_paths)
       ck(launch_back_paths_atomic(h.params, h.pparams, list, n, pd, image, st, zero_ends), "back projection");
+    else if (grouped)
+      ck(launch_back_tof_grouped(h.params, list, n, pd, image, nullptr, nullptr, st, zero_ends), "back projection");
     else
       ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
     return;
@@ -849,10 +914,14 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
     // largest column sum of A (A^T 1 over every bin): bounds every voxel's sum of |w d| / max|d|
     h.colmax.alloc(1);
     int nall = 0;
-    const int* all = h.use_paths ? path_list(h, 0, 1, nall) : subset_list(h, 0, 1, nall);
+    const int* all = h.use_paths ? path_list(h, 0, 1, nall)
+                     : grouped   ? tof_group_list(h, 0, 1, nall)
+                                 : subset_list(h, 0, 1, nall);
     ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
     if (h.use_paths)
       ck(launch_back_paths_atomic(h.params, h.pparams, all, nall, nullptr, image, st, 0), "column sums");
+    else if (grouped)
+      ck(launch_back_tof_grouped(h.params, all, nall, nullptr, image, nullptr, nullptr, st, 0), "column sums");
     else
       ck(launch_back_atomic(h.params, all, nall, nullptr, image, st, 0), "column sums");
     ck(launch_max(image, ni, h.det_partial.p, h.colmax.p, st), "column sums");
@@ -873,6 +942,9 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
   ck(cudaMemsetAsync(h.acc64.p, 0, sizeof(unsigned long long) * ni, st), "memset");
   if (h.use_paths)
     ck(launch_back_paths_fixed(h.params, h.pparams, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends),
+       "back projection");
+  else if (grouped)
+    ck(launch_back_tof_grouped(h.params, list, n, pd, nullptr, h.acc64.p, h.fixed_scale.p, st, zero_ends),
        "back projection");
   else
     ck(launch_back_fixed(h.params, list, n, pd, h.acc64.p, h.fixed_scale.p, st, zero_ends), "back projection");
@@ -1037,6 +1109,10 @@ void b200rt_destroy(b200rt_projector* h) {
     h->st_pd_a.release();
     h->st_pd_b.release();
     h->view_groups.clear();
+    h->tof_group_lists.clear();
+    h->tof_basic_rows.release();
+    h->tof_w.release();
+    h->tof_basic.release();
     h->lm_table.release();
     h->lm_partial.release();
     h->lm_sum.release();
@@ -1839,6 +1915,7 @@ struct b200rt_batch {
   DevBuf<b200::ProjParams> d_geoms;
   DevBuf<b200::PathParams> d_pgeoms;
   bool paths = false;  // every frame's projector has path items: the column-staged batched kernels
+  bool tof_grouped = false;  // otherwise, TOF frames with the timing bins of a basic bin grouped: TOF kernels
   bool packed = false;  // otherwise, every segment of every frame has few axial positions: the packed kernels
   int smem_f = 0, smem_b = 0;
   DevBuf<b200::BatchFrameDev> d_frames;
@@ -1889,7 +1966,9 @@ void batch_finalize(b200rt_batch& b) {
   b.d_geoms.upload(gp, st);
   b.paths = true;
   for (auto* h : b.geoms) b.paths = b.paths && h->use_paths;
-  b.packed = !b.paths;
+  b.tof_grouped = !b.paths;
+  for (auto* h : b.geoms) b.tof_grouped = b.tof_grouped && h->params.tof_w != nullptr;
+  b.packed = !b.paths && !b.tof_grouped;
   for (auto* h : b.geoms) b.packed = b.packed && h->params.max_nax <= b200::kPackedMaxNax;
   if (b.paths) {
     std::vector<b200::PathParams> pg;
@@ -1942,6 +2021,9 @@ void batch_finalize(b200rt_batch& b) {
   if (b.paths) {
     b.max_fwd = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
     b.max_back = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
+  } else if (b.tof_grouped) {
+    b.max_fwd = b200::batch_tof_max_ctas_per_sm(true);
+    b.max_back = b200::batch_tof_max_ctas_per_sm(false);
   } else if (b.packed) {
     b.max_fwd = b200::batch_packed_max_ctas_per_sm(true);
     b.max_back = b200::batch_packed_max_ctas_per_sm(false);
@@ -1979,6 +2061,9 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
           return static_cast<int64_t>(pa.ncols) * pa.num_lines > static_cast<int64_t>(pc.ncols) * pc.num_lines;
         });
       }
+    } else if (b.tof_grouped) {
+      for (int bin = 0; bin < static_cast<int>(h.h_tof_basic_view.size()); ++bin)
+        if (h.h_tof_basic_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
     } else {
       for (int bin = 0; bin < static_cast<int>(h.h_bins.size()); ++bin)
         if (h.h_bin_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
@@ -2039,6 +2124,9 @@ cudaError_t batch_launch(b200rt_batch& b, int dir, const BatchItem* items, int n
                                                        n, b.counters.p, grid, st)
                     : b200::launch_back_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.smem_b, b.d_frames.p, items, n,
                                                     b.counters.p + 1, grid, st);
+  if (b.tof_grouped)
+    return dir == 0 ? b200::launch_forward_batch_tof(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
+                    : b200::launch_back_batch_tof(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);
   if (b.packed)
     return dir == 0 ? b200::launch_forward_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
                     : b200::launch_back_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);

@@ -81,6 +81,12 @@ struct ProjParams {
   int max_row_len;
   int uniform_npa;  // planes per axial position if equal for all segments, else 0
   int max_nax;      // most axial positions of any segment
+  // TOF data by basic bin (the TOF-grouped packed kernels): the non-TOF basic rows, every element's weight for
+  // each timing bin ([element][timing bin], 0 where the TOF row has no element) and one entry per basic bin
+  // (row_offset into tof_basic_rows, tof = min timing bin); null without TOF
+  const RowElem* tof_basic_rows;
+  const float* tof_w;
+  const ProjBinDev* tof_basic;
 };
 // with at most this many axial positions per line the per-basic-bin kernels pack (line, axial position) pairs
 // into the lanes of a warp (project.cu)
@@ -299,6 +305,12 @@ cudaError_t launch_forward_batch_packed(const ProjParams* geoms, const BatchFram
 cudaError_t launch_back_batch_packed(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
                                      int nitems, unsigned* counter, int grid, cudaStream_t st);
 int batch_packed_max_ctas_per_sm(bool forward);
+// batched TOF-grouped kernels (TOF frames of packed geometries): items are (frame, basic bin of the TOF table)
+cudaError_t launch_forward_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                     int nitems, unsigned* counter, int grid, cudaStream_t st);
+cudaError_t launch_back_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                  int nitems, unsigned* counter, int grid, cudaStream_t st);
+int batch_tof_max_ctas_per_sm(bool forward);
 int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward);
 // dynamic shared memory of the projection kernels for a row length bound
 size_t proj_smem_bytes(int max_row_len);
@@ -429,6 +441,15 @@ struct TofParams {
   int erf_n;
   double erf_max, erf_period;
 };
+cudaError_t launch_tof_weights(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp, int ntof,
+                               float* w, cudaStream_t st);
+// TOF-grouped packed projections over basic bins (items index ProjParams::tof_basic); forward with the
+// kEpiNone / kEpiRatio / kEpiGradient epilogues; back atomic (float) or fixed point
+cudaError_t launch_forward_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* image,
+                                       float* projdata, cudaStream_t st, const FwdEpilogue* ep);
+cudaError_t launch_back_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* projdata,
+                                    float* image, unsigned long long* acc, const double* scale, cudaStream_t st,
+                                    int zero_ends);
 cudaError_t launch_tof_rows(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp,
                             const int64_t* out_offsets, RowElem* out, int* counts, cudaStream_t st);
 

@@ -16,6 +16,8 @@
 //          ProjMatrixElemsForOneBin::forward_project (ProjMatrixElemsForOneBin.cxx:354-370).
 // Back:    image[col_k][z_k + npa*a] += w_k * projdata[line][a] for projdata != 0
 //          (ProjMatrixElemsForOneBin::back_project, :333-351), with float atomics.
+#include <type_traits>
+
 #include "internal.hpp"
 #include "epilogue.cuh"
 
@@ -584,6 +586,201 @@ size_t proj_smem_bytes(int max_row_len) {
   return sizeof(XElem) * kWarps * kChunk + sizeof(RowElem) * static_cast<size_t>(max_row_len > 0 ? max_row_len : 1);
 }
 
+// ---- TOF-grouped packed kernels ------------------------------------------------
+// With TOF, every timing bin of a basic bin has its own row: the basic row's elements weighted by the timing
+// bin's kernel.  Here a warp takes a basic bin with all its timing bins: it walks the non-TOF row once per group of
+// kTofGroup timing bins, gathers each voxel once, and applies the group's weights (staged per batch of 32
+// elements in shared memory) from registers.  Forward: each (line, axial position, timing bin) sum adds the same
+// products in the same order as the TOF row (elements outside the TOF row have weight 0 and add +-0), so the
+// results are bit-identical.  Back: the contributions of the group's timing bins to a voxel are summed before the
+// one atomic (float), or rounded one by one and summed as integers (fixed point: the same integers).
+constexpr int kTofWarps = 4;
+constexpr int kTofGroup = 16;
+struct TofStage {
+  int2 xs[kPackedMaxLines][33];
+  float4 w[32][kTofGroup / 4];
+};
+
+// transforms and weights of elements [e0, e0 + cnt) of the basic row for the lines l0.. (ng of them) and the
+// timing bins [k0, k0 + kTofGroup)
+__device__ __forceinline__ void tof_stage_batch(const ProjParams& p, const ProjBinDev& pb, const RowElem* row,
+                                                const float* wrow, int K, int l0, int ng, int e0, int cnt, int k0,
+                                                TofStage& S, int lane) {
+  __syncwarp();
+  if (lane < cnt) {
+    const RowElem e = row[e0 + lane];
+    int z, y, x;
+    unpack_zyx(e.zyx, z, y, x);
+    for (int g = 0; g < ng; ++g) {
+      const LineDev L = p.lines[pb.first_line + l0 + g];
+      const int swap = L.flags & 1;
+      const int xt = (swap ? y : x) * ((L.flags & 2) ? -1 : 1);
+      const int yt = (swap ? x : y) * ((L.flags & 4) ? -1 : 1);
+      const int zt = ((L.flags & 8) ? static_cast<int>(L.q) - z : z) - p.min_z;
+      S.xs[g][lane] = make_int2(((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz, zt);
+    }
+  }
+  // weights: the batch's elements x timing bins are contiguous ([element][timing bin]); coalesced loads
+  float* sw = reinterpret_cast<float*>(S.w);
+  const float* src = wrow + static_cast<int64_t>(e0) * K;
+  for (int i = lane; i < 32 * kTofGroup; i += 32) {
+    const int e = i / kTofGroup, kk = i % kTofGroup;
+    sw[i] = (e < cnt && k0 + kk < K) ? __ldg(src + static_cast<int64_t>(e) * K + k0 + kk) : 0.f;
+  }
+  __syncwarp();
+}
+
+template <int EPI>
+__device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
+                                                         const float* __restrict__ img, float* __restrict__ out,
+                                                         const FwdEpilogue& ep, double& ll, unsigned& ncancel,
+                                                         int lane) {
+  const RowElem* row = p.tof_basic_rows + pb.row_offset;
+  const int K = p.num_tof;
+  const float* wrow = p.tof_w + pb.row_offset * K;
+  const int nax = packed_nax(p, pb);
+  const int G = min(32 / nax, kPackedMaxLines);
+  const int gi = lane / nax;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
+    const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    const int ng = min(G, pb.num_lines - l0);
+    const int zoff = t.a * t.s.npa;
+    for (int k0 = 0; k0 < K; k0 += kTofGroup) {
+      float acc[kTofGroup];
+#pragma unroll
+      for (int kk = 0; kk < kTofGroup; ++kk) acc[kk] = 0.f;
+      for (int e0 = 0; e0 < pb.row_len; e0 += 32) {
+        const int cnt = min(32, pb.row_len - e0);
+        tof_stage_batch(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
+        if (t.act)
+          for (int k = 0; k < cnt; ++k) {
+            const int2 X = S.xs[gi][k];
+            const int zz = X.y + zoff;
+            if (zz < 0 || zz >= p.nz) continue;
+            const float xv = __ldg(img + X.x + zz);
+#pragma unroll
+            for (int q = 0; q < kTofGroup / 4; ++q) {
+              const float4 w = S.w[k][q];
+              acc[4 * q] += xv * w.x;
+              acc[4 * q + 1] += xv * w.y;
+              acc[4 * q + 2] += xv * w.z;
+              acc[4 * q + 3] += xv * w.w;
+            }
+          }
+      }
+      if (t.act)
+#pragma unroll
+        for (int kk = 0; kk < kTofGroup; ++kk)
+          if (k0 + kk < K)
+            forward_store<EPI>(p, t.L.seg, t.L.view, k0 + kk, t.s.nax,
+                               t.s.out_base + static_cast<int64_t>(k0 + kk) * p.tof_stride + t.a, t.a, acc[kk], out, ep,
+                               ll, ncancel);
+    }
+  }
+  __syncwarp();
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kTofWarps * 32) forward_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
+                                                                            int nitems, const float* __restrict__ img,
+                                                                            float* __restrict__ out, FwdEpilogue ep) {
+  __shared__ TofStage stage[kTofWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kTofWarps + warp;
+  if (bi >= nitems) return;
+  double ll = 0.0;
+  unsigned ncancel = 0;
+  forward_tof_grouped_body<EPI>(p, p.tof_basic[items[bi]], stage[warp], img, out, ep, ll, ncancel, lane);
+  if (EPI == kEpiRatio || EPI == kEpiGradient) {
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
+  }
+}
+
+// sum of a voxel's contributions over the group's timing bins, then one addition to the image
+struct TofFloatSum {
+  float* img;
+  using T = float;
+  __device__ __forceinline__ T term(float v) const { return v; }
+  __device__ __forceinline__ void flush(int64_t i, T v) const {
+    if (v != 0.f) atomicAdd(img + i, v);
+  }
+};
+struct TofFixedSum {
+  unsigned long long* acc;
+  double scale;
+  using T = long long;
+  __device__ __forceinline__ T term(float v) const { return __double2ll_rn(static_cast<double>(v) * scale); }
+  __device__ __forceinline__ void flush(int64_t i, T v) const {
+    if (v != 0) atomicAdd(acc + i, static_cast<unsigned long long>(v));
+  }
+};
+
+template <typename Sum>
+__device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
+                                                      const float* __restrict__ pd, const Sum& out, int zero_ends,
+                                                      int lane) {
+  const RowElem* row = p.tof_basic_rows + pb.row_offset;
+  const int K = p.num_tof;
+  const float* wrow = p.tof_w + pb.row_offset * K;
+  const int nax = packed_nax(p, pb);
+  const int G = min(32 / nax, kPackedMaxLines);
+  const int gi = lane / nax;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
+    const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+    const int ng = min(G, pb.num_lines - l0);
+    const int zoff = t.a * t.s.npa;
+    const bool zend = zero_ends && t.L.seg == 0 && (t.a == 0 || t.a == t.s.nax - 1);
+    for (int k0 = 0; k0 < K; k0 += kTofGroup) {
+      float d[kTofGroup];
+      bool any = false;
+#pragma unroll
+      for (int kk = 0; kk < kTofGroup; ++kk) {
+        d[kk] = 0.f;
+        if (t.act && !zend && k0 + kk < K)
+          d[kk] = pd ? __ldg(pd + t.s.out_base + static_cast<int64_t>(k0 + kk) * p.tof_stride + t.a) : 1.f;
+        any |= d[kk] != 0.f;
+      }
+      if (!__any_sync(0xffffffffu, any)) continue;
+      for (int e0 = 0; e0 < pb.row_len; e0 += 32) {
+        const int cnt = min(32, pb.row_len - e0);
+        tof_stage_batch(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
+        if (any)
+          for (int k = 0; k < cnt; ++k) {
+            const int2 X = S.xs[gi][k];
+            const int zz = X.y + zoff;
+            if (zz < 0 || zz >= p.nz) continue;
+            typename Sum::T sum = 0;
+#pragma unroll
+            for (int q = 0; q < kTofGroup / 4; ++q) {
+              const float4 w = S.w[k][q];
+              // zero bins and zero weights contribute nothing, as in the per-timing-bin back projection
+              if (d[4 * q] != 0.f && w.x != 0.f) sum += out.term(w.x * d[4 * q]);
+              if (d[4 * q + 1] != 0.f && w.y != 0.f) sum += out.term(w.y * d[4 * q + 1]);
+              if (d[4 * q + 2] != 0.f && w.z != 0.f) sum += out.term(w.z * d[4 * q + 2]);
+              if (d[4 * q + 3] != 0.f && w.w != 0.f) sum += out.term(w.w * d[4 * q + 3]);
+            }
+            out.flush(X.x + zz, sum);
+          }
+      }
+    }
+  }
+}
+
+template <typename Sum>
+__global__ void __launch_bounds__(kTofWarps * 32) back_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
+                                                                         int nitems, const float* __restrict__ pd,
+                                                                         Sum out, const double* __restrict__ scale,
+                                                                         int zero_ends) {
+  __shared__ TofStage stage[kTofWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * kTofWarps + warp;
+  if (bi >= nitems) return;
+  Sum o = out;
+  if constexpr (std::is_same<Sum, TofFixedSum>::value) o.scale = *scale;
+  back_tof_grouped_body<Sum>(p, p.tof_basic[items[bi]], stage[warp], pd, o, zero_ends, lane);
+}
+
 // Batched packed kernels: a persistent grid whose warps take (frame, basic bin) items from the queue one at a time
 // and project them as forward_packed_bin / back_packed_bin; each warp stages its item's frame, geometry and bin.
 struct WarpStage {
@@ -594,7 +791,8 @@ struct WarpStage {
 
 __device__ __forceinline__ bool next_item_warp(unsigned* counter, const BatchItem* __restrict__ items, int nitems,
                                                const ProjParams* __restrict__ geoms,
-                                               const BatchFrameDev* __restrict__ frames, WarpStage& st, int lane) {
+                                               const BatchFrameDev* __restrict__ frames, WarpStage& st, int lane,
+                                               bool tof_basic = false) {
   __syncwarp();  // the warp has finished with the previous item
   int it = 0;
   if (lane == 0) it = static_cast<int>(atomicAdd(counter, 1u));
@@ -610,7 +808,7 @@ __device__ __forceinline__ bool next_item_warp(unsigned* counter, const BatchIte
       reinterpret_cast<uint32_t*>(&st.p)[t - nf] = reinterpret_cast<const uint32_t*>(geoms + g)[t - nf];
     else
       reinterpret_cast<uint32_t*>(&st.pb)[t - nf - np] =
-          reinterpret_cast<const uint32_t*>(geoms[g].bins + wi.bin)[t - nf - np];
+          reinterpret_cast<const uint32_t*>((tof_basic ? geoms[g].tof_basic : geoms[g].bins) + wi.bin)[t - nf - np];
   }
   __syncwarp();
   return true;
@@ -643,6 +841,38 @@ __global__ void __launch_bounds__(kPackedWarps * 32) back_batch_packed_kernel(co
   WarpStage& st = wst[warp];
   while (next_item_warp(counter, items, nitems, geoms, frames, st, lane))
     back_packed_bin<FloatAcc>(st.p, st.pb, stage[warp], st.f.ratio, FloatAcc{st.f.u}, 0, lane);
+}
+
+// batched TOF-grouped kernels: items are (frame, basic bin) over the frames' TOF basic-bin tables
+__global__ void __launch_bounds__(kTofWarps * 32) forward_batch_tof_kernel(const ProjParams* __restrict__ geoms,
+                                                                          const BatchFrameDev* __restrict__ frames,
+                                                                          const BatchItem* __restrict__ items, int nitems,
+                                                                          unsigned* counter) {
+  __shared__ WarpStage wst[kTofWarps];
+  __shared__ TofStage stage[kTofWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpStage& st = wst[warp];
+  while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {
+    double ll = 0.0;
+    unsigned ncancel = 0;
+    forward_tof_grouped_body<kEpiRatio>(st.p, st.pb, stage[warp], st.f.x, st.f.ratio, st.f.ep, ll, ncancel, lane);
+    for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
+    if (lane == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
+  }
+}
+
+__global__ void __launch_bounds__(kTofWarps * 32) back_batch_tof_kernel(const ProjParams* __restrict__ geoms,
+                                                                       const BatchFrameDev* __restrict__ frames,
+                                                                       const BatchItem* __restrict__ items, int nitems,
+                                                                       unsigned* counter) {
+  __shared__ WarpStage wst[kTofWarps];
+  __shared__ TofStage stage[kTofWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpStage& st = wst[warp];
+  while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {
+    back_tof_grouped_body<TofFloatSum>(st.p, st.pb, stage[warp], st.f.ratio, TofFloatSum{st.f.u}, 0, lane);
+    __syncwarp();
+  }
 }
 
 static size_t proj_smem_bytes(const ProjParams& p) { return proj_smem_bytes(p.max_row_len); }
@@ -767,6 +997,58 @@ int batch_packed_max_ctas_per_sm(bool forward) {
                            : reinterpret_cast<const void*>(back_batch_packed_kernel);
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kPackedWarps * 32, 0) != cudaSuccess) return 0;
+  return n;
+}
+
+cudaError_t launch_forward_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* image,
+                                       float* projdata, cudaStream_t st, const FwdEpilogue* ep) {
+  if (nitems <= 0) return cudaSuccess;
+  const int grid = (nitems + kTofWarps - 1) / kTofWarps;
+  FwdEpilogue none{};
+  if (!ep || ep->mode == kEpiNone)
+    forward_tof_grouped_kernel<kEpiNone><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, none);
+  else if (ep->mode == kEpiRatio)
+    forward_tof_grouped_kernel<kEpiRatio><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, *ep);
+  else if (ep->mode == kEpiGradient)
+    forward_tof_grouped_kernel<kEpiGradient><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, *ep);
+  else
+    return cudaErrorInvalidValue;  // the log-likelihood keeps one partial per timing bin: per-bin kernels
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* projdata,
+                                    float* image, unsigned long long* acc, const double* scale, cudaStream_t st,
+                                    int zero_ends) {
+  if (nitems <= 0) return cudaSuccess;
+  const int grid = (nitems + kTofWarps - 1) / kTofWarps;
+  if (acc)
+    back_tof_grouped_kernel<TofFixedSum><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, projdata,
+                                                                          TofFixedSum{acc, 0.0}, scale, zero_ends);
+  else
+    back_tof_grouped_kernel<TofFloatSum><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, projdata,
+                                                                          TofFloatSum{image}, scale, zero_ends);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_forward_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                     int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  forward_batch_tof_kernel<<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_back_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
+                                  int nitems, unsigned* counter, int grid, cudaStream_t st) {
+  if (nitems <= 0) return cudaSuccess;
+  back_batch_tof_kernel<<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  return cudaGetLastError();
+}
+
+int batch_tof_max_ctas_per_sm(bool forward) {
+  const void* fn = forward ? reinterpret_cast<const void*>(forward_batch_tof_kernel)
+                           : reinterpret_cast<const void*>(back_batch_tof_kernel);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTofWarps * 32, 0) != cudaSuccess) return 0;
   return n;
 }
 

@@ -339,7 +339,40 @@ __global__ void tof_rows_kernel(const RowElem* __restrict__ src, const TofJobDev
   if (!out) counts[j] = n;
 }
 
+// one thread per (basic bin, timing bin): the weight of every element of the non-TOF row for this timing bin,
+// w[(src_offset + e) * ntof + tof_index] = the TOF row's value (e.v * kernel value), 0 where the TOF row has no
+// element (the same arithmetic as tof_rows_kernel, so the weights equal the TOF rows' values)
+__global__ void tof_weights_kernel(const RowElem* __restrict__ src, const TofJobDev* __restrict__ jobs, int njobs,
+                                   TofParams tp, int ntof, float* __restrict__ w) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  const TofJobDev job = jobs[j];
+  const float low = tp.low[job.tof_index], high = tp.high[job.tof_index];
+  for (int k = 0; k < job.src_len; ++k) {
+    const RowElem e = src[job.src_offset + k];
+    int z, y, x;
+    unpack_zyx(e.zyx, z, y, x);
+    const float pz = (static_cast<float>(z) * tp.vox[0] + tp.origin[0]) - tp.scanner_z_offset;
+    const float py = (static_cast<float>(y) * tp.vox[1] + tp.origin[1]) - 0.0f;
+    const float px = (static_cast<float>(x) * tp.vox[2] + tp.origin[2]) - 0.0f;
+    float ip = 0.f;
+    ip = ip + (pz - job.mid[0]) * job.unit[0];
+    ip = ip + (py - job.mid[1]) * job.unit[1];
+    ip = ip + (px - job.mid[2]) * job.unit[2];
+    const float d2 = -ip;
+    const float kv = tof_value(tp, low - d2, high - d2);
+    w[(job.src_offset + k) * ntof + job.tof_index] = (kv > 0 && e.v != 0) ? e.v * kv : 0.f;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_tof_weights(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp, int ntof,
+                               float* w, cudaStream_t st) {
+  if (njobs <= 0) return cudaSuccess;
+  tof_weights_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(src, jobs, njobs, tp, ntof, w);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_tof_rows(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp,
                             const int64_t* out_offsets, RowElem* out, int* counts, cudaStream_t st) {

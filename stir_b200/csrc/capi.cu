@@ -1916,6 +1916,7 @@ struct b200rt_batch {
   DevBuf<b200::PathParams> d_pgeoms;
   bool paths = false;  // every frame's projector has path items: the column-staged batched kernels
   bool tof_grouped = false;  // otherwise, TOF frames with the timing bins of a basic bin grouped: TOF kernels
+  int num_tof = 1;
   bool packed = false;  // otherwise, every segment of every frame has few axial positions: the packed kernels
   int smem_f = 0, smem_b = 0;
   DevBuf<b200::BatchFrameDev> d_frames;
@@ -1967,7 +1968,9 @@ void batch_finalize(b200rt_batch& b) {
   b.paths = true;
   for (auto* h : b.geoms) b.paths = b.paths && h->use_paths;
   b.tof_grouped = !b.paths;
-  for (auto* h : b.geoms) b.tof_grouped = b.tof_grouped && h->params.tof_w != nullptr;
+  b.num_tof = b.geoms.empty() ? 1 : b.geoms[0]->params.num_tof;
+  for (auto* h : b.geoms)  // one timing-bin count for the whole batch (the kernels' group size)
+    b.tof_grouped = b.tof_grouped && h->params.tof_w != nullptr && h->params.num_tof == b.num_tof;
   b.packed = !b.paths && !b.tof_grouped;
   for (auto* h : b.geoms) b.packed = b.packed && h->params.max_nax <= b200::kPackedMaxNax;
   if (b.paths) {
@@ -2022,8 +2025,8 @@ void batch_finalize(b200rt_batch& b) {
     b.max_fwd = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
     b.max_back = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
   } else if (b.tof_grouped) {
-    b.max_fwd = b200::batch_tof_max_ctas_per_sm(true);
-    b.max_back = b200::batch_tof_max_ctas_per_sm(false);
+    b.max_fwd = b200::batch_tof_max_ctas_per_sm(b.num_tof, true);
+    b.max_back = b200::batch_tof_max_ctas_per_sm(b.num_tof, false);
   } else if (b.packed) {
     b.max_fwd = b200::batch_packed_max_ctas_per_sm(true);
     b.max_back = b200::batch_packed_max_ctas_per_sm(false);
@@ -2125,8 +2128,10 @@ cudaError_t batch_launch(b200rt_batch& b, int dir, const BatchItem* items, int n
                     : b200::launch_back_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.smem_b, b.d_frames.p, items, n,
                                                     b.counters.p + 1, grid, st);
   if (b.tof_grouped)
-    return dir == 0 ? b200::launch_forward_batch_tof(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
-                    : b200::launch_back_batch_tof(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);
+    return dir == 0 ? b200::launch_forward_batch_tof(b.d_geoms.p, b.num_tof, b.d_frames.p, items, n, b.counters.p, grid,
+                                                     st)
+                    : b200::launch_back_batch_tof(b.d_geoms.p, b.num_tof, b.d_frames.p, items, n, b.counters.p + 1,
+                                                  grid, st);
   if (b.packed)
     return dir == 0 ? b200::launch_forward_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
                     : b200::launch_back_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);

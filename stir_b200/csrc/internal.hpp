@@ -306,11 +306,11 @@ cudaError_t launch_back_batch_packed(const ProjParams* geoms, const BatchFrameDe
                                      int nitems, unsigned* counter, int grid, cudaStream_t st);
 int batch_packed_max_ctas_per_sm(bool forward);
 // batched TOF-grouped kernels (TOF frames of packed geometries): items are (frame, basic bin of the TOF table)
-cudaError_t launch_forward_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
-                                     int nitems, unsigned* counter, int grid, cudaStream_t st);
-cudaError_t launch_back_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
-                                  int nitems, unsigned* counter, int grid, cudaStream_t st);
-int batch_tof_max_ctas_per_sm(bool forward);
+cudaError_t launch_forward_batch_tof(const ProjParams* geoms, int num_tof, const BatchFrameDev* frames,
+                                     const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st);
+cudaError_t launch_back_batch_tof(const ProjParams* geoms, int num_tof, const BatchFrameDev* frames,
+                                  const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st);
+int batch_tof_max_ctas_per_sm(int num_tof, bool forward);
 int batch_max_ctas_per_sm(int npa, size_t smem_bytes, bool forward);
 // dynamic shared memory of the projection kernels for a row length bound
 size_t proj_smem_bytes(int max_row_len);

@@ -326,17 +326,6 @@ __device__ __forceinline__ PackedLane packed_lane(const ProjParams& p, const Pro
   return t;
 }
 
-// the image index of element (zyx) for this lane's line and axial position, or -1 outside [0, nz)
-__device__ __forceinline__ int packed_voxel(const ProjParams& p, const PackedLane& t, uint32_t zyx) {
-  int z, y, x;
-  unpack_zyx(zyx, z, y, x);
-  const int xt = (t.swap ? y : x) * t.sx;
-  const int yt = (t.swap ? x : y) * t.sy;
-  const int zz = (t.zq ? t.q - z : z) + t.zoff;
-  if (zz < 0 || zz >= p.nz) return -1;
-  return ((yt - p.min_y) * p.nx + (xt - p.min_x)) * p.nz + zz;
-}
-
 // nax of the basic bin's lines (a basic bin's related lines all have segments +-s)
 __device__ __forceinline__ int packed_nax(const ProjParams& p, const ProjBinDev& pb) {
   return p.segs[p.lines[pb.first_line].seg + p.S].nax;
@@ -589,20 +578,21 @@ size_t proj_smem_bytes(int max_row_len) {
 // ---- TOF-grouped packed kernels ------------------------------------------------
 // With TOF, every timing bin of a basic bin has its own row: the basic row's elements weighted by the timing
 // bin's kernel.  Here a warp takes a basic bin with all its timing bins: it walks the non-TOF row once per group of
-// kTofGroup timing bins, gathers each voxel once, and applies the group's weights (staged per batch of 32
+// KG timing bins, gathers each voxel once, and applies the group's weights (staged per batch of 32
 // elements in shared memory) from registers.  Forward: each (line, axial position, timing bin) sum adds the same
 // products in the same order as the TOF row (elements outside the TOF row have weight 0 and add +-0), so the
 // results are bit-identical.  Back: the contributions of the group's timing bins to a voxel are summed before the
 // one atomic (float), or rounded one by one and summed as integers (fixed point: the same integers).
 constexpr int kTofWarps = 4;
-constexpr int kTofGroup = 16;
+constexpr int kTofGroupMax = 32;  // timing bins per pass: KG in {8, 16, 20, 24, 32}, chosen from their number
 struct TofStage {
   int2 xs[kPackedMaxLines][33];
-  float4 w[32][kTofGroup / 4];
+  float4 w[32][kTofGroupMax / 4];
 };
 
 // transforms and weights of elements [e0, e0 + cnt) of the basic row for the lines l0.. (ng of them) and the
-// timing bins [k0, k0 + kTofGroup)
+// timing bins [k0, k0 + KG)
+template <int KG>
 __device__ __forceinline__ void tof_stage_batch(const ProjParams& p, const ProjBinDev& pb, const RowElem* row,
                                                 const float* wrow, int K, int l0, int ng, int e0, int cnt, int k0,
                                                 TofStage& S, int lane) {
@@ -623,14 +613,14 @@ __device__ __forceinline__ void tof_stage_batch(const ProjParams& p, const ProjB
   // weights: the batch's elements x timing bins are contiguous ([element][timing bin]); coalesced loads
   float* sw = reinterpret_cast<float*>(S.w);
   const float* src = wrow + static_cast<int64_t>(e0) * K;
-  for (int i = lane; i < 32 * kTofGroup; i += 32) {
-    const int e = i / kTofGroup, kk = i % kTofGroup;
-    sw[i] = (e < cnt && k0 + kk < K) ? __ldg(src + static_cast<int64_t>(e) * K + k0 + kk) : 0.f;
+  for (int i = lane; i < 32 * KG; i += 32) {
+    const int e = i / KG, kk = i % KG;
+    sw[e * kTofGroupMax + kk] = (e < cnt && k0 + kk < K) ? __ldg(src + static_cast<int64_t>(e) * K + k0 + kk) : 0.f;
   }
   __syncwarp();
 }
 
-template <int EPI>
+template <int KG, int EPI>
 __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
                                                          const float* __restrict__ img, float* __restrict__ out,
                                                          const FwdEpilogue& ep, double& ll, unsigned& ncancel,
@@ -645,13 +635,13 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
     const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
     const int ng = min(G, pb.num_lines - l0);
     const int zoff = t.a * t.s.npa;
-    for (int k0 = 0; k0 < K; k0 += kTofGroup) {
-      float acc[kTofGroup];
+    for (int k0 = 0; k0 < K; k0 += KG) {
+      float acc[KG];
 #pragma unroll
-      for (int kk = 0; kk < kTofGroup; ++kk) acc[kk] = 0.f;
+      for (int kk = 0; kk < KG; ++kk) acc[kk] = 0.f;
       for (int e0 = 0; e0 < pb.row_len; e0 += 32) {
         const int cnt = min(32, pb.row_len - e0);
-        tof_stage_batch(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
+        tof_stage_batch<KG>(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
         if (t.act)
           for (int k = 0; k < cnt; ++k) {
             const int2 X = S.xs[gi][k];
@@ -659,7 +649,7 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
             if (zz < 0 || zz >= p.nz) continue;
             const float xv = __ldg(img + X.x + zz);
 #pragma unroll
-            for (int q = 0; q < kTofGroup / 4; ++q) {
+            for (int q = 0; q < KG / 4; ++q) {
               const float4 w = S.w[k][q];
               acc[4 * q] += xv * w.x;
               acc[4 * q + 1] += xv * w.y;
@@ -670,7 +660,7 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
       }
       if (t.act)
 #pragma unroll
-        for (int kk = 0; kk < kTofGroup; ++kk)
+        for (int kk = 0; kk < KG; ++kk)
           if (k0 + kk < K)
             forward_store<EPI>(p, t.L.seg, t.L.view, k0 + kk, t.s.nax,
                                t.s.out_base + static_cast<int64_t>(k0 + kk) * p.tof_stride + t.a, t.a, acc[kk], out, ep,
@@ -680,7 +670,7 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
   __syncwarp();
 }
 
-template <int EPI>
+template <int KG, int EPI>
 __global__ void __launch_bounds__(kTofWarps * 32) forward_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
                                                                             int nitems, const float* __restrict__ img,
                                                                             float* __restrict__ out, FwdEpilogue ep) {
@@ -690,7 +680,7 @@ __global__ void __launch_bounds__(kTofWarps * 32) forward_tof_grouped_kernel(Pro
   if (bi >= nitems) return;
   double ll = 0.0;
   unsigned ncancel = 0;
-  forward_tof_grouped_body<EPI>(p, p.tof_basic[items[bi]], stage[warp], img, out, ep, ll, ncancel, lane);
+  forward_tof_grouped_body<KG, EPI>(p, p.tof_basic[items[bi]], stage[warp], img, out, ep, ll, ncancel, lane);
   if (EPI == kEpiRatio || EPI == kEpiGradient) {
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
@@ -716,7 +706,7 @@ struct TofFixedSum {
   }
 };
 
-template <typename Sum>
+template <int KG, typename Sum>
 __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
                                                       const float* __restrict__ pd, const Sum& out, int zero_ends,
                                                       int lane) {
@@ -731,11 +721,11 @@ __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const
     const int ng = min(G, pb.num_lines - l0);
     const int zoff = t.a * t.s.npa;
     const bool zend = zero_ends && t.L.seg == 0 && (t.a == 0 || t.a == t.s.nax - 1);
-    for (int k0 = 0; k0 < K; k0 += kTofGroup) {
-      float d[kTofGroup];
+    for (int k0 = 0; k0 < K; k0 += KG) {
+      float d[KG];
       bool any = false;
 #pragma unroll
-      for (int kk = 0; kk < kTofGroup; ++kk) {
+      for (int kk = 0; kk < KG; ++kk) {
         d[kk] = 0.f;
         if (t.act && !zend && k0 + kk < K)
           d[kk] = pd ? __ldg(pd + t.s.out_base + static_cast<int64_t>(k0 + kk) * p.tof_stride + t.a) : 1.f;
@@ -744,21 +734,21 @@ __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const
       if (!__any_sync(0xffffffffu, any)) continue;
       for (int e0 = 0; e0 < pb.row_len; e0 += 32) {
         const int cnt = min(32, pb.row_len - e0);
-        tof_stage_batch(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
+        tof_stage_batch<KG>(p, pb, row, wrow, K, l0, ng, e0, cnt, k0, S, lane);
         if (any)
           for (int k = 0; k < cnt; ++k) {
             const int2 X = S.xs[gi][k];
             const int zz = X.y + zoff;
             if (zz < 0 || zz >= p.nz) continue;
+            // zero bins and zero weights add 0: the same sum as the per-timing-bin back projection's terms
             typename Sum::T sum = 0;
 #pragma unroll
-            for (int q = 0; q < kTofGroup / 4; ++q) {
+            for (int q = 0; q < KG / 4; ++q) {
               const float4 w = S.w[k][q];
-              // zero bins and zero weights contribute nothing, as in the per-timing-bin back projection
-              if (d[4 * q] != 0.f && w.x != 0.f) sum += out.term(w.x * d[4 * q]);
-              if (d[4 * q + 1] != 0.f && w.y != 0.f) sum += out.term(w.y * d[4 * q + 1]);
-              if (d[4 * q + 2] != 0.f && w.z != 0.f) sum += out.term(w.z * d[4 * q + 2]);
-              if (d[4 * q + 3] != 0.f && w.w != 0.f) sum += out.term(w.w * d[4 * q + 3]);
+              sum += out.term(w.x * d[4 * q]);
+              sum += out.term(w.y * d[4 * q + 1]);
+              sum += out.term(w.z * d[4 * q + 2]);
+              sum += out.term(w.w * d[4 * q + 3]);
             }
             out.flush(X.x + zz, sum);
           }
@@ -767,7 +757,7 @@ __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const
   }
 }
 
-template <typename Sum>
+template <int KG, typename Sum>
 __global__ void __launch_bounds__(kTofWarps * 32) back_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
                                                                          int nitems, const float* __restrict__ pd,
                                                                          Sum out, const double* __restrict__ scale,
@@ -778,7 +768,7 @@ __global__ void __launch_bounds__(kTofWarps * 32) back_tof_grouped_kernel(ProjPa
   if (bi >= nitems) return;
   Sum o = out;
   if constexpr (std::is_same<Sum, TofFixedSum>::value) o.scale = *scale;
-  back_tof_grouped_body<Sum>(p, p.tof_basic[items[bi]], stage[warp], pd, o, zero_ends, lane);
+  back_tof_grouped_body<KG, Sum>(p, p.tof_basic[items[bi]], stage[warp], pd, o, zero_ends, lane);
 }
 
 // Batched packed kernels: a persistent grid whose warps take (frame, basic bin) items from the queue one at a time
@@ -844,6 +834,7 @@ __global__ void __launch_bounds__(kPackedWarps * 32) back_batch_packed_kernel(co
 }
 
 // batched TOF-grouped kernels: items are (frame, basic bin) over the frames' TOF basic-bin tables
+template <int KG>
 __global__ void __launch_bounds__(kTofWarps * 32) forward_batch_tof_kernel(const ProjParams* __restrict__ geoms,
                                                                           const BatchFrameDev* __restrict__ frames,
                                                                           const BatchItem* __restrict__ items, int nitems,
@@ -855,12 +846,13 @@ __global__ void __launch_bounds__(kTofWarps * 32) forward_batch_tof_kernel(const
   while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {
     double ll = 0.0;
     unsigned ncancel = 0;
-    forward_tof_grouped_body<kEpiRatio>(st.p, st.pb, stage[warp], st.f.x, st.f.ratio, st.f.ep, ll, ncancel, lane);
+    forward_tof_grouped_body<KG, kEpiRatio>(st.p, st.pb, stage[warp], st.f.x, st.f.ratio, st.f.ep, ll, ncancel, lane);
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if (lane == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
   }
 }
 
+template <int KG>
 __global__ void __launch_bounds__(kTofWarps * 32) back_batch_tof_kernel(const ProjParams* __restrict__ geoms,
                                                                        const BatchFrameDev* __restrict__ frames,
                                                                        const BatchItem* __restrict__ items, int nitems,
@@ -870,7 +862,7 @@ __global__ void __launch_bounds__(kTofWarps * 32) back_batch_tof_kernel(const Pr
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpStage& st = wst[warp];
   while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {
-    back_tof_grouped_body<TofFloatSum>(st.p, st.pb, stage[warp], st.f.ratio, TofFloatSum{st.f.u}, 0, lane);
+    back_tof_grouped_body<KG, TofFloatSum>(st.p, st.pb, stage[warp], st.f.ratio, TofFloatSum{st.f.u}, 0, lane);
     __syncwarp();
   }
 }
@@ -1000,19 +992,39 @@ int batch_packed_max_ctas_per_sm(bool forward) {
   return n;
 }
 
+// timing bins per pass: the fewest passes of at most 32 bins, spread evenly, rounded up to an instantiated size
+int tof_group_size(int K) {
+  const int passes = (K + kTofGroupMax - 1) / kTofGroupMax;
+  const int per = (K + passes - 1) / passes;
+  return per <= 8 ? 8 : per <= 16 ? 16 : per <= 20 ? 20 : per <= 24 ? 24 : 32;
+}
+
+#define TOF_KG_SWITCH(K, CALL)                       \
+  switch (tof_group_size(K)) {                       \
+    case 8: { constexpr int KG = 8; CALL; break; }   \
+    case 16: { constexpr int KG = 16; CALL; break; } \
+    case 20: { constexpr int KG = 20; CALL; break; } \
+    case 24: { constexpr int KG = 24; CALL; break; } \
+    default: { constexpr int KG = 32; CALL; break; } \
+  }
+
 cudaError_t launch_forward_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* image,
                                        float* projdata, cudaStream_t st, const FwdEpilogue* ep) {
   if (nitems <= 0) return cudaSuccess;
   const int grid = (nitems + kTofWarps - 1) / kTofWarps;
   FwdEpilogue none{};
-  if (!ep || ep->mode == kEpiNone)
-    forward_tof_grouped_kernel<kEpiNone><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, none);
-  else if (ep->mode == kEpiRatio)
-    forward_tof_grouped_kernel<kEpiRatio><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, *ep);
-  else if (ep->mode == kEpiGradient)
-    forward_tof_grouped_kernel<kEpiGradient><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, image, projdata, *ep);
-  else
+  if (!ep || ep->mode == kEpiNone) {
+    TOF_KG_SWITCH(p.num_tof, (forward_tof_grouped_kernel<KG, kEpiNone><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, image, projdata, none)));
+  } else if (ep->mode == kEpiRatio) {
+    TOF_KG_SWITCH(p.num_tof, (forward_tof_grouped_kernel<KG, kEpiRatio><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, image, projdata, *ep)));
+  } else if (ep->mode == kEpiGradient) {
+    TOF_KG_SWITCH(p.num_tof, (forward_tof_grouped_kernel<KG, kEpiGradient><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, image, projdata, *ep)));
+  } else {
     return cudaErrorInvalidValue;  // the log-likelihood keeps one partial per timing bin: per-bin kernels
+  }
   return cudaGetLastError();
 }
 
@@ -1021,32 +1033,36 @@ cudaError_t launch_back_tof_grouped(const ProjParams& p, const int* items, int n
                                     int zero_ends) {
   if (nitems <= 0) return cudaSuccess;
   const int grid = (nitems + kTofWarps - 1) / kTofWarps;
-  if (acc)
-    back_tof_grouped_kernel<TofFixedSum><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, projdata,
-                                                                          TofFixedSum{acc, 0.0}, scale, zero_ends);
-  else
-    back_tof_grouped_kernel<TofFloatSum><<<grid, kTofWarps * 32, 0, st>>>(p, items, nitems, projdata,
-                                                                          TofFloatSum{image}, scale, zero_ends);
+  if (acc) {
+    TOF_KG_SWITCH(p.num_tof, (back_tof_grouped_kernel<KG, TofFixedSum><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, projdata, TofFixedSum{acc, 0.0}, scale, zero_ends)));
+  } else {
+    TOF_KG_SWITCH(p.num_tof, (back_tof_grouped_kernel<KG, TofFloatSum><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, projdata, TofFloatSum{image}, scale, zero_ends)));
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
-                                     int nitems, unsigned* counter, int grid, cudaStream_t st) {
+cudaError_t launch_forward_batch_tof(const ProjParams* geoms, int num_tof, const BatchFrameDev* frames,
+                                     const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  forward_batch_tof_kernel<<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  TOF_KG_SWITCH(num_tof, (forward_batch_tof_kernel<KG><<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems,
+                                                                                        counter)));
   return cudaGetLastError();
 }
 
-cudaError_t launch_back_batch_tof(const ProjParams* geoms, const BatchFrameDev* frames, const BatchItem* items,
-                                  int nitems, unsigned* counter, int grid, cudaStream_t st) {
+cudaError_t launch_back_batch_tof(const ProjParams* geoms, int num_tof, const BatchFrameDev* frames,
+                                  const BatchItem* items, int nitems, unsigned* counter, int grid, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  back_batch_tof_kernel<<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems, counter);
+  TOF_KG_SWITCH(num_tof, (back_batch_tof_kernel<KG><<<grid, kTofWarps * 32, 0, st>>>(geoms, frames, items, nitems,
+                                                                                     counter)));
   return cudaGetLastError();
 }
 
-int batch_tof_max_ctas_per_sm(bool forward) {
-  const void* fn = forward ? reinterpret_cast<const void*>(forward_batch_tof_kernel)
-                           : reinterpret_cast<const void*>(back_batch_tof_kernel);
+int batch_tof_max_ctas_per_sm(int num_tof, bool forward) {
+  const void* fn = nullptr;
+  TOF_KG_SWITCH(num_tof, (fn = forward ? reinterpret_cast<const void*>(forward_batch_tof_kernel<KG>)
+                                       : reinterpret_cast<const void*>(back_batch_tof_kernel<KG>)));
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kTofWarps * 32, 0) != cudaSuccess) return 0;
   return n;

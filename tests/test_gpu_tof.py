@@ -92,3 +92,19 @@ def test_tof_33_bins_grouped_kernels(cuda_device, oracle_lib):
     assert torch.equal(a, b)
     assert float((a - c).norm() / c.norm()) < 1e-6
     proj.close()
+
+
+@pytest.mark.parametrize("ntof", [13, 23, 29])
+def test_tof_group_sizes(cuda_device, oracle_lib, ntof):
+    """Timing-bin counts that select the other group sizes of the grouped kernels (16, 24 and 32 bins per pass)."""
+    from stir_b200.projectors import RayTracingProjector
+    pdi, img = G.tof_small_3d_pet(num_tof_bins=ntof, timing_bin_ps=1650.0 / ntof, num_views=48)  # 1650 ps in all
+    proj = RayTracingProjector(pdi, img, device=cuda_device)
+    orc = oracle_lib.Oracle(proj.geometry)
+    assert proj.info.num_tof_bins == ntof
+    sub = (2, 6)
+    x = np.random.default_rng(7).uniform(0, 1, img.shape).astype(np.float32)
+    assert rel_l2(proj.forward_host(x, *sub), orc.forward(x, *sub)) <= 1e-5
+    y = np.random.default_rng(8).uniform(0, 1, proj.projdata_size).astype(np.float32)
+    assert rel_l2(proj.back_host(y, *sub), orc.back(y, *sub)) <= 1e-5
+    proj.close()

@@ -16,6 +16,10 @@
 //          ProjMatrixElemsForOneBin::forward_project (ProjMatrixElemsForOneBin.cxx:354-370).
 // Back:    image[col_k][z_k + npa*a] += w_k * projdata[line][a] for projdata != 0
 //          (ProjMatrixElemsForOneBin::back_project, :333-351), with float atomics.
+//
+// Lines with at most 16 axial positions (small scanners, TOF data) use the packed kernels below instead (a warp
+// per basic bin, lanes = (line, axial position)); with TOF, the TOF-grouped kernels project all timing bins of a
+// basic bin from its non-TOF row in one warp.
 #include <type_traits>
 
 #include "internal.hpp"

@@ -58,38 +58,47 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region: one nvidia-smi process streaming
+    a sample every 50 ms (-lms) from just before the region until its end."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, interval_ms: int = 50):
         self.idx = device_index
+        self.interval_ms = interval_ms
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._th = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5).stdout
-                for line in out.strip().splitlines():
-                    self.samples.append([c.strip() for c in line.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) >= 9:
+                self.samples.append(cols)
 
     def __enter__(self):
-        self._th = threading.Thread(target=self._run, daemon=True)
-        self._th.start()
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                           "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._th = threading.Thread(target=self._read, daemon=True)
+            self._th.start()
+            time.sleep(0.15)  # the first sample precedes the timed region
+        except OSError:
+            self._proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
         if self._th:
-            self._th.join(timeout=10)
+            self._th.join(timeout=5)
 
     def summary(self):
         if not self.samples:

@@ -832,7 +832,7 @@ void forward_subset(b200rt_projector& h, const float* image, float* out, int sub
   if (h.use_paths && (!ep || ep->mode != kEpiLoglik)) {
     const int* list = path_list(h, subset, nsub, n);
     ck(launch_forward_paths(h.params, h.pparams, list, n, image, out, st, ep), "forward projection");
-  } else if (h.params.tof_w && (!ep || ep->mode != kEpiLoglik)) {
+  } else if (h.params.tof_w && (!ep || ep->mode != kEpiLoglik)) {  // log-likelihood partials: see its entry point
     const int* list = tof_group_list(h, subset, nsub, n);
     ck(launch_forward_tof_grouped(h.params, list, n, image, out, st, ep), "forward projection");
   } else {
@@ -1496,7 +1496,10 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     int n = 0, nv = 0;
     // one partial sum per CTA: per path item with the column-staged kernel, else per basic bin
-    const int* list = h->use_paths ? path_list(*h, subset_num, num_subsets, n) : subset_list(*h, subset_num, num_subsets, n);
+    const bool grouped = !h->use_paths && h->params.tof_w;  // one partial per basic bin with all timing bins
+    const int* list = h->use_paths ? path_list(*h, subset_num, num_subsets, n)
+                      : grouped    ? tof_group_list(*h, subset_num, num_subsets, n)
+                                   : subset_list(*h, subset_num, num_subsets, n);
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
     h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
     if (h->ll_partials.n < static_cast<size_t>(std::max(n, 1))) h->ll_partials.alloc(std::max(n, 1));
@@ -1514,6 +1517,8 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     ep.partials = h->ll_partials.p;
     if (h->use_paths)
       ck(launch_forward_paths(h->params, h->pparams, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
+    else if (grouped)
+      ck(launch_forward_tof_grouped(h->params, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
     else
       ck(launch_forward(h->params, list, n, image_dev, nullptr, st, &ep), "log-likelihood");
     ck(launch_reduce_sum(h->ll_partials.p, n, h->ll_sum.p, st), "reduce");

@@ -443,8 +443,8 @@ struct TofParams {
 };
 cudaError_t launch_tof_weights(const RowElem* src, const TofJobDev* jobs, int njobs, const TofParams& tp, int ntof,
                                float* w, cudaStream_t st);
-// TOF-grouped packed projections over basic bins (items index ProjParams::tof_basic); forward with the
-// kEpiNone / kEpiRatio / kEpiGradient epilogues; back atomic (float) or fixed point
+// TOF-grouped packed projections over basic bins (items index ProjParams::tof_basic); forward with every epilogue
+// (kEpiLoglik: one partial per item); back atomic (float) or fixed point
 cudaError_t launch_forward_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* image,
                                        float* projdata, cudaStream_t st, const FwdEpilogue* ep);
 cudaError_t launch_back_tof_grouped(const ProjParams& p, const int* items, int nitems, const float* projdata,

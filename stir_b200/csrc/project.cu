@@ -689,6 +689,11 @@ __global__ void __launch_bounds__(kTofWarps * 32) forward_tof_grouped_kernel(Pro
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if (lane == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
   }
+  if (EPI == kEpiLoglik) {
+    // one partial per basic bin (all its timing bins), reduced in a fixed order by the caller
+    for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
+    if (lane == 0) ep.partials[bi] = ll;
+  }
 }
 
 // sum of a voxel's contributions over the group's timing bins, then one addition to the image
@@ -1027,7 +1032,8 @@ cudaError_t launch_forward_tof_grouped(const ProjParams& p, const int* items, in
     TOF_KG_SWITCH(p.num_tof, (forward_tof_grouped_kernel<KG, kEpiGradient><<<grid, kTofWarps * 32, 0, st>>>(
                                  p, items, nitems, image, projdata, *ep)));
   } else {
-    return cudaErrorInvalidValue;  // the log-likelihood keeps one partial per timing bin: per-bin kernels
+    TOF_KG_SWITCH(p.num_tof, (forward_tof_grouped_kernel<KG, kEpiLoglik><<<grid, kTofWarps * 32, 0, st>>>(
+                                 p, items, nitems, image, projdata, *ep)));
   }
   return cudaGetLastError();
 }

@@ -108,3 +108,22 @@ def test_tof_group_sizes(cuda_device, oracle_lib, ntof):
     y = np.random.default_rng(8).uniform(0, 1, proj.projdata_size).astype(np.float32)
     assert rel_l2(proj.back_host(y, *sub), orc.back(y, *sub)) <= 1e-5
     proj.close()
+
+
+def test_tof_log_likelihood_matches_oracle(tof):
+    """The TOF log-likelihood (TOF-grouped forward with the FP64 epilogue, one partial per basic bin)."""
+    import torch
+    from stir_b200.osmaposl import log_likelihood
+    pdi, img, proj, orc = tof
+    rng = np.random.default_rng(11)
+    x = rng.uniform(0.5, 1.5, img.shape).astype(np.float32)
+    ybar = orc.forward(x)
+    y = rng.poisson(ybar * 4.0).astype(np.float32) / np.float32(4.0)
+    add = np.full_like(y, np.float32(0.05 * ybar.mean()))
+    mult = rng.uniform(0.8, 1.2, y.shape).astype(np.float32)
+    dev_pd = lambda a: proj.projdata_to_device_layout(torch.from_numpy(a).cuda())
+    xd = proj.image_to_device_layout(torch.from_numpy(x).cuda())
+    for sub, nsub, zero in [(0, 1, False), (1, 4, True)]:
+        got = log_likelihood(proj, xd, dev_pd(y), dev_pd(add), dev_pd(mult), sub, nsub, zero)
+        ref = orc.log_likelihood(x, y, add, mult, sub, nsub, zero)
+        assert abs(got - ref) <= 1e-6 * abs(ref), (got, ref)

@@ -588,10 +588,12 @@ size_t proj_smem_bytes(int max_row_len) {
 // results are bit-identical.  Back: the contributions of the group's timing bins to a voxel are summed before the
 // one atomic (float), or rounded one by one and summed as integers (fixed point: the same integers).
 constexpr int kTofWarps = 4;
+constexpr int kTofMinCtas = 8;  // 64 registers: 32 warps per SM (79 registers left 24)
 constexpr int kTofGroupMax = 32;  // timing bins per pass: KG in {8, 16, 20, 24, 32}, chosen from their number
+template <int KG>
 struct TofStage {
   int2 xs[kPackedMaxLines][33];
-  float4 w[32][kTofGroupMax / 4];
+  float4 w[32][KG / 4];
 };
 
 // transforms and weights of elements [e0, e0 + cnt) of the basic row for the lines l0.. (ng of them) and the
@@ -599,7 +601,7 @@ struct TofStage {
 template <int KG>
 __device__ __forceinline__ void tof_stage_batch(const ProjParams& p, const ProjBinDev& pb, const RowElem* row,
                                                 const float* wrow, int K, int l0, int ng, int e0, int cnt, int k0,
-                                                TofStage& S, int lane) {
+                                                TofStage<KG>& S, int lane) {
   __syncwarp();
   if (lane < cnt) {
     const RowElem e = row[e0 + lane];
@@ -619,13 +621,13 @@ __device__ __forceinline__ void tof_stage_batch(const ProjParams& p, const ProjB
   const float* src = wrow + static_cast<int64_t>(e0) * K;
   for (int i = lane; i < 32 * KG; i += 32) {
     const int e = i / KG, kk = i % KG;
-    sw[e * kTofGroupMax + kk] = (e < cnt && k0 + kk < K) ? __ldg(src + static_cast<int64_t>(e) * K + k0 + kk) : 0.f;
+    sw[e * KG + kk] = (e < cnt && k0 + kk < K) ? __ldg(src + static_cast<int64_t>(e) * K + k0 + kk) : 0.f;
   }
   __syncwarp();
 }
 
 template <int KG, int EPI>
-__device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
+__device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage<KG>& S,
                                                          const float* __restrict__ img, float* __restrict__ out,
                                                          const FwdEpilogue& ep, double& ll, unsigned& ncancel,
                                                          int lane) {
@@ -675,10 +677,10 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
 }
 
 template <int KG, int EPI>
-__global__ void __launch_bounds__(kTofWarps * 32) forward_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
+__global__ void __launch_bounds__(kTofWarps * 32, kTofMinCtas) forward_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
                                                                             int nitems, const float* __restrict__ img,
                                                                             float* __restrict__ out, FwdEpilogue ep) {
-  __shared__ TofStage stage[kTofWarps];
+  __shared__ TofStage<KG> stage[kTofWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bi = blockIdx.x * kTofWarps + warp;
   if (bi >= nitems) return;
@@ -716,7 +718,7 @@ struct TofFixedSum {
 };
 
 template <int KG, typename Sum>
-__device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage& S,
+__device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const ProjBinDev& pb, TofStage<KG>& S,
                                                       const float* __restrict__ pd, const Sum& out, int zero_ends,
                                                       int lane) {
   const RowElem* row = p.tof_basic_rows + pb.row_offset;
@@ -767,11 +769,11 @@ __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const
 }
 
 template <int KG, typename Sum>
-__global__ void __launch_bounds__(kTofWarps * 32) back_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
+__global__ void __launch_bounds__(kTofWarps * 32, kTofMinCtas) back_tof_grouped_kernel(ProjParams p, const int* __restrict__ items,
                                                                          int nitems, const float* __restrict__ pd,
                                                                          Sum out, const double* __restrict__ scale,
                                                                          int zero_ends) {
-  __shared__ TofStage stage[kTofWarps];
+  __shared__ TofStage<KG> stage[kTofWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int bi = blockIdx.x * kTofWarps + warp;
   if (bi >= nitems) return;
@@ -849,7 +851,7 @@ __global__ void __launch_bounds__(kTofWarps * 32) forward_batch_tof_kernel(const
                                                                           const BatchItem* __restrict__ items, int nitems,
                                                                           unsigned* counter) {
   __shared__ WarpStage wst[kTofWarps];
-  __shared__ TofStage stage[kTofWarps];
+  __shared__ TofStage<KG> stage[kTofWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpStage& st = wst[warp];
   while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {
@@ -867,7 +869,7 @@ __global__ void __launch_bounds__(kTofWarps * 32) back_batch_tof_kernel(const Pr
                                                                        const BatchItem* __restrict__ items, int nitems,
                                                                        unsigned* counter) {
   __shared__ WarpStage wst[kTofWarps];
-  __shared__ TofStage stage[kTofWarps];
+  __shared__ TofStage<KG> stage[kTofWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpStage& st = wst[warp];
   while (next_item_warp(counter, items, nitems, geoms, frames, st, lane, true)) {

@@ -645,12 +645,14 @@ def b200_main(args):
                     "d2h_bytes_per_step": pd_bytes + img_bytes},
             "clocks": clocks.summary(),
             "gpu_launches": 2 * K}
-    if not args.no_extras:
+    # the secondary workloads and the batched reconstructions are measured on one GPU only (the scaling runs
+    # hold every GPU of the node; they report the headline alone)
+    if not args.no_extras and ws == 1:
         try:
             line.update(listmode_and_priors(proj, pdi, img, xd, cb))
         except Exception as e:  # reported, never hides the headline line
             line["listmode"] = {"error": f"{type(e).__name__}: {e}"}
-    if not args.no_batch:
+    if not args.no_batch and ws == 1:
         proj.close()
         del pd, bk, flush, y, xd
         torch.cuda.empty_cache()

@@ -640,9 +640,7 @@ void setup_projector(b200rt_projector& h) {
     std::swap(h.rows.p, tof_rows.p);
     std::swap(h.rows.n, tof_rows.n);
     total = off[njobs];
-    int max_nax = 0;
-    for (int sg = -g.S(); sg <= g.S(); ++sg) max_nax = std::max(max_nax, g.nax(sg));
-    if (max_nax <= kPackedMaxNax) {
+    {
       // keep the non-TOF rows (now in tof_rows) and the weights of every timing bin for the TOF-grouped kernels
       std::swap(h.tof_basic_rows.p, tof_rows.p);
       std::swap(h.tof_basic_rows.n, tof_rows.n);

@@ -335,6 +335,21 @@ __device__ __forceinline__ int packed_nax(const ProjParams& p, const ProjBinDev&
   return p.segs[p.lines[pb.first_line].seg + p.S].nax;
 }
 
+// the lane's (line, axial position) in the TOF-grouped kernels: packed (line groups of nax lanes) with at most
+// kPackedMaxNax axial positions, else one line at a time in blocks of 32 axial positions from a0
+__device__ __forceinline__ PackedLane tof_lane(const ProjParams& p, const ProjBinDev& pb, int l0, int G, int nax, int a0,
+                                               int lane) {
+  if (nax <= kPackedMaxNax) return packed_lane(p, pb, l0, G, nax, lane);
+  PackedLane t{};
+  t.a = a0 + lane;
+  t.act = t.a < nax && l0 < pb.num_lines;
+  if (t.act) {
+    t.L = p.lines[pb.first_line + l0];
+    t.act = setup_line(p, pb, t.L, t.s);
+  }
+  return t;
+}
+
 // The transformed elements of a batch of 32, per line of the group being projected: xs[g][k] = (image index of
 // element k under line g without its z, z after the line's z operation - min_z); lane k computes element k for
 // every line, so each transform is done once instead of once per axial position.
@@ -635,10 +650,12 @@ __device__ __forceinline__ void forward_tof_grouped_body(const ProjParams& p, co
   const int K = p.num_tof;
   const float* wrow = p.tof_w + pb.row_offset * K;
   const int nax = packed_nax(p, pb);
-  const int G = min(32 / nax, kPackedMaxLines);
-  const int gi = lane / nax;
-  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
-    const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+  const bool blocked = nax > kPackedMaxNax;
+  const int G = blocked ? 1 : min(32 / nax, kPackedMaxLines);
+  const int gi = blocked ? 0 : lane / nax;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G)
+  for (int a0 = 0; a0 < (blocked ? nax : 1); a0 += 32) {
+    const PackedLane t = tof_lane(p, pb, l0, G, nax, a0, lane);
     const int ng = min(G, pb.num_lines - l0);
     const int zoff = t.a * t.s.npa;
     for (int k0 = 0; k0 < K; k0 += KG) {
@@ -725,10 +742,12 @@ __device__ __forceinline__ void back_tof_grouped_body(const ProjParams& p, const
   const int K = p.num_tof;
   const float* wrow = p.tof_w + pb.row_offset * K;
   const int nax = packed_nax(p, pb);
-  const int G = min(32 / nax, kPackedMaxLines);
-  const int gi = lane / nax;
-  for (int l0 = 0; l0 < pb.num_lines; l0 += G) {
-    const PackedLane t = packed_lane(p, pb, l0, G, nax, lane);
+  const bool blocked = nax > kPackedMaxNax;
+  const int G = blocked ? 1 : min(32 / nax, kPackedMaxLines);
+  const int gi = blocked ? 0 : lane / nax;
+  for (int l0 = 0; l0 < pb.num_lines; l0 += G)
+  for (int a0 = 0; a0 < (blocked ? nax : 1); a0 += 32) {
+    const PackedLane t = tof_lane(p, pb, l0, G, nax, a0, lane);
     const int ng = min(G, pb.num_lines - l0);
     const int zoff = t.a * t.s.npa;
     const bool zend = zero_ends && t.L.seg == 0 && (t.a == 0 || t.a == t.s.nax - 1);

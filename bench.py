@@ -196,11 +196,18 @@ def listmode_and_priors(proj, pdi, img, xd, cpu_ref):
     bins = random_lm_bins(pdi, LM_EVENTS, rng)
     obj = LM(proj, pack_events(bins, None, np.full(LM_EVENTS, 0.1, np.float32), proj.device), has_add=True)
     g = proj.empty_image(zero=False)
+    obj.set_method(_abi.LISTMODE_PER_EVENT)
+    ms_ev = time_dev(lambda: obj.compute_sub_gradient_without_penalty(xd, 0, out=g))
+    obj.set_method(_abi.LISTMODE_AUTO)
     ms = time_dev(lambda: obj.compute_sub_gradient_without_penalty(xd, 0, out=g))
     lm = {"metric": "list-mode sub-gradient events/s", "value": LM_EVENTS / (ms / 1e3), "unit": "events/s",
-          "events": LM_EVENTS, "ms": ms, "gpu_launches": 2,
+          "events": LM_EVENTS, "ms": ms, "gpu_launches": 3,
           "workload": "10M events on uniformly drawn bins of the clinical geometry (seed 5), value 1, additive 0.1, "
-                      "one subset; one warp per event: forward, ratio, back projection"}
+                      "one subset",
+          "method": "binned (chosen automatically: events >= bins / 16): forward projection of the subset, one "
+                    "thread per event adding y / (A x + c) to its bin, back projection of the subset",
+          "per_event": {"value": LM_EVENTS / (ms_ev / 1e3), "ms": ms_ev, "gpu_launches": 1,
+                        "method": "one warp per event: the event's row gathered, ratio, row scattered"}}
     if cpu_ref is not None:
         from stir_b200.subsets import views_in_subset
         views = views_in_subset(cpu_ref.geo, cpu_ref.sub, cpu_ref.nsub, cpu_ref.orc.symmetries_used)

@@ -406,6 +406,18 @@ int b200rt_listmode_hessian_times_input_dev(b200rt_projector* h, const b200rt_lm
                                             void* stream);
 /* events skipped as outside the projection data since the last call of this function; synchronises */
 int b200rt_listmode_num_invalid(b200rt_projector* h, int64_t* count);
+/* How the three list-mode sums above visit the events' rows.
+ * PER_EVENT: one warp per event walks the event's row (a gather for A_e x, a scatter for the back projection).
+ * BINNED: the rows of all events of one bin are that bin's row, so A_e x is read from the forward projection A x
+ *   of the subset, each event's term is added to its bin of a projection-data buffer h, and A^T h is one back
+ *   projection of the subset.  The terms of one bin's events are summed before the weights multiply them, a
+ *   rounding difference only; the cancellation rules and the value's FP64 sum are those of PER_EVENT.  Costs two
+ *   (three for the Hessian) subset projections plus a few bytes per event, and three projection-data buffers.
+ * AUTO (the default): BINNED when the events number at least 1/16 of the projector's bins, else PER_EVENT. */
+#define B200RT_LISTMODE_AUTO 0
+#define B200RT_LISTMODE_PER_EVENT 1
+#define B200RT_LISTMODE_BINNED 2
+int b200rt_listmode_set_method(b200rt_projector* h, int method);
 
 /* ---- projection data streams (ProjDataFromStream) ------------------------
  * The bytes of a projection data file (from its data offset on, e.g. an Interfile ".s"), copied to the device

@@ -33,6 +33,10 @@ PRIOR_RELATIVE_DIFFERENCE = 2
 MAP_ADDITIVE = 0
 MAP_MULTIPLICATIVE = 1
 
+LISTMODE_AUTO = 0
+LISTMODE_PER_EVENT = 1
+LISTMODE_BINNED = 2
+
 
 class Geometry(ctypes.Structure):
     """b200rt_geometry"""
@@ -257,6 +261,7 @@ EXPORTS = [
     ("b200rt_listmode_value_dev", _I, [_P, _P, _I64, _P, _I, _I, _I, ctypes.POINTER(ctypes.c_double), _P]),
     ("b200rt_listmode_hessian_times_input_dev", _I, [_P, _P, _I64, _P, _P, _I, _I, _I, _P, _P]),
     ("b200rt_listmode_num_invalid", _I, [_P, ctypes.POINTER(_I64)]),
+    ("b200rt_listmode_set_method", _I, [_P, _I]),
     ("b200rt_stream_bytes", _I, [_P, ctypes.POINTER(StreamFormat), ctypes.POINTER(_I64)]),
     ("b200rt_projdata_from_stream_dev", _I, [_P, _P, _I64, ctypes.POINTER(StreamFormat), _P, _P]),
     ("b200rt_projdata_to_stream_dev", _I, [_P, _P, ctypes.POINTER(StreamFormat), _P, _I64, _P]),

@@ -334,6 +334,14 @@ cudaError_t launch_subtract(float* out, const float* s, int64_t n, cudaStream_t 
 cudaError_t launch_listmode(const ProjParams& p, const int4* table, const LmEventDev* events, int64_t n, int op,
                             const float* x, const float* rhs, int subset, int nsub, int has_add, float* out,
                             double* partial, unsigned* invalid, cudaStream_t st);
+// binned form: fwd (and fwd_rhs for op 2) = the subset's forward projections (device layout); op 0 and 2 add each
+// event's term to hist[bin] (device layout) for a back projection afterwards, op 1 writes
+// listmode_binned_num_blocks partials
+int listmode_binned_num_blocks(int64_t n);
+cudaError_t launch_listmode_binned(const ProjParams& p, const int4* table, const LmEventDev* events, int64_t n, int op,
+                                   const float* fwd, const float* fwd_rhs, int subset, int nsub, int has_add,
+                                   float* hist, double* partial, unsigned* invalid, cudaStream_t st);
+cudaError_t launch_add(float* out, const float* s, int64_t n, cudaStream_t st);  // out += s
 
 // Projection data streams (stream.cu): NumericType codes and storage orders as b200rt_stream_format
 constexpr int kNumSChar = 0, kNumUChar = 1, kNumShort = 2, kNumUShort = 3, kNumInt = 4, kNumUInt = 5, kNumFloat = 6,

@@ -175,13 +175,119 @@ __global__ void __launch_bounds__(kLmThreads) listmode_kernel(const ProjParams p
   }
 }
 
+// Binned form of the same three sums.  The rows of all events of one bin are the same row, so
+//   sum_e A_e^T t_e = A^T h,  h[bin] = sum over the bin's events of t_e,
+// and A_e x is entry `bin` of the forward projection A x of the subset.  One thread per event reads its bin's
+// A x (and A rhs), applies the event's term exactly as the per-event kernel does, and adds it to h (device
+// layout, float atomics); the projection kernels then take A x before and A^T h after.  Per event this costs a
+// few bytes instead of a walk over ~400 row elements, so once the events number a fair fraction of the bins
+// the two whole-subset projections are cheaper than the per-event rows.
+constexpr int kLmBinThreads = 256;
+
+template <int OP>
+__global__ void __launch_bounds__(kLmBinThreads) listmode_binned_kernel(
+    const ProjParams p, const int4* __restrict__ table, const LmEventDev* __restrict__ ev, int64_t n,
+    const float* __restrict__ fwd, const float* __restrict__ fwd_rhs, int subset, int nsub, int has_add,
+    float* __restrict__ hist, double* __restrict__ partial, unsigned* __restrict__ invalid) {
+  double val = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(kLmBinThreads) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * kLmBinThreads) {
+    const LmEventDev e = ev[i];
+    if (e.value == 0.0f) continue;
+    const int s = e.seg + p.S, tofi = e.tof - p.min_tof, ti = e.tang - p.min_tang;
+    bool ok = s >= 0 && s <= 2 * p.S && tofi >= 0 && tofi < p.num_tof && e.view >= 0 && e.view < p.num_views &&
+              ti >= 0 && ti < p.num_tang;
+    int4 t = make_int4(-1, 0, 0, 0);
+    if (ok) t = table[((static_cast<int64_t>(tofi) * (2 * p.S + 1) + s) * p.num_views + e.view) * p.num_tang + ti];
+    SegDev sd{};
+    if (ok) sd = p.segs[s];
+    ok = ok && t.x >= 0 && e.axial >= 0 && e.axial < sd.nax;
+    if (!ok) {
+      atomicAdd(invalid, 1u);
+      continue;
+    }
+    if (nsub > 1 && t.z % nsub != subset) continue;
+    const int64_t bin = static_cast<int64_t>(tofi) * p.tof_stride + sd.dev_offset +
+                        (static_cast<int64_t>(e.view) * p.num_tang + ti) * sd.nax + e.axial;
+    const float y = e.value;
+    const float f = fwd[bin] + (has_add ? e.corr : 0.f);
+    const bool cancel = y > kMaxQuotient * f;
+    if (OP == 1) {
+      val -= cancel ? y * log(static_cast<double>(y / kMaxQuotient)) : y * log(static_cast<double>(f));
+      continue;
+    }
+    if (OP == 2 && cancel) continue;
+    float data;
+    if (OP == 0) {
+      data = y / f;
+    } else {
+      const float r = fwd_rhs[bin];
+      if (r == 0.f) continue;
+      data = (-y / (f * f)) * r;
+    }
+    if (data == 0.f) continue;
+    atomicAdd(hist + bin, data);
+  }
+  if (OP == 1) {
+    // fixed order: a shuffle tree per warp, then the warps in order; one partial per block
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+    __shared__ double red[kLmBinThreads / 32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = val;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kLmBinThreads / 32; ++w) t += red[w];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
 __global__ void subtract_kernel(float* __restrict__ out, const float* __restrict__ s, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     out[i] -= s[i];
 }
 
+__global__ void add_kernel(float* __restrict__ out, const float* __restrict__ s, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] += s[i];
+}
+
 }  // namespace
+
+cudaError_t launch_add(float* out, const float* s, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t want = (n + 255) / 256;
+  add_kernel<<<static_cast<int>(want > 148 * 32 ? 148 * 32 : want), 256, 0, st>>>(out, s, n);
+  return cudaGetLastError();
+}
+
+int listmode_binned_num_blocks(int64_t n) {
+  const int64_t want = (n + kLmBinThreads - 1) / kLmBinThreads;
+  return static_cast<int>(want < 1 ? 1 : (want > 148 * 8 ? 148 * 8 : want));
+}
+
+cudaError_t launch_listmode_binned(const ProjParams& p, const int4* table, const LmEventDev* events, int64_t n, int op,
+                                   const float* fwd, const float* fwd_rhs, int subset, int nsub, int has_add,
+                                   float* hist, double* partial, unsigned* invalid, cudaStream_t st) {
+  const int blocks = listmode_binned_num_blocks(n);
+  switch (op) {
+    case 0:
+      listmode_binned_kernel<0><<<blocks, kLmBinThreads, 0, st>>>(p, table, events, n, fwd, fwd_rhs, subset, nsub,
+                                                                  has_add, hist, partial, invalid);
+      break;
+    case 1:
+      listmode_binned_kernel<1><<<blocks, kLmBinThreads, 0, st>>>(p, table, events, n, fwd, fwd_rhs, subset, nsub,
+                                                                  has_add, hist, partial, invalid);
+      break;
+    default:
+      listmode_binned_kernel<2><<<blocks, kLmBinThreads, 0, st>>>(p, table, events, n, fwd, fwd_rhs, subset, nsub,
+                                                                  has_add, hist, partial, invalid);
+      break;
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_subtract(float* out, const float* s, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;

@@ -3,7 +3,9 @@
 Mirrors STIR's PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByBin
 (src/recon_buildblock/PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByBin.cxx): the
 events are the objective's cached BinAndCorr records (bin, value, additive term) held on the GPU; the gradient,
-value and Hessian-times-input of a subset are one kernel each (listmode.cu).  `ListModeOSEM` runs STIR's
+value and Hessian-times-input of a subset are one kernel each over the events' rows (listmode.cu), or, once the
+events number a fair fraction of the bins, one kernel over the events between the subset's forward and back
+projections (the binned method, see set_method).  `ListModeOSEM` runs STIR's
 OSMAPOSL update with this objective: x *= (gradient without the sensitivity) / subset sensitivity, with the
 sensitivities back-projected from the (binned) multiplicative factors.  Reading vendor list-mode files is not
 part of this module: events come as arrays (segment, view, axial, tangential, timing) with values.
@@ -49,6 +51,13 @@ class PoissonLogLikelihoodWithLinearModelForMeanAndListModeDataWithProjMatrixByB
         self.num_events = events.numel() // EVENT_DTYPE.itemsize
         self.num_subsets = num_subsets
         self.has_add = bool(has_add)
+
+    def set_method(self, method: int):
+        """_abi.LISTMODE_AUTO (default), LISTMODE_PER_EVENT (one row walk per event) or LISTMODE_BINNED (A x of
+        the subset read per event, the events' terms summed per bin and back projected once); the method is a
+        setting of the projector."""
+        _abi.check(self.proj.lib.b200rt_listmode_set_method(self.proj.h, int(method)), self.proj.h,
+                   "b200rt_listmode_set_method")
 
     def compute_sub_gradient_without_penalty(self, x, subset_num: int, subset_sensitivity=None, out=None,
                                              accumulate=False, stream=None):

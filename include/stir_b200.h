@@ -173,6 +173,19 @@ int b200rt_image_from_device_layout(b200rt_projector* h, const float* dev, float
 int b200rt_projdata_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream);
 int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream);
 
+/* Viewgrams of device-layout projection data: the viewgram API of ForwardProjectorByBin / BackProjectorByBin
+ * served from device buffers, as ForwardProjectorByBinParallelproj::actual_forward_project serves the related
+ * viewgrams from the projection that set_input made (ForwardProjectorByBinParallelproj.cxx:128-145) and
+ * BackProjectorByBinParallelproj::actual_back_project stores them for get_output's back projection
+ * (BackProjectorByBinParallelproj.cxx:313-328).  A viewgram is STIR's Viewgram<float> of (segment, view, timing
+ * position): [axial_pos][tangential_pos] floats.  `viewgram` may be host or device memory; with host memory the
+ * call synchronises `stream` before it returns.  set: accumulate = 0 overwrites the viewgram, 1 adds to it.
+ * B200RT_ERR_INVALID_ARGUMENT for a segment, view or timing position outside the projector's data. */
+int b200rt_get_viewgram(b200rt_projector* h, const float* projdata_dev, int segment_num, int view_num,
+                        int timing_pos_num, float* viewgram, void* stream);
+int b200rt_set_viewgram(b200rt_projector* h, float* projdata_dev, int segment_num, int view_num, int timing_pos_num,
+                        const float* viewgram, int accumulate, void* stream);
+
 /* ---- projectors on device-resident data (device layouts) ---------------- */
 
 /* ForwardProjectorByBin::forward_project(ProjData&, image, subset_num, num_subsets, zero)

@@ -224,6 +224,8 @@ EXPORTS = [
     ("b200rt_image_from_device_layout", _I, [_P, _P, _P, _P]),
     ("b200rt_projdata_to_device_layout", _I, [_P, _P, _P, _P]),
     ("b200rt_projdata_from_device_layout", _I, [_P, _P, _P, _P]),
+    ("b200rt_get_viewgram", _I, [_P, _P, _I, _I, _I, _P, _P]),
+    ("b200rt_set_viewgram", _I, [_P, _P, _I, _I, _I, _P, _I, _P]),
     ("b200rt_forward_project_dev", _I, [_P, _P, _P, _I, _I, _P]),
     ("b200rt_back_project_dev", _I, [_P, _P, _P, _I, _I, _I, _P]),
     ("b200rt_sensitivity_dev", _I, [_P, _P, _P, _I, _I, _I, _I, _P]),

@@ -155,6 +155,8 @@ struct b200rt_projector {
   // binned list mode: A x and A rhs of the subset, the events' terms per bin, a scratch image
   int lm_method = B200RT_LISTMODE_AUTO;
   DevBuf<float> lm_fwd, lm_fwd_rhs, lm_hist, lm_img;
+  // viewgram access: a viewgram in STIR order and a transposed copy
+  DevBuf<float> vg_scratch;
 
   long long bin_key(int view, int seg, int tang, int tof) const {
     const Geometry& g = *geo;
@@ -1122,6 +1124,7 @@ void b200rt_destroy(b200rt_projector* h) {
     h->lm_fwd_rhs.release();
     h->lm_hist.release();
     h->lm_img.release();
+    h->vg_scratch.release();
     if (h->copy_stream) {
       cudaStreamSynchronize(h->copy_stream);
       cudaStreamDestroy(h->copy_stream);
@@ -1219,6 +1222,97 @@ int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, fl
   DeviceGuard dg(h->device);
   const cudaError_t e = projdata_layout(*h->geo, dev, stir_dev, false, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
+}
+
+}  // extern "C"
+
+namespace {
+
+// the device-layout block of viewgram (segment, view, timing position): [tangential][axial], contiguous
+const char* viewgram_block(const b200rt_projector& h, int seg, int view, int tof, int64_t& off, int& nax) {
+  const Geometry& g = *h.geo;
+  if (seg < -g.S() || seg > g.S()) return "segment out of range";
+  if (view < 0 || view >= g.num_views()) return "view out of range";
+  if (tof < g.min_tof() || tof >= g.min_tof() + g.num_tof()) return "timing position out of range";
+  nax = g.nax(seg);
+  off = static_cast<int64_t>(tof - g.min_tof()) * g.tof_stride() + g.dev_segment_offset(seg) +
+        static_cast<int64_t>(view) * g.num_tang() * nax;
+  return nullptr;
+}
+
+bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200rt_get_viewgram(b200rt_projector* h, const float* projdata_dev, int segment_num, int view_num,
+                        int timing_pos_num, float* viewgram, void* stream) {
+  if (!h || !projdata_dev || !viewgram) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  int64_t off = 0;
+  int nax = 0;
+  if (const char* why = viewgram_block(*h, segment_num, view_num, timing_pos_num, off, nax))
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, why);
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nt = h->geo->num_tang();
+    const size_t n = static_cast<size_t>(nt) * nax;
+    const bool dev_out = is_device_pointer(viewgram);
+    float* dst = viewgram;
+    if (!dev_out) {
+      h->vg_scratch.alloc(std::max(h->vg_scratch.n, 2 * n));
+      dst = h->vg_scratch.p;
+    }
+    ck(launch_transpose(projdata_dev + off, dst, nt, nax, nax, nt, st), "viewgram");
+    if (!dev_out) {
+      ck(cudaMemcpyAsync(viewgram, dst, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "D2H");
+      ck(cudaStreamSynchronize(st), "viewgram");
+    }
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
+int b200rt_set_viewgram(b200rt_projector* h, float* projdata_dev, int segment_num, int view_num, int timing_pos_num,
+                        const float* viewgram, int accumulate, void* stream) {
+  if (!h || !projdata_dev || !viewgram) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  int64_t off = 0;
+  int nax = 0;
+  if (const char* why = viewgram_block(*h, segment_num, view_num, timing_pos_num, off, nax))
+    return fail(h, B200RT_ERR_INVALID_ARGUMENT, why);
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nt = h->geo->num_tang();
+    const size_t n = static_cast<size_t>(nt) * nax;
+    h->vg_scratch.alloc(std::max(h->vg_scratch.n, 2 * n));
+    const float* src = viewgram;
+    if (!is_device_pointer(viewgram)) {
+      ck(cudaMemcpyAsync(h->vg_scratch.p, viewgram, sizeof(float) * n, cudaMemcpyHostToDevice, st), "H2D");
+      src = h->vg_scratch.p;
+    }
+    // [axial][tangential] -> [tangential][axial]
+    if (accumulate) {
+      ck(launch_transpose(src, h->vg_scratch.p + n, nax, nt, nt, nax, st), "viewgram");
+      ck(launch_add(projdata_dev + off, h->vg_scratch.p + n, static_cast<int64_t>(n), st), "viewgram");
+    } else {
+      ck(launch_transpose(src, projdata_dev + off, nax, nt, nt, nax, st), "viewgram");
+    }
+    // the host source may be reused by the caller as soon as this returns
+    if (src != viewgram) ck(cudaStreamSynchronize(st), "viewgram");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
 }
 
 int b200rt_forward_project_dev(b200rt_projector* h, const float* image_dev, float* projdata_dev, int subset_num,

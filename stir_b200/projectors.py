@@ -169,6 +169,40 @@ class RayTracingProjector:
                    "b200rt_projdata_from_device_layout")
         return out
 
+    # viewgrams of device-layout projection data ([axial][tangential], STIR's Viewgram order)
+    def viewgram_shape(self, segment: int):
+        return (self.proj_data_info.get_num_axial_poss(segment), self.proj_data_info.num_tangential_poss)
+
+    def get_viewgram(self, projdata_dev, segment: int, view: int, timing_pos: int = 0, out=None, stream=None):
+        """The viewgram (segment, view, timing position) of projdata_dev; `out` a numpy array (default) or a CUDA
+        tensor of viewgram_shape(segment)."""
+        _check_tensor(projdata_dev, self.projdata_size)
+        if out is None:
+            out = np.empty(self.viewgram_shape(segment), np.float32)
+        ptr = _np_ptr(out) if isinstance(out, np.ndarray) else ctypes.c_void_p(out.data_ptr())
+        if isinstance(out, np.ndarray) and (out.dtype != np.float32 or not out.flags.c_contiguous or
+                                            out.shape != self.viewgram_shape(segment)):
+            raise ValueError("expected a contiguous float32 array of the viewgram's shape")
+        _abi.check(self.lib.b200rt_get_viewgram(self.h, ctypes.c_void_p(projdata_dev.data_ptr()), segment, view,
+                                                timing_pos, ptr, _stream_ptr(stream)), self.h, "b200rt_get_viewgram")
+        return out
+
+    def set_viewgram(self, projdata_dev, viewgram, segment: int, view: int, timing_pos: int = 0,
+                     accumulate: bool = False, stream=None):
+        """Overwrite (or add to) the viewgram (segment, view, timing position) of projdata_dev."""
+        _check_tensor(projdata_dev, self.projdata_size)
+        if isinstance(viewgram, np.ndarray):
+            viewgram = np.ascontiguousarray(viewgram, np.float32)
+            if viewgram.shape != self.viewgram_shape(segment):
+                raise ValueError("viewgram shape differs from (axial positions, tangential positions)")
+            ptr = _np_ptr(viewgram)
+        else:
+            ptr = ctypes.c_void_p(viewgram.data_ptr())
+        _abi.check(self.lib.b200rt_set_viewgram(self.h, ctypes.c_void_p(projdata_dev.data_ptr()), segment, view,
+                                                timing_pos, ptr, int(accumulate), _stream_ptr(stream)), self.h,
+                   "b200rt_set_viewgram")
+        return projdata_dev
+
 
 def _check_tensor(t, numel):
     if not t.is_cuda or not t.is_contiguous() or t.numel() != numel or str(t.dtype) != "torch.float32":
@@ -182,6 +216,7 @@ class ForwardProjectorByBinB200RayTracing:
         self._projector = projector
         self._matrix_params = matrix_params
         self._input = None
+        self._cached = None  # device projection of the input, serving forward_project_viewgram
 
     def set_up(self, proj_data_info: ProjDataInfo, image: ImageGeometry):
         if self._projector is None or self._projector.proj_data_info != proj_data_info or self._projector.image != image:
@@ -194,6 +229,21 @@ class ForwardProjectorByBinB200RayTracing:
     def set_input(self, image: np.ndarray):
         self._check_set_up()
         self._input = np.ascontiguousarray(image, np.float32)
+        self._cached = None
+
+    def forward_project_viewgram(self, segment: int, view: int, timing_pos: int = 0):
+        """actual_forward_project for one viewgram (the related set of a projector with trivial symmetries):
+        the first call after set_input projects the whole data on the device, later calls copy their viewgram
+        out of that projection (ForwardProjectorByBinParallelproj.cxx:128-145, 160-282)."""
+        self._check_set_up()
+        if self._input is None:
+            raise RuntimeError("ForwardProjectorByBin: no input image")
+        p = self._projector
+        if self._cached is None:
+            import torch
+            img = p.image_to_device_layout(torch.from_numpy(self._input).to(f"cuda:{p.device}"))
+            self._cached = p.forward_dev(img)
+        return p.get_viewgram(self._cached, segment, view, timing_pos)
 
     def forward_project(self, proj_data: np.ndarray, image: Optional[np.ndarray] = None, subset_num: int = 0,
                         num_subsets: int = 1, zero: bool = True):
@@ -225,6 +275,7 @@ class BackProjectorByBinB200RayTracing:
         self._matrix_params = matrix_params
         self.mode = mode
         self._acc = None
+        self._staged = None  # device projection data of back_project_viewgram, back projected by get_output
 
     def set_up(self, proj_data_info: ProjDataInfo, image: ImageGeometry):
         if self._projector is None or self._projector.proj_data_info != proj_data_info or self._projector.image != image:
@@ -237,6 +288,17 @@ class BackProjectorByBinB200RayTracing:
     def start_accumulating_in_new_target(self):
         self._check_set_up()
         self._acc = np.zeros(self._projector.image_shape, np.float32)
+        self._staged = None
+
+    def back_project_viewgram(self, viewgram: np.ndarray, segment: int, view: int, timing_pos: int = 0):
+        """actual_back_project for one viewgram: added to projection data staged on the device, back projected
+        by get_output (BackProjectorByBinParallelproj.cxx:161-328)."""
+        self._check_set_up()
+        if self._acc is None:
+            raise RuntimeError("You need to call start_accumulating_in_new_target() before back_project()")
+        if self._staged is None:
+            self._staged = self._projector.empty_projdata()
+        self._projector.set_viewgram(self._staged, viewgram, segment, view, timing_pos, accumulate=True)
 
     def back_project(self, image_or_proj_data, proj_data=None, subset_num: int = 0, num_subsets: int = 1):
         """back_project(image, proj_data, subset, nsub): overwrite `image` with A^T of the subset;
@@ -254,6 +316,10 @@ class BackProjectorByBinB200RayTracing:
     def get_output(self, image: np.ndarray):
         if self._acc is None:
             raise RuntimeError("BackProjectorByBin: nothing accumulated")
+        if self._staged is not None:
+            p = self._projector
+            self._acc += p.image_from_device_layout(p.back_dev(self._staged, mode=self.mode)).cpu().numpy()
+            self._staged = None
         image[...] = self._acc.reshape(image.shape)
         return image
 

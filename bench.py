@@ -407,6 +407,11 @@ def profile_value(key, kernel_name):
     return None
 
 
+def _ratio(nbytes, ms):
+    """GB/s of nbytes moved in ms, or None without a byte count"""
+    return None if nbytes is None else nbytes / (ms / 1e3) / 1e9
+
+
 def profile_traffic(kernel_name):
     """DRAM bytes per launch of `kernel_name` from the committed ncu summary (profiles/), or None."""
     return profile_value("traffic_per_launch", kernel_name)
@@ -627,7 +632,17 @@ def b200_main(args):
                         "frac_forward": profile_value("smem_wavefront_frac", FWD_KERNEL),
                         "frac_back": profile_value("smem_wavefront_frac", BACK_KERNEL),
                         "issue_active_forward": profile_value("issue_active_frac", FWD_KERNEL),
-                        "issue_active_back": profile_value("issue_active_frac", BACK_KERNEL)}}
+                        "issue_active_back": profile_value("issue_active_frac", BACK_KERNEL)},
+            # compulsory traffic: the image and the projection data once each way (forward reads the image and
+            # writes the bins, back reads the bins and writes the image), against the same copy bandwidth
+            "compulsory": {"bytes_forward": img_bytes + pd_bytes, "bytes_back": pd_bytes + img_bytes,
+                           "frac_forward": (img_bytes + pd_bytes) / (fwd_ms / 1e3) / 1e9 / hbm,
+                           "frac_back": (pd_bytes + img_bytes) / (back_ms / 1e3) / 1e9 / hbm},
+            # DRAM bytes per launch (committed ncu summaries) over the live kernel time, and the L2 hit rate there
+            "dram_GBs": {FWD_KERNEL: _ratio(profile_traffic(FWD_KERNEL), fwd_ms),
+                         BACK_KERNEL: _ratio(profile_traffic(BACK_KERNEL), back_ms)},
+            "l2_hit_rate": {FWD_KERNEL: profile_value("l2_hit_rate", FWD_KERNEL),
+                            BACK_KERNEL: profile_value("l2_hit_rate", BACK_KERNEL)}}
 
     cpu = None
     cb = None

@@ -1001,7 +1001,7 @@ cudaError_t copy_views(const Geometry& g, float* dst, const float* src, int v0, 
 
 constexpr int kHostViewGroups = 8;
 
-// the subset's path items ordered by the group of views they write (kHostViewGroups equal view ranges)
+// the subset's path items ordered by the group of views they write (kHostViewGroups view ranges)
 const b200rt_projector::ViewGroups& view_groups(b200rt_projector& h, int subset, int nsub) {
   const auto key = std::make_pair(subset, nsub);
   auto it = h.view_groups.find(key);
@@ -1009,7 +1009,21 @@ const b200rt_projector::ViewGroups& view_groups(b200rt_projector& h, int subset,
   const int nv = h.geo->num_views();
   const int G = std::min(kHostViewGroups, nv);
   b200rt_projector::ViewGroups vg;
-  for (int gi = 0; gi <= G; ++gi) vg.v0.push_back(static_cast<int>(static_cast<int64_t>(nv) * gi / G));
+  if (G == kHostViewGroups && nv >= 120) {
+    // tapered (with at least 4 views per unit of size): the copy that cannot overlap a projection (the forward's last group, the back projection's first)
+    // is of a small group; relative sizes 1, 2, 4, 8, 8, 4, 2, 1
+    static const int w[kHostViewGroups] = {1, 2, 4, 8, 8, 4, 2, 1};
+    int acc = 0, total = 0;
+    for (int gi = 0; gi < G; ++gi) total += w[gi];
+    vg.v0.push_back(0);
+    for (int gi = 0; gi < G; ++gi) {
+      acc += w[gi];
+      vg.v0.push_back(std::max(vg.v0.back() + 1, static_cast<int>(static_cast<int64_t>(nv) * acc / total)));
+    }
+    vg.v0.back() = nv;
+  } else {
+    for (int gi = 0; gi <= G; ++gi) vg.v0.push_back(static_cast<int>(static_cast<int64_t>(nv) * gi / G));
+  }
   std::vector<std::vector<int>> per(G);
   for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i) {
     if (h.h_item_view[i] % nsub != subset) continue;

@@ -7,7 +7,7 @@ import pytest
 from stir_b200 import _abi
 from stir_b200 import interfile
 
-REF_HS = "/root/reference/recon_test_pack/scatter_cylinder.hs"
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scatter_cylinder.npz")
 
 
 def test_segment_sequence():
@@ -63,10 +63,13 @@ matrix axis label [2] := axial coordinate
         interfile.InterfileProjDataHeader(_header(tmp_path, common))  # no view / axial labels
 
 
-@pytest.mark.skipif(not os.path.exists(REF_HS), reason="STIR's recon_test_pack is not here")
-def test_reads_stir_test_pack_header(oracle_lib):
-    """scatter_cylinder.hs of STIR's recon_test_pack: 1 segment, 32 views, 8 rings, 35 bins, float LE, view-major."""
-    h = interfile.InterfileProjDataHeader(REF_HS)
+def test_reads_stir_test_pack_header(oracle_lib, tmp_path):
+    """scatter_cylinder.hs of STIR's recon_test_pack (header text and data bytes in a fixture written by
+    golden/make_fixtures.py): 1 segment, 32 views, 8 rings, 35 bins, float LE, view-major."""
+    fx = np.load(GOLDEN)
+    (tmp_path / "scatter_cylinder.hs").write_bytes(fx["header"].tobytes())
+    (tmp_path / "scatter_cylinder.s").write_bytes(fx["data"].tobytes())
+    h = interfile.InterfileProjDataHeader(str(tmp_path / "scatter_cylinder.hs"))
     assert h.storage_order == _abi.STORAGE_SEGMENT_VIEW_AXIAL_TANG
     assert (h.num_views, h.num_axial_poss, h.num_tangential_poss) == (32, [8], 35)
     assert h.segment_sequence == [0] and h.number_type == "float" and not h.big_endian

@@ -293,8 +293,9 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
     over = std::max(over, G.over);
   }
   // padded staging: zero planes between the staged columns cover every pass's reads outside [0, nz), so
-  // the forward needs no per-lane range tests (a cap keeps the staging buffer small)
-  const int zpad = over <= 64 ? (over + 3) & ~3 : -1;
+  // the forward needs no per-lane range tests (a cap keeps the staging buffer small, and at most 2048 planes
+  // per staged column keep every staged index within the 16 bits the padded kernels store it in)
+  const int zpad = over <= 64 && nz + ((over + 3) & ~3) <= 2048 ? (over + 3) & ~3 : -1;
   const int K = std::max(8, 32768 / (4 * (nz + std::max(zpad, 0))));  // 32 KB of staged float columns
   // chunk c of a row covers its elements with slot in [c K, (c + 1) K)
   for (Group& G : groups) {

@@ -100,6 +100,19 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
 }
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// one packed element of the padded path: staged indices (16-bit, signed) of axial position 0 for both lines
+template <int NJ, bool TWO>
+__device__ __forceinline__ void padded_fma(const float* cols, uint32_t idx, float v, int zo0, int npa, float* acc1,
+                                           float* acc2) {
+  const float* q1 = cols + (static_cast<int>(static_cast<int16_t>(idx & 0xffffu)) + zo0);
+  const float* q2 = cols + ((static_cast<int>(idx) >> 16) + zo0);
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    acc1[j] += q1[j * 32 * npa] * v;
+    if (TWO) acc2[j] += q2[j * 32 * npa] * v;
+  }
+}
+
 // One pass of one unit over elements [e0, e1) of its row: NJ groups of 32 axial positions from a0.
 // The warp's lanes transform 32 elements at a time (column slot -> staged index, z reflection) into
 // the warp's buffer; then every element costs one broadcast read and NJ shared loads and FMAs.
@@ -122,6 +135,9 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
     acc2[j] = (TWO && act[j]) ? acc_row2[a0 + j * 32 + lane] : 0.f;
   }
   const int zlo = a0 * npa, zhi = (a0 + nact - 1) * npa;
+  // padded staging: every read stays inside the staging buffer (fewer than 2^14 floats), so the two staged
+  // indices fit 16 bits each and an element is 8 bytes; one 16-byte broadcast read serves two elements
+  uint2* xp = reinterpret_cast<uint2*>(xb);
   for (int k0 = e0; k0 < e1; k0 += 32) {
     const int cnt = min(32, e1 - k0);
     __syncwarp();
@@ -132,16 +148,36 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
       const int sl = static_cast<int>(m.sz & 0xffffu) - c0;
       const int zt1 = L1.zsign * zr + L1.zadd;
       const int zt2 = TWO ? L2.zsign * zr + L2.zadd : 0;
-      const int f1 = (zt1 + zlo >= 0) && (zt1 + zhi < nz);
-      const int f2 = TWO ? ((zt2 + zlo >= 0) && (zt2 + zhi < nz)) : 1;
-      PathXElem x;
-      x.base = sl * cstride + coff + zt1;
-      x.zt = sl * cstride + coff + zt2;
-      x.v = m.v;
-      x.full = sl | ((PADDED ? 1 : (f1 & f2)) << 30);
-      xb[lane] = x;
+      if (PADDED) {
+        const int b1 = sl * cstride + coff + zt1, b2 = TWO ? sl * cstride + coff + zt2 : 0;
+        xp[lane] = make_uint2((static_cast<uint32_t>(b1) & 0xffffu) | (static_cast<uint32_t>(b2) << 16),
+                              __float_as_uint(m.v));
+      } else {
+        const int f1 = (zt1 + zlo >= 0) && (zt1 + zhi < nz);
+        const int f2 = TWO ? ((zt2 + zlo >= 0) && (zt2 + zhi < nz)) : 1;
+        PathXElem x;
+        x.base = sl * cstride + coff + zt1;
+        x.zt = sl * cstride + coff + zt2;
+        x.v = m.v;
+        x.full = sl | ((f1 & f2) << 30);
+        xb[lane] = x;
+      }
     }
     __syncwarp();
+    if (PADDED) {
+      const uint4* xq = reinterpret_cast<const uint4*>(xb);
+      int i = 0;
+      for (; i + 1 < cnt; i += 2) {
+        const uint4 w = xq[i >> 1];
+        padded_fma<NJ, TWO>(cols, w.x, __uint_as_float(w.y), zo0, npa, acc1, acc2);
+        padded_fma<NJ, TWO>(cols, w.z, __uint_as_float(w.w), zo0, npa, acc1, acc2);
+      }
+      if (i < cnt) {
+        const uint2 w = xp[i];
+        padded_fma<NJ, TWO>(cols, w.x, __uint_as_float(w.y), zo0, npa, acc1, acc2);
+      }
+      continue;
+    }
     for (int i = 0; i < cnt; ++i) {
       const PathXElem e = xb[i];
       const float* q1 = cols + (e.base + zo0);

@@ -233,7 +233,7 @@ __host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int zpad, in
 // back path CTA: line set-up, per line (z sign, z offset, window length, data offset), per member its
 // first line and line count, padded line data
 struct PathSmemBack {
-  int lines, lz, members, dl, total;
+  int lines, lz, members, dl, ebuf, total;
 };
 __host__ __device__ inline PathSmemBack path_smem_back(int nz, int max_lines, int max_members, int nax_max,
                                                        int npa_max) {
@@ -242,7 +242,8 @@ __host__ __device__ inline PathSmemBack path_smem_back(int nz, int max_lines, in
   s.lz = path_align16(max_lines * static_cast<int>(sizeof(PathLineSmem)));
   s.members = path_align16(s.lz + max_lines * 16);
   s.dl = path_align16(s.members + max_members * 8);
-  s.total = path_align16(s.dl + max_lines * path_dl_len(nz, nax_max, npa_max) * 4);
+  s.ebuf = path_align16(s.dl + max_lines * path_dl_len(nz, nax_max, npa_max) * 4);
+  s.total = s.ebuf + kPathWarpsH * 32 * 8;  // per warp: 32 column-order elements
   return s;
 }
 

@@ -367,17 +367,12 @@ struct FixedCols {
 template <typename Cols, bool HIT>
 __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int k0, int k1, const int4* lz,
                                             const int2* members, const float* dl, int zp, int nz, int lane, int b,
-                                            const Cols& acc) {
+                                            const Cols& acc, PathCElem* eb) {
   typename Cols::T sum[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) sum[j] = typename Cols::T(0);
-  for (int kb = k0; kb < k1; kb += 32) {
-    PathCElem mine{0u, 0.f};
-    if (kb + lane < k1) mine = E[kb + lane];
-    const int cnt = min(32, k1 - kb);
-    for (int i = 0; i < cnt; ++i) {
-      const uint32_t mz = __shfl_sync(0xffffffffu, mine.mz, i);
-      const float v = __shfl_sync(0xffffffffu, mine.v, i);
+  // the warp's 32 elements at a time go through its shared buffer; one 16-byte broadcast read serves two
+  auto element = [&](uint32_t mz, float v) {
       const int zr = static_cast<int>(mz & 0xffffu);
       const int2 mem = members[mz >> 16];  // (first line, number of lines) of the element's basic bin
       auto line = [&](int l) {
@@ -393,6 +388,22 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
       if (mem.y > 0) line(mem.x);
       if (mem.y > 1) line(mem.x + 1);
       for (int l = mem.x + 2; l < mem.x + mem.y; ++l) line(l);
+  };
+  for (int kb = k0; kb < k1; kb += 32) {
+    const int cnt = min(32, k1 - kb);
+    __syncwarp();
+    if (lane < cnt) eb[lane] = E[kb + lane];
+    __syncwarp();
+    const uint4* eq = reinterpret_cast<const uint4*>(eb);
+    int i = 0;
+    for (; i + 1 < cnt; i += 2) {
+      const uint4 w = eq[i >> 1];
+      element(w.x, __uint_as_float(w.y));
+      element(w.z, __uint_as_float(w.w));
+    }
+    if (i < cnt) {
+      const PathCElem e = eb[i];
+      element(e.mz, e.v);
     }
   }
   if (b < 0) return;
@@ -415,6 +426,7 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
   int4* lz = reinterpret_cast<int4*>(smem + lay.lz);
   int2* members = reinterpret_cast<int2*>(smem + lay.members);
   float* dl = reinterpret_cast<float*>(smem + lay.dl);
+  PathCElem* eb = reinterpret_cast<PathCElem*>(smem + lay.ebuf) + warp * 32;
   const int nl = it.num_lines;
   setup_path_lines(p, pp, it, ls);
   for (int m = threadIdx.x; m < pp.max_members; m += blockDim.x) members[m] = make_int2(0, 0);
@@ -461,9 +473,9 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
     const int k0 = __ldg(cs + ci), k1 = __ldg(cs + ci + 1);
     for (int zp = 0; zp < nz; zp += 128) {
       if (pp.zpad >= 0)
-        back_column<Cols, true>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+        back_column<Cols, true>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
       else
-        back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc);
+        back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
     }
   }
 }

@@ -243,7 +243,7 @@ __host__ __device__ inline PathSmemBack path_smem_back(int nz, int max_lines, in
   s.members = path_align16(s.lz + max_lines * 16);
   s.dl = path_align16(s.members + max_members * 8);
   s.ebuf = path_align16(s.dl + max_lines * path_dl_len(nz, nax_max, npa_max) * 4);
-  s.total = s.ebuf + kPathWarpsH * 32 * 8;  // per warp: 32 column-order elements
+  s.total = s.ebuf + kPathWarpsH * 32 * 16;  // per warp: 32 column-order elements with their member's lines
   return s;
 }
 

@@ -367,14 +367,13 @@ struct FixedCols {
 template <typename Cols, bool HIT>
 __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int k0, int k1, const int4* lz,
                                             const int2* members, const float* dl, int zp, int nz, int lane, int b,
-                                            const Cols& acc, PathCElem* eb) {
+                                            const Cols& acc, int4* eb) {
   typename Cols::T sum[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) sum[j] = typename Cols::T(0);
-  // the warp's 32 elements at a time go through its shared buffer; one 16-byte broadcast read serves two
-  auto element = [&](uint32_t mz, float v) {
-      const int zr = static_cast<int>(mz & 0xffffu);
-      const int2 mem = members[mz >> 16];  // (first line, number of lines) of the element's basic bin
+  // the warp's 32 elements at a time go through its shared buffer as (z, value, first line and number of lines
+  // of the element's basic bin): one 16-byte broadcast read per element
+  auto element = [&](int zr, float v, int2 mem) {
       auto line = [&](int l) {
         const int4 L = lz[l];  // (z sign, z offset, window length, data offset)
         int zt = L.x * zr + L.y;
@@ -392,18 +391,15 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
   for (int kb = k0; kb < k1; kb += 32) {
     const int cnt = min(32, k1 - kb);
     __syncwarp();
-    if (lane < cnt) eb[lane] = E[kb + lane];
-    __syncwarp();
-    const uint4* eq = reinterpret_cast<const uint4*>(eb);
-    int i = 0;
-    for (; i + 1 < cnt; i += 2) {
-      const uint4 w = eq[i >> 1];
-      element(w.x, __uint_as_float(w.y));
-      element(w.z, __uint_as_float(w.w));
+    if (lane < cnt) {
+      const PathCElem e = E[kb + lane];
+      const int2 mem = members[e.mz >> 16];
+      eb[lane] = make_int4(static_cast<int>(e.mz & 0xffffu), __float_as_int(e.v), mem.x, mem.y);
     }
-    if (i < cnt) {
-      const PathCElem e = eb[i];
-      element(e.mz, e.v);
+    __syncwarp();
+    for (int i = 0; i < cnt; ++i) {
+      const int4 w = eb[i];
+      element(w.x, __int_as_float(w.y), make_int2(w.z, w.w));
     }
   }
   if (b < 0) return;
@@ -426,7 +422,7 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
   int4* lz = reinterpret_cast<int4*>(smem + lay.lz);
   int2* members = reinterpret_cast<int2*>(smem + lay.members);
   float* dl = reinterpret_cast<float*>(smem + lay.dl);
-  PathCElem* eb = reinterpret_cast<PathCElem*>(smem + lay.ebuf) + warp * 32;
+  int4* eb = reinterpret_cast<int4*>(smem + lay.ebuf) + warp * 32;
   const int nl = it.num_lines;
   setup_path_lines(p, pp, it, ls);
   for (int m = threadIdx.x; m < pp.max_members; m += blockDim.x) members[m] = make_int2(0, 0);

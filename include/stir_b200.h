@@ -267,17 +267,22 @@ int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const
  * For callers that must not allocate device memory once they are set up: for example a
  * reconstruction service that hands all device memory to a caching allocator at start-up, or
  * that cannot afford the device-wide synchronisation a cudaMalloc/cudaFree implies in the middle
- * of a frame.  This call allocates nothing: its scratch (the subset's bin list, the viewgram
- * thresholds and one partial sum per CTA) lives in a fixed 1.77 MiB array compiled into the
- * library, which every GPU that loads the library holds until the process exits.
- *   - limits: at most 131072 basic bins in the subset, 4096 views, 65536 viewgrams
- *     ((2*max_segment_num+1)*num_views); larger requests return B200RT_ERR_TOO_LARGE;
+ * of a frame.  This call allocates nothing and copies nothing from the host: the subset's work list
+ * and view list are selected on the device from tables made by b200rt_create, and its scratch (those
+ * lists, the viewgram thresholds and one FP64 partial sum per work item) lives in a fixed 2.02 MiB
+ * array compiled into the library, which every GPU that loads the library holds until the process
+ * exits.  It runs the same kernel on the same work items as b200rt_log_likelihood_dev (path items,
+ * or basic bins with all their timing bins for a TOF projector), so the two agree to the last bit.
+ *   - limits: at most 131072 work items in the subset (path items, or basic bins), 4096 views of the
+ *     subset, and 131072 viewgrams in the data (num_tof_bins * (2*max_segment_num+1) * num_views);
+ *     larger requests return B200RT_ERR_TOO_LARGE with the counts in b200rt_last_error;
  *   - the result is written to out_dev, a device double the caller provides; the call is
  *     asynchronous on `stream` and does not synchronise;
  *   - all calls share the one array: calls that overlap on the GPU (other streams, other threads)
  *     race and corrupt each other's results;
- *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress); make
- *     that first call before any stream capture. */
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) and
+ *     keeps it for the life of the process; make that first call before any stream capture, and do
+ *     not reset the device (cudaDeviceReset) between calls. */
 int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const float* image_dev, const float* y_dev,
                                       const float* additive_dev, const float* mult_dev, int subset_num, int num_subsets,
                                       int zero_seg0_end_planes, double* out_dev, void* stream);

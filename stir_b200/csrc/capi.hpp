@@ -94,6 +94,9 @@ struct b200rt_projector {
   std::vector<ProjBinDev> h_bins;
   std::vector<int> h_bin_view;  // basic view of each bin
   std::vector<int> h_bin_seg;
+  std::vector<int> h_view_basic;  // basic view of each view (-1: none)
+  // basic views of h_bin_view, h_tof_basic_view, h_item_view and h_view_basic on the device (set-up)
+  DevBuf<int> bin_view_dev, tof_basic_view_dev, item_view_dev, view_basic_dev;
   std::map<long long, int> bin_index;  // (view, seg, tang, tof) -> bin
   int64_t total_nnz = 0;
   int num_basic_views = 0;

@@ -605,6 +605,22 @@ void setup_projector(b200rt_projector& h) {
       build_paths(h, hr, lines, static_cast<int>(bviews.size()), static_cast<int>(bsegs.size()),
                   static_cast<int>(btangs.size()), bviews);
   }
+  // the basic view of every entry of each work list (bins, TOF basic bins, path items) and of every view (-1: a
+  // view no basic view reaches), on the device: the allocation-free entry point selects a subset's work and views
+  // from these without host copies
+  std::vector<int> view_basic(g.num_views(), -1);
+  for (int v : g.basic_views())
+    for (int seg : g.basic_segments()) {
+      std::vector<RelatedLine> rel;
+      g.related_lines(v, seg, true, rel);
+      for (const auto& r : rel) view_basic[r.view] = v;
+    }
+  h.bin_view_dev.upload(h.h_bin_view, h.stream);
+  h.view_basic_dev.upload(view_basic, h.stream);
+  if (h.use_paths) h.item_view_dev.upload(h.h_item_view, h.stream);
+  if (!h.h_tof_basic_view.empty()) h.tof_basic_view_dev.upload(h.h_tof_basic_view, h.stream);
+  h.h_view_basic = std::move(view_basic);
+  ck(cudaStreamSynchronize(h.stream), "basic view tables");
 }
 
 // device list of the basic bins in subset `subset` of `nsub` (find_basic_vs_nums_in_subset.cxx:32-70)
@@ -908,11 +924,13 @@ int b200rt_create(const b200rt_geometry* geometry, int device, b200rt_projector*
   }
   auto h = std::make_unique<b200rt_projector>();
   try {
+    // STIR's geometry checks (projection data, image grid, symmetries) run on the host first, so that an invalid
+    // geometry gets STIR's message before any device work
+    h->geo = std::make_unique<Geometry>(*geometry);
     int ndev = 0;
     ck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
     if (device < 0 || device >= ndev) throw std::runtime_error("invalid CUDA device");
     h->device = device;
-    h->geo = std::make_unique<Geometry>(*geometry);
     setup_projector(*h);
   } catch (const std::exception& e) {
     std::lock_guard<std::mutex> lk(g_err_mu);

@@ -7,8 +7,9 @@ the multiplicative factors m and the estimate stay in HBM between sub-iterations
 one fused forward-projection/ratio kernel, one back projection and two elementwise kernels.
 
 Parameters keep STIR's .par names (as keyword arguments): num_subsets, num_subiterations, start_subset_num,
-start_subiteration_num, zero_seg0_end_planes, use_subset_sensitivities, maximum/minimum_relative_change,
-enforce_initial_positivity, prior (QuadraticPrior / RelativeDifferencePrior), MAP_model.
+start_subiteration_num, uniformly_randomise_subset_order (+ subset_order_seed), zero_seg0_end_planes,
+use_subset_sensitivities, maximum/minimum_relative_change, enforce_initial_positivity, prior (QuadraticPrior /
+RelativeDifferencePrior), MAP_model.
 """
 from __future__ import annotations
 
@@ -18,6 +19,7 @@ from typing import Optional
 
 from . import _abi
 from .projectors import RayTracingProjector, _stream_ptr
+from .subsets import SubsetOrder
 
 
 @dataclasses.dataclass
@@ -61,7 +63,8 @@ class OSMAPOSLReconstruction:
                  zero_seg0_end_planes: bool = False, use_subset_sensitivities: bool = True,
                  maximum_relative_change: float = 3.4028234663852886e38, minimum_relative_change: float = 0.0,
                  enforce_initial_positivity: bool = True, prior=None, MAP_model: str = "multiplicative",
-                 back_projection_mode: int = _abi.BACKPROJECT_ATOMIC, stream=None):
+                 back_projection_mode: int = _abi.BACKPROJECT_ATOMIC, stream=None,
+                 uniformly_randomise_subset_order: bool = False, subset_order_seed=None):
         if num_subsets < 1 or num_subsets > projector.geometry.num_views:
             raise ValueError("number of subsets out of range")
         if MAP_model not in ("additive", "multiplicative"):
@@ -82,6 +85,8 @@ class OSMAPOSLReconstruction:
         self.mode = back_projection_mode
         self.stream = stream
         self.subiteration_num = start_subiteration_num
+        self.subset_order = SubsetOrder(num_subsets, start_subset_num, uniformly_randomise_subset_order,
+                                        subset_order_seed)
         self.sensitivities = None
         self.last_num_cancelled = 0
 
@@ -109,8 +114,9 @@ class OSMAPOSLReconstruction:
         return self
 
     def get_subset_num(self):
-        """IterativeReconstruction::get_subset_num (IterativeReconstruction.cxx:628-640), non-random order."""
-        return (self.subiteration_num + self.start_subset_num - 1) % self.num_subsets
+        """IterativeReconstruction::get_subset_num (IterativeReconstruction.cxx:628-640), in order or uniformly
+        randomised (subsets.SubsetOrder)."""
+        return self.subset_order(self.subiteration_num)
 
     def _prior_abi(self):
         return None if self.prior is None else ctypes.byref(self.prior.as_abi(self.map_model))

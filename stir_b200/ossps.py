@@ -12,6 +12,7 @@ import ctypes
 
 from . import _abi
 from .osmaposl import QuadraticPrior, _ptr
+from .subsets import SubsetOrder
 from .projectors import RayTracingProjector, _stream_ptr
 
 
@@ -23,7 +24,8 @@ class OSSPSReconstruction:
                  num_subiterations: int = 1, start_subset_num: int = 0, start_subiteration_num: int = 1,
                  zero_seg0_end_planes: bool = False, relaxation_parameter: float = 1.0, relaxation_gamma: float = 0.1,
                  upper_bound: float = 3.4028234663852886e38, prior=None,
-                 back_projection_mode: int = _abi.BACKPROJECT_ATOMIC, stream=None):
+                 back_projection_mode: int = _abi.BACKPROJECT_ATOMIC, stream=None,
+                 uniformly_randomise_subset_order: bool = False, subset_order_seed=None):
         if prior is not None and not isinstance(prior, QuadraticPrior):
             raise ValueError("OSSPS needs a prior with a parabolic surrogate (QuadraticPrior)")
         if relaxation_parameter <= 0:
@@ -42,6 +44,8 @@ class OSSPSReconstruction:
         self.mode = back_projection_mode
         self.stream = stream
         self.subiteration_num = start_subiteration_num
+        self.subset_order = SubsetOrder(num_subsets, start_subset_num, uniformly_randomise_subset_order,
+                                        subset_order_seed)
         self.denominator = None
         self.sensitivity = None
 
@@ -57,8 +61,9 @@ class OSSPSReconstruction:
         return self
 
     def get_subset_num(self):
-        """IterativeReconstruction::get_subset_num (IterativeReconstruction.cxx:628-640), non-random order."""
-        return (self.subiteration_num + self.start_subset_num - 1) % self.num_subsets
+        """IterativeReconstruction::get_subset_num (IterativeReconstruction.cxx:628-640), in order or uniformly
+        randomised (subsets.SubsetOrder)."""
+        return self.subset_order(self.subiteration_num)
 
     def update_estimate(self, x):
         lib, h = self.proj.lib, self.proj.h

@@ -53,3 +53,44 @@ def views_in_subset(geometry, subset_num: int, num_subsets: int, bits: int = Non
     for v in basic_views_in_subset(nv, bits, subset_num, num_subsets):
         views += related_views(v, nv, bits)
     return sorted(set(views))
+
+
+class SubsetOrder:
+    """IterativeReconstruction::get_subset_num (src/recon_buildblock/IterativeReconstruction.cxx:628-640).
+
+    In order: subset (subiteration_num + start_subset_num - 1) mod num_subsets.  With
+    `uniformly_randomise_subset_order` ("uniformly randomise subset order", :87): a new random permutation of the
+    subsets at the first sub-iteration of every full iteration ((subiteration_num - 1) mod num_subsets == 0), drawn
+    as randomly_permute_subset_order does (:577-600: repeatedly pick one of the remaining subsets uniformly and
+    remove it), and sub-iteration k takes entry (k - 1) mod num_subsets.  STIR seeds rand() with the time
+    (:495-498); `seed` makes the order reproducible (None: seeded from the time, as STIR).  The permutation is
+    made once per full iteration, however often the subset of one sub-iteration is asked for."""
+
+    def __init__(self, num_subsets: int, start_subset_num: int = 0, uniformly_randomise_subset_order: bool = False,
+                 seed=None):
+        import random
+        import time
+        self.num_subsets = num_subsets
+        self.start_subset_num = start_subset_num
+        self.randomise = bool(uniformly_randomise_subset_order)
+        self._rng = random.Random(int(time.time()) if seed is None else seed)
+        self._perm = None
+        self._perm_iteration = None
+
+    def randomly_permute_subset_order(self):
+        remaining = list(range(self.num_subsets))
+        out = []
+        for i in range(self.num_subsets):
+            index = int(self._rng.random() * (self.num_subsets - i))
+            index = min(index, self.num_subsets - i - 1)
+            out.append(remaining.pop(index))
+        return out
+
+    def __call__(self, subiteration_num: int) -> int:
+        if not self.randomise:
+            return (subiteration_num + self.start_subset_num - 1) % self.num_subsets
+        iteration = (subiteration_num - 1) // self.num_subsets
+        if self._perm is None or iteration != self._perm_iteration:
+            self._perm = self.randomly_permute_subset_order()
+            self._perm_iteration = iteration
+        return self._perm[(subiteration_num - 1) % self.num_subsets]

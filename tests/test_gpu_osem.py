@@ -193,3 +193,25 @@ def test_numerator_and_apply_equal_subiteration(setup):
         u = b.numerator(x2, sub, 6)
         b.apply(x2, u, rec.sensitivities[sub], 6, it, min_rel=0.2, max_rel=5.0)
         assert torch.equal(x1, x2)
+
+
+def test_randomised_subset_order_matches_oracle(setup):
+    """"uniformly randomise subset order": the GPU reconstruction visits a new permutation of the 6 subsets each
+    full iteration; the oracle, given the same sequence, reaches the same image (12 sub-iterations)."""
+    from stir_b200.osmaposl import OSMAPOSLReconstruction
+    s = setup
+    rec = OSMAPOSLReconstruction(s["proj"], s["dev_pd"](s["y"]), additive=s["dev_pd"](s["add"]), num_subsets=6,
+                                 num_subiterations=12, uniformly_randomise_subset_order=True, subset_order_seed=11,
+                                 minimum_relative_change=0.2, maximum_relative_change=5.0).set_up()
+    x = s["dev_img"](np.ones(s["img"].shape, np.float32))
+    xo = np.ones(s["img"].shape, np.float32)
+    seq = []
+    for it in range(1, 13):
+        rec.subiteration_num = it
+        sub = rec.get_subset_num()
+        seq.append(sub)
+        rec.update_estimate(x)
+        sens = s["host_img"](rec.sensitivities[sub])
+        xo, _ = s["orc"].osmaposl_update(xo, s["y"], s["add"], sens, sub, 6, it, min_rel=0.2, max_rel=5.0)
+    assert sorted(seq[:6]) == sorted(seq[6:]) == list(range(6)) and seq[:6] != list(range(6))
+    assert rel_l2(s["host_img"](x), xo) <= OSEM_TOL

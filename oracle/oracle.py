@@ -52,6 +52,8 @@ def _load():
         "or_sensitivity_f32": (_I, [_P, _P, _P, _I, _I, _I, _I]),
         "or_osmaposl_update_f32": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F, _I,
                                         ctypes.POINTER(_I)]),
+        "or_sensitivity_f64": (_I, [_P, _P, _P, _I, _I, _I, _I]),
+        "or_osmaposl_update_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(_abi.Prior), _D, _D, _I]),
         "or_log_likelihood_f32": (_D, [_P, _P, _P, _P, _P, _I, _I, _I, _I]),
         "or_osmaposl_numerator_f32": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(_I)]),
         "or_osmaposl_apply_f32": (_I, [_P, _P, _P, _P, _I, _I, ctypes.POINTER(_abi.Prior), _P, _F, _F]),
@@ -163,14 +165,30 @@ class Oracle:
 
     def sensitivity(self, mult=None, subset=0, nsub=1, zero_seg0_end_planes=False, nthreads=None):
         m = None if mult is None else np.ascontiguousarray(mult, np.float32).ravel()
-        img = np.zeros(self.image_shape, np.float32)
-        if lib().or_sensitivity_f32(self.h, _ptr(m), _ptr(img), subset, nsub, int(zero_seg0_end_planes),
+        img = np.zeros(self.image_shape, self.dtype)
+        f = lib().or_sensitivity_f64 if self.precision == 64 else lib().or_sensitivity_f32
+        if f(self.h, _ptr(m), _ptr(img), subset, nsub, int(zero_seg0_end_planes),
                                     nthreads or default_threads()) != 0:
             raise RuntimeError("oracle sensitivity failed")
         return img
 
     def osmaposl_update(self, estimate, y, additive, sens, subset, nsub, subiteration_num, prior=None, kappa=None,
                         min_rel=0.0, max_rel=1e37, zero_seg0_end_planes=False, nthreads=None):
+        """One OSMAPOSL sub-iteration; returns (estimate, number of cancelled ratios).  A precision-64 oracle runs
+        the FP64 restatement (no kappa; the cancelled count is not reported: -1)."""
+        if self.precision == 64:
+            x = np.ascontiguousarray(estimate, np.float64).copy().reshape(self.image_shape)
+            y = np.ascontiguousarray(y, np.float32).ravel()
+            a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()
+            s = np.ascontiguousarray(sens, np.float64).ravel()
+            p = prior if prior is not None else _abi.Prior(type=_abi.PRIOR_NONE)
+            if kappa is not None:
+                raise ValueError("the FP64 OSMAPOSL restatement has no kappa")
+            if lib().or_osmaposl_update_f64(self.h, _ptr(x), _ptr(y), _ptr(a), _ptr(s), subset, nsub, subiteration_num,
+                                            int(zero_seg0_end_planes), ctypes.byref(p), float(min_rel), float(max_rel),
+                                            nthreads or default_threads()) != 0:
+                raise RuntimeError("oracle FP64 OSMAPOSL update failed")
+            return x, -1
         x = np.ascontiguousarray(estimate, np.float32).copy().reshape(self.image_shape)
         y = np.ascontiguousarray(y, np.float32).ravel()
         a = None if additive is None else np.ascontiguousarray(additive, np.float32).ravel()

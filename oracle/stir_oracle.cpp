@@ -970,7 +970,7 @@ template <typename T> struct Handle : HandleBase {
 const float SMALL_NUM = 0.000001F; /* recon_array_functions.cxx:44 */
 
 /* divide_and_truncate (recon_array_functions.cxx:171-266) for one viewgram [ax][tang] of a (seg,view) */
-template <typename Fn> void for_viewgram(const Geometry<float>& g, int seg, int view, int tof, Fn fn) {
+template <typename T, typename Fn> void for_viewgram(const Geometry<T>& g, int seg, int view, int tof, Fn fn) {
   for (int a = 0; a < g.nax(seg); ++a)
     for (int t = g.min_tang; t <= g.max_tang; ++t) fn(a, t, g.stir_index(seg, view, a, t, tof));
 }
@@ -1388,6 +1388,135 @@ int or_osmaposl_update_f32(or_handle* h, float* x, const float* y, const float* 
   std::vector<float> u(ni, 0.f);
   if (or_osmaposl_numerator_f32(h, x, y, add, subset, nsub, zero_ends, nthreads, u.data(), num_cancelled) != 0) return -1;
   return or_osmaposl_apply_f32(h, x, u.data(), sens, nsub, subiter, prior, kappa, min_rel, max_rel);
+}
+
+/* ---------------------------------------------------------------------------
+ * FP64 OSMAPOSL: the same algorithm as the float path above, every quantity in double (the data y, a and m are
+ * float inputs, converted once).  It is the "error against an FP64 oracle" reference; the float path is the
+ * parity reference.
+ * ------------------------------------------------------------------------- */
+static void zero_seg0_ends_f64(const Geometry<double>& g, double* pd) {
+  for (int k = g.min_tof; k <= g.max_tof; ++k)
+    for (int view = 0; view < g.num_views; ++view)
+      for (int t = g.min_tang; t <= g.max_tang; ++t) {
+        pd[g.stir_index(0, view, 0, t, k)] = 0;
+        pd[g.stir_index(0, view, g.nax(0) - 1, t, k)] = 0;
+      }
+}
+
+int or_sensitivity_f64(or_handle* h, const float* mult, double* sens, int subset, int nsub, int zero_ends,
+                       int nthreads) {
+  if (!h->d) return -1;
+  try {
+    const auto& g = h->d->g;
+    std::vector<double> m(g.projdata_size, 1.0);
+    if (mult) std::copy(mult, mult + g.projdata_size, m.begin());
+    if (zero_ends) zero_seg0_ends_f64(g, m.data());
+    h->d->back(m.data(), sens, subset, nsub, nthreads);
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "oracle: %s\n", e.what());
+    return -1;
+  }
+}
+
+/* RelativeDifferencePrior::derivative_10 (RelativeDifferencePrior.cxx:287-300) in double */
+static double rdp_derivative_10_f64(double x, double y, double gamma, double epsilon) {
+  if (epsilon == 0.0 && x == 0 && y == 0) return 0.;
+  const double d = x + y + gamma * std::abs(x - y) + epsilon;
+  return (x - y) * (gamma * std::abs(x - y) + x + 3 * y + 2 * epsilon) / (d * d);
+}
+
+/* QuadraticPrior / RelativeDifferencePrior compute_gradient (QuadraticPrior.cxx:303-372,
+   RelativeDifferencePrior.cxx:376-452) in double */
+static void prior_gradient_f64(const b200rt_prior& p, const double* img, int nz, int ny, int nx, double vz, double vy,
+                               double vx, double* grad) {
+  const int64_t ni = static_cast<int64_t>(nz) * ny * nx;
+  if (p.type == B200RT_PRIOR_NONE || p.penalisation_factor == 0) {
+    std::fill(grad, grad + ni, 0.);
+    return;
+  }
+  double w[3][3][3];
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x)
+        w[z + 1][y + 1][x + 1] = ((p.only_2D && z != 0) || (z == 0 && y == 0 && x == 0))
+                                     ? 0.
+                                     : vx / std::sqrt(square(x * vx) + square(y * vy) + square(z * vz));
+  const int dzmin = p.only_2D ? 0 : -1, dzmax = p.only_2D ? 0 : 1;
+  auto at = [&](int z, int y, int x) { return (static_cast<int64_t>(z) * ny + y) * nx + x; };
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const double xc = img[at(z, y, x)];
+        double gsum = 0.;
+        for (int dz = std::max(dzmin, -z); dz <= std::min(dzmax, nz - 1 - z); ++dz)
+          for (int dy = std::max(-1, -y); dy <= std::min(1, ny - 1 - y); ++dy)
+            for (int dx = std::max(-1, -x); dx <= std::min(1, nx - 1 - x); ++dx) {
+              const double xn = img[at(z + dz, y + dy, x + dx)];
+              const double wt = w[dz + 1][dy + 1][dx + 1];
+              gsum += p.type == B200RT_PRIOR_QUADRATIC ? wt * (xc - xn)
+                                                       : wt * rdp_derivative_10_f64(xc, xn, p.gamma, p.epsilon);
+            }
+        grad[at(z, y, x)] = gsum * p.penalisation_factor;
+      }
+}
+
+/* one OSMAPOSL sub-iteration (or_osmaposl_update_f32's steps) in double; no kappa */
+int or_osmaposl_update_f64(or_handle* h, double* x, const float* y, const float* add, const double* sens, int subset,
+                           int nsub, int subiter, int zero_ends, const b200rt_prior* prior, double min_rel,
+                           double max_rel, int nthreads) {
+  if (!h->d) return -1;
+  try {
+    auto& H = *h->d;
+    auto& g = H.g;
+    const int64_t ni = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+    std::vector<double> est(g.projdata_size, 0.), ratio(g.projdata_size, 0.), u(ni, 0.);
+    H.forward(x, est.data(), subset, nsub, nthreads);
+    for (const auto& b : basic_vs_in_subset(g, subset, nsub))
+      for (int k = g.min_tof; k <= g.max_tof; ++k) {
+        std::vector<std::pair<int, int>> rel;
+        related_vs(g, b.first, b.second, rel);
+        for (const auto& r : rel) {
+          const int seg = r.second, view = r.first;
+          const bool zero_this = zero_ends && seg == 0;
+          auto end = [&](int a) { return zero_this && (a == 0 || a == g.nax(0) - 1); };
+          double vmax = -std::numeric_limits<double>::infinity();
+          for_viewgram(g, seg, view, k, [&](int a, int, int64_t i) { vmax = std::max(vmax, end(a) ? 0. : double(y[i])); });
+          const double small_value = std::max(vmax * 0.000001, 0.);
+          for_viewgram(g, seg, view, k, [&](int a, int, int64_t i) {
+            const double num = end(a) ? 0. : double(y[i]);
+            const double denom = est[i] + (add && !end(a) ? double(add[i]) : 0.);
+            ratio[i] = num <= small_value ? 0. : (num > 10000. * denom ? 10000. : num / denom);
+          });
+        }
+      }
+    H.back(ratio.data(), u.data(), subset, nsub, nthreads);
+    const bool no_prior = !prior || prior->type == B200RT_PRIOR_NONE || prior->penalisation_factor == 0;
+    std::vector<double> den(sens, sens + ni);
+    double small_num = 0.;
+    if (!no_prior) {
+      prior_gradient_f64(*prior, x, g.nz, g.ny, g.nx, g.d.voxel_size_z, g.d.voxel_size_y, g.d.voxel_size_x, den.data());
+      for (int64_t i = 0; i < ni; ++i) {
+        if (prior->map_model == B200RT_MAP_ADDITIVE)
+          den[i] = std::max(std::min(den[i] / nsub + sens[i], sens[i] * 10), sens[i] / 10);
+        else
+          den[i] = std::max(std::min(den[i] + 1, 10.), 0.1) * sens[i];
+      }
+      small_num = 0.000001;
+    }
+    const double small_value = std::max(*std::max_element(u.begin(), u.end()) * small_num, 0.);
+    for (int64_t i = 0; i < ni; ++i) {
+      double v = (std::fabs(den[i]) <= small_value && std::fabs(u[i]) <= small_value) ? 0. : u[i] / den[i];
+      if (subiter != 1) v = v > max_rel ? max_rel : (min_rel > v ? min_rel : v);
+      x[i] *= v;
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "oracle: %s\n", e.what());
+    return -1;
+  }
 }
 
 /* sub-gradient of the log-likelihood without penalty: A^T [divide_and_truncate(y, A x + a) - m]

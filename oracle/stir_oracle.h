@@ -57,6 +57,12 @@ int or_sensitivity_f32(or_handle* h, const float* mult, float* sens, int subset,
 
 /* One OSMAPOSL sub-iteration (OSMAPOSLReconstruction.cxx:371-516) on `estimate` (in/out).
    additive may be NULL.  sens is the sensitivity used for this subset. */
+/* FP64 restatement of the sensitivity and of one OSMAPOSL sub-iteration (no kappa) on a precision-64 handle */
+int or_sensitivity_f64(or_handle* h, const float* mult, double* sens, int subset, int nsub, int zero_seg0_end_planes,
+                       int nthreads);
+int or_osmaposl_update_f64(or_handle* h, double* estimate, const float* y, const float* additive, const double* sens,
+                           int subset, int nsub, int subiteration_num, int zero_seg0_end_planes, const b200rt_prior* prior,
+                           double min_rel, double max_rel, int nthreads);
 int or_osmaposl_update_f32(or_handle* h, float* estimate, const float* y, const float* additive, const float* sens,
                            int subset, int nsub, int subiteration_num, int zero_seg0_end_planes,
                            const b200rt_prior* prior, const float* kappa, float min_rel, float max_rel, int nthreads,

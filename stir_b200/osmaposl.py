@@ -64,7 +64,8 @@ class OSMAPOSLReconstruction:
                  maximum_relative_change: float = 3.4028234663852886e38, minimum_relative_change: float = 0.0,
                  enforce_initial_positivity: bool = True, prior=None, MAP_model: str = "multiplicative",
                  back_projection_mode: int = _abi.BACKPROJECT_ATOMIC, stream=None,
-                 uniformly_randomise_subset_order: bool = False, subset_order_seed=None):
+                 uniformly_randomise_subset_order: bool = False, subset_order_seed=None,
+                 use_tofsens: bool = False, sensitivity_mult=None):
         if num_subsets < 1 or num_subsets > projector.geometry.num_views:
             raise ValueError("number of subsets out of range")
         if MAP_model not in ("additive", "multiplicative"):
@@ -89,16 +90,26 @@ class OSMAPOSLReconstruction:
                                         subset_order_seed)
         self.sensitivities = None
         self.last_num_cancelled = 0
+        # TOF data: the sensitivity comes from the non-TOF projector with non-TOF multiplicative factors unless
+        # use_tofsens (PoissonLogLikelihoodWithLinearModelForMeanAndProjData.cxx:642-670)
+        self.use_tofsens = bool(use_tofsens)
+        self.sensitivity_mult = sensitivity_mult
+        if projector.info.num_tof_bins > 1 and not use_tofsens and mult is not None and sensitivity_mult is None:
+            raise ValueError("TOF data with multiplicative factors: give their non-TOF factors as sensitivity_mult "
+                             "(or set use_tofsens)")
 
     # PoissonLogLikelihoodWithLinearModelForMean::compute_sensitivities / set_total_or_subset_sensitivities
     # (PoissonLogLikelihoodWithLinearModelForMean.cxx:372-455)
     def set_up(self):
         import torch
-        lib, h = self.proj.lib, self.proj.h
+        tof = self.proj.info.num_tof_bins > 1
+        sp = self.proj if (self.use_tofsens or not tof) else self.proj.non_tof_projector()
+        mult = self.mult if sp is self.proj else self.sensitivity_mult
+        lib, h = sp.lib, sp.h
         subs = []
         for s in range(self.num_subsets):
-            t = self.proj.empty_image(zero=False)
-            _abi.check(lib.b200rt_sensitivity_dev(h, _ptr(self.mult), _ptr(t), s, self.num_subsets,
+            t = sp.empty_image(zero=False)
+            _abi.check(lib.b200rt_sensitivity_dev(h, _ptr(mult), _ptr(t), s, self.num_subsets,
                                                   int(self.zero_seg0_end_planes), self.mode, _stream_ptr(self.stream)), h,
                        "b200rt_sensitivity_dev")
             subs.append(t)

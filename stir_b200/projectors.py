@@ -19,7 +19,7 @@ from typing import Optional
 import numpy as np
 
 from . import _abi
-from .geometry import ImageGeometry, ProjDataInfo, make_geometry
+from .geometry import ImageGeometry, ProjDataInfo, make_geometry, non_tof
 
 
 def _np_ptr(a: np.ndarray):
@@ -55,6 +55,19 @@ class RayTracingProjector:
         info = _abi.Info()
         _abi.check(self.lib.b200rt_get_info(self.h, ctypes.byref(info)), self.h, "b200rt_get_info")
         self.info = info
+        self._non_tof = None
+
+    def non_tof_projector(self) -> "RayTracingProjector":
+        """This projector without timing bins (ProjDataInfo::create_non_tof_clone, the same matrix settings); itself
+        for non-TOF data.  STIR back-projects a TOF reconstruction's sensitivity with it unless "use time-of-flight
+        sensitivities" is set (PoissonLogLikelihoodWithLinearModelForMeanAndProjData.cxx:642-670).  Made once."""
+        if self.info.num_tof_bins <= 1:
+            return self
+        if self._non_tof is None:
+            g = _abi.Geometry.from_buffer_copy(self.geometry)
+            g.tof_mash_factor = 0
+            self._non_tof = RayTracingProjector(non_tof(self.proj_data_info), self.image, device=self.device, geometry=g)
+        return self._non_tof
 
     def close(self):
         if getattr(self, "h", None):

@@ -36,11 +36,15 @@ def _attenuation_factors(proj, mu):
 
 
 def _poisson(mean, total, seed):
+    """Poisson counts with about `total` events in all, returned in the units of `mean` (counts / scale), and
+    the number of events."""
     import torch
     g = torch.Generator(device=mean.device)
     g.manual_seed(seed)
     scale = float(total) / float(mean.double().sum())
-    return torch.poisson(mean * scale, generator=g).div_(scale)
+    n = torch.poisson(mean * scale, generator=g)
+    events = float(n.double().sum())
+    return n.div_(scale), events
 
 
 def small_3d_pet_data(proj, counts=5e6):
@@ -50,8 +54,8 @@ def small_3d_pet_data(proj, counts=5e6):
     m = _attenuation_factors(proj, mu)
     ybar = m * proj.forward_dev(_dev_img(proj, xt))
     b = 0.1 * float(ybar.double().mean())
-    y = _poisson(ybar + b, counts, 2)
-    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m)
+    y, events = _poisson(ybar + b, counts, 2)
+    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m, events=events)
 
 
 def clinical_data(proj, counts=3e8, seed=4):
@@ -73,9 +77,9 @@ def clinical_data(proj, counts=3e8, seed=4):
     w = torch.from_numpy(np.exp(-0.5 * (t / (nt / 6.0)) ** 2).astype(np.float32)).to(m.device)
     prof = _tangential_profile(proj, w)
     b = prof * (0.3 * float(ybar.double().mean()) / float(prof.double().mean()))
-    y = _poisson(ybar + b, counts, seed + 1)
+    y, events = _poisson(ybar + b, counts, seed + 1)
     del ybar
-    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m)
+    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m, events=events)
 
 
 def _tangential_profile(proj, w):
@@ -106,8 +110,8 @@ def tof_data(proj, counts=3e8):
     m = m_nt.repeat(ntof)  # every timing bin of a LOR has the LOR's attenuation
     ybar = m * proj.forward_dev(_dev_img(proj, xt))
     b = 0.1 * float(ybar.double().mean())
-    y = _poisson(ybar + b, counts, 2)
-    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m, sensitivity_mult=m_nt)
+    y, events = _poisson(ybar + b, counts, 2)
+    return dict(x_true=xt, mu=mu, y=y, additive=b / m, mult=m, sensitivity_mult=m_nt, events=events)
 
 
 def dynamic_frames(projs, device, seed=3):

@@ -272,7 +272,7 @@ def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5)
         data.append((y, torch.full_like(y, bg)))
     n = nsub * iterations
     objs = [OSMAPOSLReconstruction(proj, y, additive=a, num_subsets=nsub, num_subiterations=n,
-                                   prior=QuadraticPrior(beta)).set_up() for y, a in data]
+                                   prior=QuadraticPrior(beta), use_tofsens=True).set_up() for y, a in data]
     xs = [proj.empty_image() for _ in objs]
 
     def per_frame():
@@ -289,7 +289,8 @@ def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5)
     batch = BatchedOSMAPOSL()
     bx = []
     for (y, a), r0 in zip(data, objs):
-        r = OSMAPOSLReconstruction(proj, y, additive=a, num_subsets=nsub, num_subiterations=n, prior=QuadraticPrior(beta))
+        r = OSMAPOSLReconstruction(proj, y, additive=a, num_subsets=nsub, num_subiterations=n, prior=QuadraticPrior(beta),
+                                   use_tofsens=True)
         r.sensitivities = r0.sensitivities
         x = proj.empty_image().fill_(1.0)
         batch.add(r, x)

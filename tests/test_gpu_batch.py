@@ -178,7 +178,8 @@ def test_batch_tof_frames_equal_frame_by_frame(cuda_device):
         scale = (1e6 * (k + 1)) / float((ybar + bg).sum())
         y = torch.from_numpy(rng.poisson(((ybar + bg) * scale).cpu().numpy()).astype(np.float32) / np.float32(scale)).cuda()
         add = torch.full_like(y, bg)
-        ref = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n, prior=prior)
+        ref = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n, prior=prior,
+                                     use_tofsens=True)
         xr = proj.empty_image().fill_(1.0)
         ref.reconstruct(xr)
         rec = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n, prior=prior)

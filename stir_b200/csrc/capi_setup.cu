@@ -60,7 +60,8 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
         }
         std::sort(keys.begin(), keys.end());
         keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-        if (keys.size() > 65535) {
+        // column slots and basic segments must fit the packed elements (16 and 5 bits)
+        if (keys.size() > 65535 || nsegs > 32) {
           G.ok = false;
           continue;
         }
@@ -110,7 +111,8 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
             const size_t end = si + 1 < nsegs ? static_cast<size_t>(G.member_off[si + 1]) : G.elems.size();
             while (cur[si] < end && static_cast<int>(G.elems[cur[si]].sz & 0xffffu) == slot) {
               const PathElem& e = G.elems[cur[si]];
-              G.cmaj.push_back(PathCElem{(e.sz >> 16) | (static_cast<uint32_t>(si) << 16), e.v});
+              G.cmaj.push_back(PathCElem{(e.sz >> 16) | (static_cast<uint32_t>(si) << 11) |
+                                             (static_cast<uint32_t>(slot) << 16), e.v});
               ++cur[si];
             }
           }

@@ -153,7 +153,8 @@ struct PathItemDev {
   int col_starts;               // the path's column table in col_starts[] (ncols + 1 entries)
   int64_t cmaj_off;             // the path's elements in column order in cmaj[]
 };
-// A path element in column order: z + 512 (bits 0..15), the member (bits 16..31), the value.
+// A path element in column order: z + 512 (bits 0..10), the member (bits 11..15), the column slot (bits 16..31),
+// the value.
 struct __align__(8) PathCElem {
   uint32_t mz;
   float v;

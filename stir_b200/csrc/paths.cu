@@ -361,99 +361,122 @@ struct FixedCols {
   }
 };
 
-// Groups of 32 planes outside an (element, line) window hold only the zero padding of the line data, so the
-// window-aware back projection skips their loads: a load whose predicate is off for the whole warp moves no
-// shared-memory data.  The skipped terms are zeros, so the sums are the same bit for bit.
-constexpr bool kBackSkipOutsideWindow = false;
-
-__device__ __forceinline__ float ld_shared_if(const float* p, unsigned pred) {
-  float v = 0.f;
-  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
-  asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.shared.f32 %0, [%1];\n\t}" : "+f"(v) : "r"(a), "r"(pred));
-  return v;
+// image offset of column `slot` of the item's path under its symmetry operation (-1 outside the image)
+__device__ __forceinline__ int column_base(const ProjParams& p, const PathParams& pp, const PathItemDev& it, int slot) {
+  const uint32_t pk = __ldg(pp.cols + it.col_offset + slot);
+  const int x = static_cast<int>(pk & 2047u) - 1024;
+  const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
+  const int swap = it.flags & 1;
+  const int xi = (swap ? y : x) * ((it.flags & 2) ? -1 : 1) - p.min_x;
+  const int yi = (swap ? x : y) * ((it.flags & 4) ? -1 : 1) - p.min_y;
+  return (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * p.nz : -1;
 }
 
-// which of the 4 groups of 32 planes from zp meet the window [zt, zt + len] (bit j: planes zp + 32 j ..)
-__device__ __forceinline__ unsigned window_groups(int zt, int len, int zp) {
-  unsigned m = 0;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) m |= static_cast<unsigned>(zp + 32 * j <= zt + len && zp + 32 * j + 31 >= zt) << j;
-  return m;
-}
-
-// planes [zp, zp + 128) of one column: elements [k0, k1) of the path in column order, when every window of every
-// (element, line) meets the image (checked at set-up, PathParams::zpad >= 0; an inactive line's data are all
-// zero).  The warp's lanes stage 32 elements at a time, each with the data offsets of its basic bin's first two
-// lines (the z orientations) and the groups of planes their windows meet, so that an element costs one
-// 16-byte broadcast read and, per line, the loads and FMAs of the planes alone; further lines of a basic bin
-// (rare) read their line entry.
+// Planes [zp, zp + 128) of the columns whose elements are [e_begin, e_end) of the path in column order, when every
+// window of every (element, line) meets the image (checked at set-up, PathParams::zpad >= 0; an inactive line's
+// data are all zero).  One warp streams through the elements of a contiguous range of columns, 32 at a time: each
+// lane stages one element with the data offsets of its basic bin's first two lines (the z orientations) and
+// whether it starts a new column, so that in the loop an element costs one 16-byte broadcast read and, per line,
+// the plane loads and FMAs; the column's sums are added to the image when the next column starts.  Further lines
+// of a basic bin (rare) read their line entries.
 template <typename Cols>
-__device__ __forceinline__ void back_column_hit(const PathCElem* __restrict__ E, int k0, int k1, const int4* lz,
-                                                const int2* members, const float* dl, int zp, int nz, int lane, int b,
-                                                const Cols& acc, int4* eb) {
+__device__ __forceinline__ void back_span(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+                                          const PathCElem* __restrict__ E, int e_begin, int e_end, const int4* lz,
+                                          const int2* members, const float* dl, int zp, int lane, const Cols& acc,
+                                          int4* eb) {
+  const int nz = p.nz;
   typename Cols::T sum[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) sum[j] = typename Cols::T(0);
-  auto line = [&](float v, int off, unsigned groups) {
+  int b = -1;          // image offset of the current column
+  int prev_slot = -1;  // column of the last element staged
+  auto flush = [&]() {
+    if (b >= 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int z = zp + 32 * j + lane;
+        if (z < nz) acc.flush(static_cast<int64_t>(b) + z, sum[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sum[j] = typename Cols::T(0);
+  };
+  auto line = [&](float v, int off) {
     const float* q = dl + (off + lane);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float t = kBackSkipOutsideWindow ? ld_shared_if(q + 32 * j, (groups >> j) & 1u) : q[32 * j];
-      sum[j] += acc.term(v * t);
-    }
+    for (int j = 0; j < 4; ++j) sum[j] += acc.term(v * q[32 * j]);
   };
-  for (int kb = k0; kb < k1; kb += 32) {
-    const int cnt = min(32, k1 - kb);
+  for (int kb = e_begin; kb < e_end; kb += 32) {
+    const int cnt = min(32, e_end - kb);
     __syncwarp();
+    int slot = -1, off1 = 0, off2 = 0, nlines = 0;
+    float v = 0.f;
     if (lane < cnt) {
-      // (value, data offset of line 1, of line 2, lines | groups of line 1 << 5 | of line 2 << 9 | first line << 13
-      //  | z + 512 << 21); a basic bin has fewer than 32 lines in an item, an item fewer than 256 lines, and
-      //  z + 512 < 2048 (10 bits in the rows)
       const PathCElem e = E[kb + lane];
-      const int zr = static_cast<int>(e.mz & 0xffffu);
-      const int2 mem = members[e.mz >> 16];
-      int off1 = 0, off2 = 0;
-      unsigned g1 = 0, g2 = 0;
+      const int zr = static_cast<int>(e.mz & 2047u);
+      const int2 mem = members[(e.mz >> 11) & 31u];
+      slot = static_cast<int>(e.mz >> 16);
+      v = e.v;
+      nlines = mem.y;
       if (mem.y > 0) {
         const int4 L = lz[mem.x];
-        const int zt = L.x * zr + L.y;
-        off1 = L.w + zp - zt;
-        g1 = window_groups(zt, L.z, zp);
+        off1 = L.w + zp - (L.x * zr + L.y);
       }
       if (mem.y > 1) {
         const int4 L = lz[mem.x + 1];
-        const int zt = L.x * zr + L.y;
-        off2 = L.w + zp - zt;
-        g2 = window_groups(zt, L.z, zp);
+        off2 = L.w + zp - (L.x * zr + L.y);
       }
-      const unsigned pk = static_cast<unsigned>(mem.y) | (g1 << 5) | (g2 << 9) | (static_cast<unsigned>(mem.x) << 13) |
-                          (static_cast<unsigned>(zr) << 21);
-      eb[lane] = make_int4(__float_as_int(e.v), off1, off2, static_cast<int>(pk));
+    }
+    const int up = __shfl_up_sync(0xffffffffu, slot, 1);
+    const int prev = lane == 0 ? prev_slot : up;
+    prev_slot = __shfl_sync(0xffffffffu, slot, cnt - 1);
+    if (lane < cnt) {
+      // (value, data offset of line 1, of line 2, min(lines, 3) | new column << 2 | column << 3)
+      const unsigned pk = static_cast<unsigned>(min(nlines, 3)) | (static_cast<unsigned>(slot != prev) << 2) |
+                          (static_cast<unsigned>(slot) << 3);
+      eb[lane] = make_int4(__float_as_int(v), off1, off2, static_cast<int>(pk));
     }
     __syncwarp();
     for (int i = 0; i < cnt; ++i) {
       const int4 w = eb[i];
-      const float v = __int_as_float(w.x);
       const unsigned pk = static_cast<unsigned>(w.w);
-      const unsigned n = pk & 31u;
-      if (n > 0) line(v, w.y, (pk >> 5) & 15u);
-      if (n > 1) line(v, w.z, (pk >> 9) & 15u);
-      if (n > 2) {
-        const int first = static_cast<int>((pk >> 13) & 255u), zr = static_cast<int>(pk >> 21);
-        for (int l = first + 2; l < first + static_cast<int>(n); ++l) {
-          const int4 L = lz[l];
-          const int zt = L.x * zr + L.y;
-          line(v, L.w + zp - zt, window_groups(zt, L.z, zp));
+      if (pk & 4u) {
+        flush();
+        b = column_base(p, pp, it, static_cast<int>(pk >> 3));
+      }
+      const float ev = __int_as_float(w.x);
+      const unsigned n = pk & 3u;
+      if (n >= 2) {
+        line(ev, w.y);
+        line(ev, w.z);
+        if (n == 3) {
+          const PathCElem e = E[kb + i];
+          const int zr = static_cast<int>(e.mz & 2047u);
+          const int2 mem = members[(e.mz >> 11) & 31u];
+          for (int l = mem.x + 2; l < mem.x + mem.y; ++l) {
+            const int4 L = lz[l];
+            line(ev, L.w + zp - (L.x * zr + L.y));
+          }
         }
+      } else if (n == 1) {
+        line(ev, w.y);
       }
     }
   }
-  if (b < 0) return;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int z = zp + 32 * j + lane;
-    if (z < nz) acc.flush(static_cast<int64_t>(b) + z, sum[j]);
+  flush();
+}
+
+// the first element of the first column that starts at or after element t (col_starts cs, ncols + 1 entries)
+__device__ __forceinline__ int column_boundary(const int* cs, int ncols, int t) {
+  int lo = 0, hi = ncols;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(cs + mid) < t)
+      lo = mid + 1;
+    else
+      hi = mid;
   }
+  return __ldg(cs + lo);
 }
 
 // the same where a window may miss the image (PathParams::zpad < 0): such (element, line) pairs read the zero
@@ -487,8 +510,8 @@ __device__ __forceinline__ void back_column(const PathCElem* __restrict__ E, int
     __syncwarp();
     if (lane < cnt) {
       const PathCElem e = E[kb + lane];
-      const int2 mem = members[e.mz >> 16];
-      eb[lane] = make_int4(static_cast<int>(e.mz & 0xffffu), __float_as_int(e.v), mem.x, mem.y);
+      const int2 mem = members[(e.mz >> 11) & 31u];
+      eb[lane] = make_int4(static_cast<int>(e.mz & 2047u), __float_as_int(e.v), mem.x, mem.y);
     }
     __syncwarp();
     for (int i = 0; i < cnt; ++i) {
@@ -548,30 +571,20 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
     }
   }
   __syncthreads();
-  const int swap = it.flags & 1;
-  const int sx = (it.flags & 2) ? -1 : 1;
-  const int sy = (it.flags & 4) ? -1 : 1;
   const PathCElem* E = pp.cmaj + it.cmaj_off;
   const int* cs = pp.col_starts + it.col_starts;
-  // the packed staging of back_column_hit holds line indices below 256, member line counts below 32 and z + 512
-  // below 2048
-  const bool hit_packed = pp.zpad >= 0 && pp.max_lines < 32 && nz + 512 < 2048;
+  if (pp.zpad >= 0) {
+    // every window meets the image: each warp streams through an equal share of the elements, cut at columns
+    const int ne = __ldg(cs + it.ncols);
+    const int e0 = column_boundary(cs, it.ncols, static_cast<int>(static_cast<int64_t>(ne) * warp / kPathWarps));
+    const int e1 = column_boundary(cs, it.ncols, static_cast<int>(static_cast<int64_t>(ne) * (warp + 1) / kPathWarps));
+    for (int zp = 0; zp < nz; zp += 128) back_span<Cols>(p, pp, it, E, e0, e1, lz, members, dl, zp, lane, acc, eb);
+    return;
+  }
   for (int ci = warp; ci < it.ncols; ci += kPathWarps) {
-    const uint32_t pk = pp.cols[it.col_offset + ci];
-    const int x = static_cast<int>(pk & 2047u) - 1024;
-    const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
-    const int xi = (swap ? y : x) * sx - p.min_x;
-    const int yi = (swap ? x : y) * sy - p.min_y;
-    const int b = (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * nz : -1;
+    const int b = column_base(p, pp, it, ci);
     const int k0 = __ldg(cs + ci), k1 = __ldg(cs + ci + 1);
-    for (int zp = 0; zp < nz; zp += 128) {
-      if (hit_packed)
-        back_column_hit<Cols>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
-      else if (pp.zpad >= 0)
-        back_column<Cols, true>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
-      else
-        back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
-    }
+    for (int zp = 0; zp < nz; zp += 128) back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
   }
 }
 

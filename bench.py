@@ -245,11 +245,51 @@ def listmode_and_priors(proj, pdi, img, xd, cpu_ref):
         dt = time.perf_counter() - t0
         pr["cpu_baseline"] = {"value": slab.size / dt, "unit": "voxels/s", "cores": 1, "kind": "port",
                               "sample": "16 planes of the image, the oracle's GibbsPenalty::compute_gradient loop"}
+    pr["reference_cuda"] = reference_cuda_priors(p, shape, vox, proj.device)
     out["gibbs_rdp_gradient"] = pr
     del p
     torch.cuda.empty_cache()
     out["tof"] = tof_workload(cpu_ref is not None, proj.device)
     return out
+
+
+def reference_cuda_priors(p_dev_layout, shape, vox, device):
+    """The same gradient by STIR's own CUDA kernels built for this GPU (oracle/_ref: CudaGibbsPenalty's gradient
+    kernel with the Relative Difference potential, and CudaRelativeDifferencePrior's), against the B200 kernels in
+    both arithmetics, all on one device image in STIR's [z][y][x] order (the reference's layout), no host copies.
+    A baseline leg: the reference's kernels are timed, not used."""
+    import ctypes
+    import torch
+    from oracle import oracle as O
+    from stir_b200 import _abi, gibbs
+    if not O.ref_cuda_priors_available():
+        return {"unavailable": "STIR's CUDA prior kernels were not built (oracle/_ref needs the STIR sources)"}
+    ref = O.ref_cuda_priors()
+    g = torch.Generator(device=f"cuda:{device}").manual_seed(9)
+    x = torch.rand(shape, device=f"cuda:{device}", generator=g) + 0.1
+    out = torch.empty_like(x)
+    w = torch.from_numpy(np.ascontiguousarray(O.gibbs_default_weights(vox), np.float32)).to(x.device)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    nz, ny, nx = shape
+    args = (ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(w.data_ptr()))
+    ms_gibbs = time_dev(lambda: ref.ref_cuda_gibbs_gradient(1, *args, 3, 3, 3, None, 0.1, 2.0, 1e-7, nz, ny, nx,
+                                                            -(ny // 2), -(nx // 2), sp))
+    ref_out = out.clone()
+    ms_rdp = time_dev(lambda: ref.ref_cuda_rdp_prior_gradient(*args, None, 2.0, 1e-7, 0.1, nz, ny, nx, sp))
+    res = {"layout": "[z][y][x]", "stir_CudaGibbsPenalty_gradient_ms": ms_gibbs,
+           "stir_CudaRelativeDifferencePrior_gradient_ms": ms_rdp}
+    for name, cls in (("b200_cuda_arithmetic", gibbs.CudaGibbsRelativeDifferencePenalty),
+                      ("b200_host_arithmetic", gibbs.GibbsRelativeDifferencePenalty)):
+        q = cls(penalisation_factor=0.1, gamma=2.0, epsilon=1e-7, device=device)
+        q.set_up(shape, vox, _abi.LAYOUT_STIR)
+        ms = time_dev(lambda: q.compute_gradient(x, out))
+        res[name + "_ms"] = ms
+        if name == "b200_cuda_arithmetic":
+            res["b200_cuda_arithmetic_bit_equal_to_stir_cuda"] = bool(torch.equal(out, ref_out))
+        del q
+    res["speedup_vs_stir_CudaGibbsPenalty"] = ms_gibbs / res["b200_cuda_arithmetic_ms"]
+    res["speedup_vs_stir_CudaRelativeDifferencePrior"] = ms_rdp / res["b200_host_arithmetic_ms"]
+    return res
 
 
 def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5):

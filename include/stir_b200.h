@@ -513,6 +513,16 @@ typedef struct b200rt_gibbs b200rt_gibbs;
 int b200rt_gibbs_create(const b200rt_gibbs_params* params, int device, b200rt_gibbs** out);
 void b200rt_gibbs_destroy(b200rt_gibbs* g);
 const char* b200rt_gibbs_last_error(const b200rt_gibbs* g);
+
+/* Arithmetic of the gradient (b200rt_gibbs_gradient_dev).  B200RT_GIBBS_ARITH_HOST (the default): GibbsPenalty.inl's
+ * host loop, a double sum per voxel (src/include/stir/recon_buildblock/GibbsPenalty.inl).  B200RT_GIBBS_ARITH_CUDA:
+ * STIR's CUDA build, a float sum per voxel over the whole neighbourhood and the float product weight x derivative
+ * per term (CudaGibbsPenalty_gradient_kernel, src/include/stir/recon_buildblock/CUDA/CudaGibbsPenalty.cuh:141-206),
+ * the drop-in arithmetic for CudaGibbsQuadraticPenalty / CudaGibbsRelativeDifferencePenalty.  The other operations
+ * keep the host arithmetic. */
+#define B200RT_GIBBS_ARITH_HOST 0
+#define B200RT_GIBBS_ARITH_CUDA 1
+int b200rt_gibbs_set_arithmetic(b200rt_gibbs* g, int arithmetic);
 /* get_weights: sizes[3] = (z, y, x); w receives sizes[0]*sizes[1]*sizes[2] floats (may be NULL) */
 int b200rt_gibbs_get_weights(const b200rt_gibbs* g, float* w, int32_t sizes[3]);
 /* set_kappa_sptr: a device image in the penalty's layout, or NULL */

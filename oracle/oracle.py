@@ -378,6 +378,30 @@ def _trace(fn, start, stop, vox, norm_const, capacity):
 _ref = None
 
 
+REF_CUDA_PRIORS_LIB = os.path.join(HERE, "_ref", "libref_cuda_priors.so")
+_ref_cuda = None
+
+
+def ref_cuda_priors_available():
+    """STIR's own CUDA prior kernels built by oracle/Makefile (needs the STIR sources when building)."""
+    return os.path.exists(REF_CUDA_PRIORS_LIB)
+
+
+def ref_cuda_priors():
+    """ctypes handle of oracle/_ref/libref_cuda_priors.so: STIR's CudaRelativeDifferencePrior gradient kernel and
+    CudaGibbsPenalty gradient kernel with its potentials, launched as STIR's host classes launch them, on device
+    images in STIR's [z][y][x] order (pointers, a CUDA stream as void*)."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        lib = ctypes.CDLL(REF_CUDA_PRIORS_LIB)
+        lib.ref_cuda_rdp_prior_gradient.restype = _I
+        lib.ref_cuda_rdp_prior_gradient.argtypes = [_P, _P, _P, _P, _F, _F, _F, _I, _I, _I, _P]
+        lib.ref_cuda_gibbs_gradient.restype = _I
+        lib.ref_cuda_gibbs_gradient.argtypes = [_I, _P, _P, _P, _I, _I, _I, _P, _F, _F, _F, _I, _I, _I, _I, _I, _P]
+        _ref_cuda = lib
+    return _ref_cuda
+
+
 def ref_available():
     return os.path.exists(REF_LIB)
 

@@ -177,6 +177,8 @@ class StreamFormat(ctypes.Structure):
 
 GIBBS_QUADRATIC = 1
 GIBBS_RELATIVE_DIFFERENCE = 2
+GIBBS_ARITH_HOST = 0
+GIBBS_ARITH_CUDA = 1
 LAYOUT_DEVICE = 0  # [y][x][z]
 LAYOUT_STIR = 1    # [z][y][x]
 
@@ -270,6 +272,7 @@ EXPORTS = [
     ("b200rt_gibbs_create", _I, [ctypes.POINTER(GibbsParams), _I, ctypes.POINTER(_P)]),
     ("b200rt_gibbs_destroy", None, [_P]),
     ("b200rt_gibbs_last_error", ctypes.c_char_p, [_P]),
+    ("b200rt_gibbs_set_arithmetic", _I, [_P, _I]),
     ("b200rt_gibbs_get_weights", _I, [_P, _P, ctypes.POINTER(ctypes.c_int32)]),
     ("b200rt_gibbs_set_kappa", _I, [_P, _P]),
     ("b200rt_gibbs_value_dev", _I, [_P, _P, ctypes.POINTER(ctypes.c_double), _P]),

@@ -8,6 +8,7 @@ struct b200rt_gibbs {
   GibbsDev d{};
   std::vector<float> host_w;
   DevBuf<double> partial, result;
+  int arithmetic = B200RT_GIBBS_ARITH_HOST;
   std::string err;
 };
 
@@ -43,7 +44,10 @@ int gibbs_op(b200rt_gibbs* g, int op, const float* x, const float* in, float* ou
       g->partial.alloc(static_cast<size_t>(gibbs_num_partials(g->d)));
       g->result.alloc(1);
     }
-    ck(launch_gibbs(g->d, op, x, in, out, g->partial.p, g->result.p, st), "Gibbs penalty");
+    if (op == 1 && g->arithmetic == B200RT_GIBBS_ARITH_CUDA)
+      ck(launch_gibbs_gradient_cuda(g->d, x, out, st), "Gibbs penalty");
+    else
+      ck(launch_gibbs(g->d, op, x, in, out, g->partial.p, g->result.p, st), "Gibbs penalty");
     if (op == 0 || op == 2) {
       ck(cudaMemcpyAsync(value, g->result.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
       ck(cudaStreamSynchronize(st), "Gibbs penalty");
@@ -136,6 +140,14 @@ void b200rt_gibbs_destroy(b200rt_gibbs* g) {
 }
 
 const char* b200rt_gibbs_last_error(const b200rt_gibbs* g) { return g ? g->err.c_str() : "null penalty"; }
+
+int b200rt_gibbs_set_arithmetic(b200rt_gibbs* g, int arithmetic) {
+  if (!g) return B200RT_ERR_INVALID_ARGUMENT;
+  if (arithmetic != B200RT_GIBBS_ARITH_HOST && arithmetic != B200RT_GIBBS_ARITH_CUDA)
+    return gfail(g, B200RT_ERR_INVALID_ARGUMENT, "unknown Gibbs arithmetic");
+  g->arithmetic = arithmetic;
+  return B200RT_OK;
+}
 
 int b200rt_gibbs_get_weights(const b200rt_gibbs* g, float* w, int32_t sizes[3]) {
   if (!g || !sizes) return B200RT_ERR_INVALID_ARGUMENT;

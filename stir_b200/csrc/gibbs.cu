@@ -239,6 +239,66 @@ __global__ void gibbs_reduce_kernel(const double* __restrict__ partial, int n, d
   }
 }
 
+// ---- the gradient with the arithmetic of STIR's CUDA build (CudaGibbsPenalty_gradient_kernel,
+// CudaGibbsPenalty.cuh:141-206): a float sum per voxel over the whole neighbourhood (the centre included), each
+// term the float of weight x derivative_10 (a double product of two floats: one rounding), and the result the float
+// of sum x 2 x beta.  The potentials' float expressions are written with explicit round-to-nearest operations in the
+// form nvcc gives the reference's source (a product added to a sum contracted into one fused multiply-add), and
+// their double steps as float steps that round identically (as for RDPot above), so that the result does not depend
+// on this file's compilation flags.
+struct QuadPotCuda {
+  // (double)(c - n) / 2.0, times the weight and rounded to float: the float product w (c - n) / 2
+  __device__ __forceinline__ float term(float w, float c, float n) const { return __fmul_rn(w, 0.5f * __fsub_rn(c, n)); }
+};
+struct RDPotCuda {
+  float gamma, epsilon;
+  // RelativeDifferencePotential::derivative_10 (GibbsRelativeDifferencePenalty.h:81-91) as STIR's CUDA build
+  // evaluates it, times the weight and rounded to float
+  __device__ __forceinline__ float term(float w, float c, float n) const {
+    const float diff = __fsub_rn(c, n);
+    const float factor = __fadd_rn(__fmaf_rn(gamma, fabsf(diff), __fadd_rn(c, n)), epsilon);
+    const float num = __fmul_rn(0.5f * diff, __fadd_rn(__fmaf_rn(2.f, n, factor), epsilon));
+    const float den = __frcp_rn(__fmul_rn(factor, factor));
+    return __fmul_rn(w, __fmul_rn(num, den));
+  }
+};
+
+template <typename Pot>
+__global__ void __launch_bounds__(kGibbsThreads) gibbs_gradient_cuda_kernel(const GibbsDev g, const Pot pot,
+                                                                            const float* __restrict__ x,
+                                                                            float* __restrict__ out) {
+  const int n = g.nz * g.ny * g.nx;
+  const int j = blockIdx.x * kGibbsThreads + threadIdx.x;
+  if (j >= n) return;
+  int z, y, xx;
+  gibbs_coords(g, j, z, y, xx);
+  const int sz = static_cast<int>(g.sz), sy = static_cast<int>(g.sy), sx = static_cast<int>(g.sx);
+  const float c = __ldg(x + j);
+  const float kj = g.kappa ? __ldg(g.kappa + j) : 1.f;
+  float sum = 0.f;
+  if (g.wy == 3 && g.wx == 3 && g.wz == 3 && y >= 1 && y + 1 < g.ny && xx >= 1 && xx + 1 < g.nx && z >= 1 &&
+      z + 1 < g.nz) {
+#pragma unroll
+    for (int t = 0; t < 27; ++t) {
+      const int k = j + (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1) * sx;
+      float cur = pot.term(g.w[t], c, __ldg(x + k));
+      if (g.kappa) cur = __fmul_rn(cur, __fmul_rn(kj, __ldg(g.kappa + k)));
+      sum = __fadd_rn(sum, cur);
+    }
+  } else {
+    const Range r = gibbs_range(g, z, y, xx);
+    for (int dz = r.z0; dz <= r.z1; ++dz)
+      for (int dy = r.y0; dy <= r.y1; ++dy)
+        for (int dx = r.x0; dx <= r.x1; ++dx) {
+          const int k = j + dz * sz + dy * sy + dx * sx;
+          float cur = pot.term(gibbs_w(g, dz, dy, dx), c, __ldg(x + k));
+          if (g.kappa) cur = __fmul_rn(cur, __fmul_rn(kj, __ldg(g.kappa + k)));
+          sum = __fadd_rn(sum, cur);
+        }
+  }
+  out[j] = __fmul_rn(sum * 2.f, g.beta);
+}
+
 template <typename Pot>
 cudaError_t gibbs_launch_pot(const GibbsDev& g, const Pot& pot, int op, const float* x, const float* in, float* out,
                              double* partial, double* result, cudaStream_t st) {
@@ -268,6 +328,16 @@ cudaError_t launch_gibbs(const GibbsDev& g, int op, const float* x, const float*
                          double* result, cudaStream_t st) {
   if (g.potential == 1) return gibbs_launch_pot(g, QuadPot{}, op, x, in, out, partial, result, st);
   return gibbs_launch_pot(g, RDPot{g.gamma, g.epsilon}, op, x, in, out, partial, result, st);
+}
+
+cudaError_t launch_gibbs_gradient_cuda(const GibbsDev& g, const float* x, float* out, cudaStream_t st) {
+  const int64_t n = static_cast<int64_t>(g.nz) * g.ny * g.nx;
+  const unsigned nb = static_cast<unsigned>((n + kGibbsThreads - 1) / kGibbsThreads);
+  if (g.potential == 1)
+    gibbs_gradient_cuda_kernel<<<nb, kGibbsThreads, 0, st>>>(g, QuadPotCuda{}, x, out);
+  else
+    gibbs_gradient_cuda_kernel<<<nb, kGibbsThreads, 0, st>>>(g, RDPotCuda{g.gamma, g.epsilon}, x, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_gibbs_hessian_voxel(const GibbsDev& g, const float* x, int z, int y, int xx, float* out,

@@ -379,6 +379,8 @@ cudaError_t launch_gibbs(const GibbsDev& g, int op, const float* x, const float*
                          double* result, cudaStream_t st);
 cudaError_t launch_gibbs_hessian_voxel(const GibbsDev& g, const float* x, int z, int y, int xx, float* out,
                                        cudaStream_t st);
+// the gradient with the arithmetic of STIR's CUDA build (float sums), B200RT_GIBBS_ARITH_CUDA
+cudaError_t launch_gibbs_gradient_cuda(const GibbsDev& g, const float* x, float* out, cudaStream_t st);
 
 // out[c * ld_out + r] = in[r * ld_in + c], r < rows, c < cols
 cudaError_t launch_transpose(const float* in, float* out, int rows, int64_t cols, int64_t ld_in, int64_t ld_out,

@@ -26,6 +26,7 @@ class GibbsPenalty:
 
     potential = 0
     registered_name = ""
+    arithmetic = _abi.GIBBS_ARITH_HOST  # the gradient's sums: GibbsPenalty.inl's doubles
 
     def __init__(self, only_2D: bool = False, penalisation_factor: float = 0.0, device: int = 0):
         self.only_2D = bool(only_2D)
@@ -115,6 +116,7 @@ class GibbsPenalty:
         self._h = h
         self._shape = (nz, ny, nx)
         self._layout = layout
+        _abi.check(self._lib.b200rt_gibbs_set_arithmetic(self._h, self.arithmetic), what="set_up", gibbs=self._h)
 
     def _release(self):
         if getattr(self, "_h", None) is not None:
@@ -227,13 +229,17 @@ class GibbsRelativeDifferencePenalty(GibbsPenalty):
         return self.gamma, self.epsilon
 
 
-# the CUDA classes of the reference are the same objects here (everything runs on the GPU)
+# The reference's CUDA classes (src/include/stir/recon_buildblock/CUDA/CudaGibbsPenalty.h) run on the same kernels;
+# their gradient takes the CUDA build's arithmetic (float sums, CudaGibbsPenalty.cuh:141-206), the other
+# operations GibbsPenalty.inl's.
 class CudaGibbsQuadraticPenalty(GibbsQuadraticPenalty):
     registered_name = "Cuda Gibbs Quadratic"
+    arithmetic = _abi.GIBBS_ARITH_CUDA
 
 
 class CudaGibbsRelativeDifferencePenalty(GibbsRelativeDifferencePenalty):
     registered_name = "Cuda Gibbs Relative Difference"
+    arithmetic = _abi.GIBBS_ARITH_CUDA
 
 
 REGISTRY = {c.registered_name: c for c in (GibbsQuadraticPenalty, GibbsRelativeDifferencePenalty,

@@ -115,3 +115,78 @@ def test_gibbs_clinical_image_and_errors(cuda_device, oracle_lib):
     bad = gibbs.GibbsQuadraticPenalty(penalisation_factor=1.0)
     with pytest.raises(ValueError):
         bad.set_weights(np.ones((9, 3, 3), np.float32))
+
+
+def _ref_cuda(oracle_lib):
+    if not oracle_lib.ref_cuda_priors_available():
+        pytest.skip("STIR's CUDA prior kernels were not built (oracle/_ref needs the STIR sources)")
+    return oracle_lib.ref_cuda_priors()
+
+
+@pytest.mark.parametrize("potential", ["quadratic", "rdp"])
+@pytest.mark.parametrize("with_kappa", [False, True])
+@pytest.mark.parametrize("layout", [_abi.LAYOUT_STIR, _abi.LAYOUT_DEVICE])
+def test_cuda_arithmetic_gradient_equals_stirs_cuda_kernel(cuda_device, oracle_lib, potential, with_kappa, layout):
+    """CudaGibbs*Penalty's gradient (float sums) against STIR's own CudaGibbsPenalty_gradient_kernel built for this
+    GPU (oracle/_ref), on the same device image with the default 3x3x3 weights: equal bit for bit; and within float
+    rounding of the host arithmetic (double sums, the oracle)."""
+    import ctypes
+    import torch
+    from stir_b200 import gibbs
+    ref = _ref_cuda(oracle_lib)
+    shape, vox, beta = (23, 37, 41), (2.03, 2.09, 2.09), 0.3
+    rng = np.random.default_rng(11 + with_kappa)
+    x = torch.from_numpy(rng.uniform(0.0, 3.0, shape).astype(np.float32)).cuda()
+    x[3:5] = 0.0  # zero voxels: the Relative Difference potential's special case
+    kappa = torch.from_numpy(rng.uniform(0.5, 1.5, shape).astype(np.float32)).cuda() if with_kappa else None
+    cls = gibbs.CudaGibbsQuadraticPenalty if potential == "quadratic" else gibbs.CudaGibbsRelativeDifferencePenalty
+    p = cls(penalisation_factor=beta) if potential == "quadratic" else cls(penalisation_factor=beta, gamma=2.0,
+                                                                            epsilon=1e-7)
+
+    def to_layout(t):  # [z][y][x] -> the penalty's layout
+        return t if layout == _abi.LAYOUT_STIR else t.permute(1, 2, 0).contiguous()
+
+    def from_layout(t):
+        return t if layout == _abi.LAYOUT_STIR else t.view(shape[1], shape[2], shape[0]).permute(2, 0, 1).contiguous()
+
+    if kappa is not None:
+        p.set_kappa_sptr(to_layout(kappa))
+    p.set_up(shape, vox, layout)
+    got = from_layout(p.compute_gradient(to_layout(x)))
+    w = torch.from_numpy(np.ascontiguousarray(p.get_weights(), np.float32)).cuda()
+    out = torch.full(shape, float("nan"), device="cuda")
+    st = ref.ref_cuda_gibbs_gradient(1 if potential == "rdp" else 0, ctypes.c_void_p(out.data_ptr()),
+                                     ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(w.data_ptr()), 3, 3, 3,
+                                     None if kappa is None else ctypes.c_void_p(kappa.data_ptr()), beta, 2.0, 1e-7,
+                                     shape[0], shape[1], shape[2], -(shape[1] // 2), -(shape[2] // 2),
+                                     ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0
+    torch.cuda.synchronize()
+    assert torch.equal(got, out), float((got - out).abs().max())
+    host = gibbs.GibbsRelativeDifferencePenalty(penalisation_factor=beta, gamma=2.0, epsilon=1e-7) \
+        if potential == "rdp" else gibbs.GibbsQuadraticPenalty(penalisation_factor=beta)
+    if kappa is not None:
+        host.set_kappa_sptr(kappa)
+    host.set_up(shape, vox)
+    assert _rel(got.cpu().numpy(), host.compute_gradient(x).cpu().numpy()) <= 1e-6
+
+
+def test_stirs_cuda_rdp_prior_kernel_matches_oracle(cuda_device, oracle_lib):
+    """STIR's CudaRelativeDifferencePrior gradient kernel (built for this GPU) against the oracle's
+    RelativeDifferencePrior gradient: both sum in double, so they agree to float rounding."""
+    import ctypes
+    import torch
+    from stir_b200 import _abi as A
+    ref = _ref_cuda(oracle_lib)
+    shape, vox = (17, 29, 31), (2.03, 2.09, 2.09)
+    x = torch.from_numpy(np.random.default_rng(3).uniform(0.1, 3.0, shape).astype(np.float32)).cuda()
+    w = torch.from_numpy(np.ascontiguousarray(oracle_lib.gibbs_default_weights(vox), np.float32)).cuda()
+    out = torch.zeros(shape, device="cuda")
+    st = ref.ref_cuda_rdp_prior_gradient(ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(x.data_ptr()),
+                                         ctypes.c_void_p(w.data_ptr()), None, 2.0, 0.01, 0.5, *shape,
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0
+    torch.cuda.synchronize()
+    pr = A.Prior(type=A.PRIOR_RELATIVE_DIFFERENCE, penalisation_factor=0.5, gamma=2.0, epsilon=0.01, only_2D=0,
+                 map_model=A.MAP_MULTIPLICATIVE, kappa_dev=None)
+    assert _rel(out.cpu().numpy(), oracle_lib.prior_gradient(pr, x.cpu().numpy(), vox)) <= 1e-6

@@ -240,30 +240,39 @@ __global__ void gibbs_reduce_kernel(const double* __restrict__ partial, int n, d
 }
 
 // ---- the gradient with the arithmetic of STIR's CUDA build (CudaGibbsPenalty_gradient_kernel,
-// CudaGibbsPenalty.cuh:141-206): a float sum per voxel over the whole neighbourhood (the centre included), each
-// term the float of weight x derivative_10 (a double product of two floats: one rounding), and the result the float
-// of sum x 2 x beta.  The potentials' float expressions are written with explicit round-to-nearest operations in the
-// form nvcc gives the reference's source (a product added to a sum contracted into one fused multiply-add), and
-// their double steps as float steps that round identically (as for RDPot above), so that the result does not depend
-// on this file's compilation flags.
+// CudaGibbsPenalty.cuh:141-206): a float sum per voxel over the whole neighbourhood (the centre included) of
+// weight x derivative_10 (x kappa_j kappa_k), and the float of sum x 2 x beta.  nvcc compiles the reference's
+// source with contraction on and folds a double step between floats to the float step when that rounds the same
+// (an operation of two floats carried out in double and rounded back: double holds more than 2 x 24 + 2 bits);
+// so a term whose last operation becomes a float product is fused into the sum (one fused multiply-add), and the
+// other float expressions are contracted as written.  Each step is written here with an explicit round-to-nearest
+// operation so that the result does not depend on this file's compilation flags:
+//   Quadratic: the term w ((double)(c - n) / 2.0) stays a double product rounded to float, added to the sum;
+//              with kappa that float times (kappa_j kappa_k) is fused into the sum;
+//   Relative Difference (GibbsRelativeDifferencePenalty.h:81-91): factor = fma(gamma, |c - n|, c + n) + epsilon,
+//              num = (0.5 (c - n)) (fma(2, n, factor) + epsilon), den = 1 / (factor factor) (the double reciprocal
+//              rounded to float is the correctly rounded float reciprocal), d = num den; the term w d is fused into
+//              the sum, or with kappa w d rounded and (w d) (kappa_j kappa_k) fused into the sum.
 struct QuadPotCuda {
-  // (double)(c - n) / 2.0, times the weight and rounded to float: the float product w (c - n) / 2
-  __device__ __forceinline__ float term(float w, float c, float n) const { return __fmul_rn(w, 0.5f * __fsub_rn(c, n)); }
+  template <bool KAPPA>
+  __device__ __forceinline__ float add(float sum, float w, float c, float n, float kk) const {
+    const float cur = __fmul_rn(w, 0.5f * __fsub_rn(c, n));
+    return KAPPA ? __fmaf_rn(cur, kk, sum) : __fadd_rn(sum, cur);
+  }
 };
 struct RDPotCuda {
   float gamma, epsilon;
-  // RelativeDifferencePotential::derivative_10 (GibbsRelativeDifferencePenalty.h:81-91) as STIR's CUDA build
-  // evaluates it, times the weight and rounded to float
-  __device__ __forceinline__ float term(float w, float c, float n) const {
+  template <bool KAPPA>
+  __device__ __forceinline__ float add(float sum, float w, float c, float n, float kk) const {
     const float diff = __fsub_rn(c, n);
     const float factor = __fadd_rn(__fmaf_rn(gamma, fabsf(diff), __fadd_rn(c, n)), epsilon);
     const float num = __fmul_rn(0.5f * diff, __fadd_rn(__fmaf_rn(2.f, n, factor), epsilon));
-    const float den = __frcp_rn(__fmul_rn(factor, factor));
-    return __fmul_rn(w, __fmul_rn(num, den));
+    const float d = __fmul_rn(num, __frcp_rn(__fmul_rn(factor, factor)));
+    return KAPPA ? __fmaf_rn(__fmul_rn(w, d), kk, sum) : __fmaf_rn(w, d, sum);
   }
 };
 
-template <typename Pot>
+template <typename Pot, bool KAPPA>
 __global__ void __launch_bounds__(kGibbsThreads) gibbs_gradient_cuda_kernel(const GibbsDev g, const Pot pot,
                                                                             const float* __restrict__ x,
                                                                             float* __restrict__ out) {
@@ -274,16 +283,14 @@ __global__ void __launch_bounds__(kGibbsThreads) gibbs_gradient_cuda_kernel(cons
   gibbs_coords(g, j, z, y, xx);
   const int sz = static_cast<int>(g.sz), sy = static_cast<int>(g.sy), sx = static_cast<int>(g.sx);
   const float c = __ldg(x + j);
-  const float kj = g.kappa ? __ldg(g.kappa + j) : 1.f;
+  const float kj = KAPPA ? __ldg(g.kappa + j) : 1.f;
   float sum = 0.f;
   if (g.wy == 3 && g.wx == 3 && g.wz == 3 && y >= 1 && y + 1 < g.ny && xx >= 1 && xx + 1 < g.nx && z >= 1 &&
       z + 1 < g.nz) {
 #pragma unroll
     for (int t = 0; t < 27; ++t) {
       const int k = j + (t / 9 - 1) * sz + ((t / 3) % 3 - 1) * sy + (t % 3 - 1) * sx;
-      float cur = pot.term(g.w[t], c, __ldg(x + k));
-      if (g.kappa) cur = __fmul_rn(cur, __fmul_rn(kj, __ldg(g.kappa + k)));
-      sum = __fadd_rn(sum, cur);
+      sum = pot.template add<KAPPA>(sum, g.w[t], c, __ldg(x + k), KAPPA ? __fmul_rn(kj, __ldg(g.kappa + k)) : 1.f);
     }
   } else {
     const Range r = gibbs_range(g, z, y, xx);
@@ -291,9 +298,8 @@ __global__ void __launch_bounds__(kGibbsThreads) gibbs_gradient_cuda_kernel(cons
       for (int dy = r.y0; dy <= r.y1; ++dy)
         for (int dx = r.x0; dx <= r.x1; ++dx) {
           const int k = j + dz * sz + dy * sy + dx * sx;
-          float cur = pot.term(gibbs_w(g, dz, dy, dx), c, __ldg(x + k));
-          if (g.kappa) cur = __fmul_rn(cur, __fmul_rn(kj, __ldg(g.kappa + k)));
-          sum = __fadd_rn(sum, cur);
+          sum = pot.template add<KAPPA>(sum, gibbs_w(g, dz, dy, dx), c, __ldg(x + k),
+                                        KAPPA ? __fmul_rn(kj, __ldg(g.kappa + k)) : 1.f);
         }
   }
   out[j] = __fmul_rn(sum * 2.f, g.beta);
@@ -333,10 +339,15 @@ cudaError_t launch_gibbs(const GibbsDev& g, int op, const float* x, const float*
 cudaError_t launch_gibbs_gradient_cuda(const GibbsDev& g, const float* x, float* out, cudaStream_t st) {
   const int64_t n = static_cast<int64_t>(g.nz) * g.ny * g.nx;
   const unsigned nb = static_cast<unsigned>((n + kGibbsThreads - 1) / kGibbsThreads);
-  if (g.potential == 1)
-    gibbs_gradient_cuda_kernel<<<nb, kGibbsThreads, 0, st>>>(g, QuadPotCuda{}, x, out);
+  const RDPotCuda rdp{g.gamma, g.epsilon};
+  if (g.potential == 1 && g.kappa)
+    gibbs_gradient_cuda_kernel<QuadPotCuda, true><<<nb, kGibbsThreads, 0, st>>>(g, QuadPotCuda{}, x, out);
+  else if (g.potential == 1)
+    gibbs_gradient_cuda_kernel<QuadPotCuda, false><<<nb, kGibbsThreads, 0, st>>>(g, QuadPotCuda{}, x, out);
+  else if (g.kappa)
+    gibbs_gradient_cuda_kernel<RDPotCuda, true><<<nb, kGibbsThreads, 0, st>>>(g, rdp, x, out);
   else
-    gibbs_gradient_cuda_kernel<<<nb, kGibbsThreads, 0, st>>>(g, RDPotCuda{g.gamma, g.epsilon}, x, out);
+    gibbs_gradient_cuda_kernel<RDPotCuda, false><<<nb, kGibbsThreads, 0, st>>>(g, rdp, x, out);
   return cudaGetLastError();
 }
 

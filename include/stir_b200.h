@@ -263,6 +263,36 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
 int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
                            void* stream);
 
+/* A batch of images through one projector (no STIR counterpart: STIR projects one image at a time; the batches of
+ * torch.autograd and of noise realisations).  Image b is at images_dev + b*image_stride (device layout), its
+ * projection data at projdata_dev + b*projdata_stride; strides in floats, at least an image / the projection data.
+ * Where the column-staged kernels apply (non-TOF projectors) each call is one launch over (path item, image);
+ * otherwise, and for the deterministic back projection, the images go one at a time.  Results equal the
+ * single-image entry points' (the forward bit for bit; the atomic back projection to the order of float additions).
+ * Replaces a loop over ForwardProjectorByBin::forward_project / BackProjectorByBin::back_project
+ * (src/recon_buildblock/ForwardProjectorByBin.cxx:168-230, BackProjectorByBin.cxx:182-229). */
+int b200rt_forward_project_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
+                                     float* projdata_dev, int64_t projdata_stride, int batch, int subset_num,
+                                     int num_subsets, void* stream);
+int b200rt_back_project_batch_dev(b200rt_projector* h, const float* projdata_dev, int64_t projdata_stride,
+                                  float* images_dev, int64_t image_stride, int batch, int subset_num, int num_subsets,
+                                  int back_projection_mode, void* stream);
+/* b200rt_log_likelihood_dev / b200rt_log_likelihood_gradient_dev of every image of a batch: the data of image b at
+ * y_dev + b*y_stride (additive, mult likewise; a stride of 0 shares one array across the batch; additive and mult
+ * may be NULL).  values[batch] are written on the host (synchronises); gradient b at gradients_dev +
+ * b*gradient_stride. */
+int b200rt_log_likelihood_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
+                                    const float* y_dev, int64_t y_stride, const float* additive_dev,
+                                    int64_t additive_stride, const float* mult_dev, int64_t mult_stride, int batch,
+                                    int subset_num, int num_subsets, int zero_seg0_end_planes, double* values,
+                                    void* stream);
+int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
+                                             const float* y_dev, int64_t y_stride, const float* additive_dev,
+                                             int64_t additive_stride, const float* mult_dev, int64_t mult_stride,
+                                             int batch, int subset_num, int num_subsets, int zero_seg0_end_planes,
+                                             int back_projection_mode, float* gradients_dev, int64_t gradient_stride,
+                                             void* stream);
+
 /* Allocation-free variant of b200rt_log_likelihood_dev.  No counterpart in the reference.
  * For callers that must not allocate device memory once they are set up: for example a
  * reconstruction service that hands all device memory to a caching allocator at start-up, or

@@ -2,6 +2,7 @@
 
 * `forward_project(x, projector)`: A x, whose backward is the hand-written back projector A^T g.
 * `back_project(y, projector)`: A^T y, whose backward is A g.
+  A batch [B][...] goes through the batch entry points: one launch over (path item, image) per direction.
 * `PoissonLogLikelihood`: the objective of PoissonLogLikelihoodWithLinearModelForMeanAndProjData
   (value: accumulate_loglikelihood in FP64; gradient: A^T[divide_and_truncate(y, A x + a) - m],
   ...AndProjData.cxx:1421-1515).  Only x is saved for backward: the projection A x is recomputed
@@ -29,25 +30,45 @@ def _batched(t, per_item):
     return t.dim() > 1 and t.numel() != per_item
 
 
+def _forward_batch(proj, xs, out, subset_num, num_subsets):
+    """out[b] = A xs[b] for the images of xs [B][image] (one launch over (path item, image))"""
+    n_img, n_pd = xs.shape[1], proj.projdata_size
+    _abi.check(proj.lib.b200rt_forward_project_batch_dev(proj.h, _p(xs), n_img, _p(out), n_pd, xs.shape[0], subset_num,
+                                                         num_subsets, _stream_ptr(None)), proj.h,
+               "b200rt_forward_project_batch_dev")
+    return out
+
+
+def _back_batch(proj, ys, out, subset_num, num_subsets, mode):
+    """out[b] = A^T ys[b] for the projection data of ys [B][bins]"""
+    n_img, n_pd = out.shape[1], proj.projdata_size
+    _abi.check(proj.lib.b200rt_back_project_batch_dev(proj.h, _p(ys), n_pd, _p(out), n_img, ys.shape[0], subset_num,
+                                                      num_subsets, mode, _stream_ptr(None)), proj.h,
+               "b200rt_back_project_batch_dev")
+    return out
+
+
+def _n_img(proj):
+    return proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+
+
 class _ForwardProject(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, proj: RayTracingProjector, subset_num, num_subsets, mode):
         ctx.proj, ctx.subset, ctx.nsub, ctx.mode = proj, subset_num, num_subsets, mode
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+        n_img = _n_img(proj)
         xs = x.detach().contiguous().reshape(-1, n_img)
         out = torch.zeros((xs.shape[0], proj.projdata_size), dtype=torch.float32, device=x.device)
-        for b in range(xs.shape[0]):
-            proj.forward_dev(xs[b], out=out[b], subset_num=subset_num, num_subsets=num_subsets)
+        _forward_batch(proj, xs, out, subset_num, num_subsets)
         return out if _batched(x, n_img) else out[0]
 
     @staticmethod
     def backward(ctx, g):
         proj = ctx.proj
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+        n_img = _n_img(proj)
         gs = g.contiguous().reshape(-1, proj.projdata_size)
         out = torch.empty((gs.shape[0], n_img), dtype=torch.float32, device=g.device)
-        for b in range(gs.shape[0]):
-            proj.back_dev(gs[b], out=out[b], subset_num=ctx.subset, num_subsets=ctx.nsub, mode=ctx.mode)
+        _back_batch(proj, gs, out, ctx.subset, ctx.nsub, ctx.mode)
         shape = (gs.shape[0],) + proj.device_image_shape if g.dim() > 1 else proj.device_image_shape
         return out.reshape(shape), None, None, None, None
 
@@ -57,69 +78,74 @@ class _BackProject(torch.autograd.Function):
     def forward(ctx, y, proj: RayTracingProjector, subset_num, num_subsets, mode):
         ctx.proj, ctx.subset, ctx.nsub = proj, subset_num, num_subsets
         ys = y.detach().contiguous().reshape(-1, proj.projdata_size)
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
-        out = torch.empty((ys.shape[0], n_img), dtype=torch.float32, device=y.device)
-        for b in range(ys.shape[0]):
-            proj.back_dev(ys[b], out=out[b], subset_num=subset_num, num_subsets=num_subsets, mode=mode)
+        out = torch.empty((ys.shape[0], _n_img(proj)), dtype=torch.float32, device=y.device)
+        _back_batch(proj, ys, out, subset_num, num_subsets, mode)
         shape = (ys.shape[0],) + proj.device_image_shape if y.dim() > 1 else proj.device_image_shape
         return out.reshape(shape)
 
     @staticmethod
     def backward(ctx, g):
         proj = ctx.proj
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
-        gs = g.contiguous().reshape(-1, n_img)
+        gs = g.contiguous().reshape(-1, _n_img(proj))
         out = torch.zeros((gs.shape[0], proj.projdata_size), dtype=torch.float32, device=g.device)
-        for b in range(gs.shape[0]):
-            proj.forward_dev(gs[b], out=out[b], subset_num=ctx.subset, num_subsets=ctx.nsub)
+        _forward_batch(proj, gs, out, ctx.subset, ctx.nsub)
         return (out if gs.shape[0] > 1 or g.dim() > 3 else out[0]), None, None, None, None
 
 
 def forward_project(x, projector, subset_num=0, num_subsets=1, mode=_abi.BACKPROJECT_ATOMIC):
+    """A x for an image [y][x][z] or a batch [B][y][x][z] (device layout); differentiable, backward A^T g."""
     return _ForwardProject.apply(x, projector, subset_num, num_subsets, mode)
 
 
 def back_project(y, projector, subset_num=0, num_subsets=1, mode=_abi.BACKPROJECT_ATOMIC):
+    """A^T y for projection data [bins] or a batch [B][bins] (device layout); differentiable, backward A g."""
     return _BackProject.apply(y, projector, subset_num, num_subsets, mode)
+
+
+def _data_strides(proj, B, y, additive, mult):
+    """(array, stride) of the data of a batch of B images: one array per image (stride = bins) or one shared by
+    the batch (stride 0)."""
+    n = proj.projdata_size
+
+    def one(t, name):
+        if t is None:
+            return None, 0
+        t = t.contiguous()
+        if t.numel() == n:
+            return t, 0
+        if t.numel() == B * n:
+            return t, n
+        raise ValueError(f"{name} must hold the projection data of one image or of each of the {B} images")
+    return one(y, "y"), one(additive, "additive"), one(mult, "mult")
 
 
 class _LogLikelihood(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode):
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+        n_img = _n_img(proj)
         xs = x.detach().contiguous().reshape(-1, n_img)
         B = xs.shape[0]
-        ys = y.reshape(B, -1)
-        adds = None if additive is None else additive.reshape(B, -1) if additive.numel() == B * proj.projdata_size else None
-        total = 0.0
-        out = ctypes.c_double(0.0)
-        for b in range(B):
-            a = additive if additive is None or additive.numel() == proj.projdata_size else adds[b]
-            m = mult if mult is None or mult.numel() == proj.projdata_size else mult.reshape(B, -1)[b]
-            _abi.check(proj.lib.b200rt_log_likelihood_dev(proj.h, _p(xs[b]), _p(ys[b]), _p(a), _p(m), subset_num,
-                                                          num_subsets, int(zero_ends), ctypes.byref(out),
-                                                          _stream_ptr(None)), proj.h, "b200rt_log_likelihood_dev")
-            total += out.value
+        (yy, ys), (aa, as_), (mm, ms) = _data_strides(proj, B, y, additive, mult)
+        values = (ctypes.c_double * B)()
+        _abi.check(proj.lib.b200rt_log_likelihood_batch_dev(proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B,
+                                                            subset_num, num_subsets, int(zero_ends), values,
+                                                            _stream_ptr(None)), proj.h, "b200rt_log_likelihood_batch_dev")
         ctx.save_for_backward(x)
         ctx.args = (proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode)
-        return torch.tensor(total, dtype=torch.float64, device=x.device)
+        return torch.tensor(sum(values[b] for b in range(B)), dtype=torch.float64, device=x.device)
 
     @staticmethod
     def backward(ctx, gout):
         (x,) = ctx.saved_tensors
         proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode = ctx.args
-        n_img = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+        n_img = _n_img(proj)
         xs = x.detach().contiguous().reshape(-1, n_img)
         B = xs.shape[0]
-        ys = y.reshape(B, -1)
+        (yy, ys), (aa, as_), (mm, ms) = _data_strides(proj, B, y, additive, mult)
         grad = torch.empty_like(xs)
-        for b in range(B):
-            a = additive if additive is None or additive.numel() == proj.projdata_size else additive.reshape(B, -1)[b]
-            m = mult if mult is None or mult.numel() == proj.projdata_size else mult.reshape(B, -1)[b]
-            _abi.check(proj.lib.b200rt_log_likelihood_gradient_dev(proj.h, _p(xs[b]), _p(ys[b]), _p(a), _p(m), subset_num,
-                                                                   num_subsets, int(zero_ends), mode, _p(grad[b]),
-                                                                   _stream_ptr(None)), proj.h,
-                       "b200rt_log_likelihood_gradient_dev")
+        _abi.check(proj.lib.b200rt_log_likelihood_gradient_batch_dev(
+            proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B, subset_num, num_subsets, int(zero_ends), mode,
+            _p(grad), n_img, _stream_ptr(None)), proj.h, "b200rt_log_likelihood_gradient_batch_dev")
         return (grad.reshape(x.shape) * gout.to(torch.float32)), None, None, None, None, None, None, None, None
 
 

@@ -107,6 +107,7 @@ struct b200rt_projector {
   std::map<std::pair<int, int>, int> subset_view_counts;
   // OSMAPOSL scratch
   DevBuf<float> ratio, upd, grad, small_value, partial_max, umax;
+  DevBuf<float> ratio_batch;  // gradient ratios of an image batch (b200rt_log_likelihood_gradient_batch_dev)
   DevBuf<unsigned int> cancelled;
   DevBuf<double> ll_partials, ll_sum;
   // deterministic back projection

@@ -967,6 +967,11 @@ void b200rt_destroy(b200rt_projector* h) {
     h->path_cmaj.release();
     h->path_col_starts.release();
     h->ratio.release();
+    h->ratio_batch.release();
+    h->bin_view_dev.release();
+    h->tof_basic_view_dev.release();
+    h->item_view_dev.release();
+    h->view_basic_dev.release();
     h->upd.release();
     h->grad.release();
     h->small_value.release();

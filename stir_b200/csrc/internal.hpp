@@ -111,6 +111,9 @@ struct FwdEpilogue {
   const float* small_value;    // per ((tof-min)*(2S+1)+segment+S)*num_views+view: max(viewgram y)*SMALL_NUM, >= 0
   unsigned int* cancelled;     // number of ratios clipped at 1e4
   double* partials;            // one log-likelihood partial sum per CTA
+  // a batch of images projected in one launch (grid.y = image): image b's y, add, mult and thresholds are at these
+  // strides (0: shared by the batch), its partial sums at b x grid.x
+  int64_t y_stride, add_stride, mult_stride, sv_stride;
 };
 
 // One reconstruction of a batch: its geometry (index into a ProjParams table), estimate, ratio
@@ -256,6 +259,14 @@ cudaError_t launch_back_paths_atomic(const ProjParams& p, const PathParams& pp, 
 cudaError_t launch_back_paths_fixed(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
                                     const float* projdata, unsigned long long* acc, const double* scale,
                                     cudaStream_t st, int zero_ends);
+// the same over a batch of images in one launch (grid.y = image): image b at image + b img_stride, its projection
+// data at projdata + b pd_stride (the forward's epilogue data at the strides of FwdEpilogue)
+cudaError_t launch_forward_paths_batch(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                       const float* images, int64_t img_stride, float* projdata, int64_t pd_stride,
+                                       int batch, cudaStream_t st, const FwdEpilogue* ep);
+cudaError_t launch_back_paths_atomic_batch(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                           const float* projdata, int64_t pd_stride, float* images, int64_t img_stride,
+                                           int batch, cudaStream_t st, int zero_ends);
 
 // persistent batched projectors over (frame, path item) work items (BatchItem::bin holds the path item)
 cudaError_t launch_forward_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int npa, int smem_bytes,

@@ -343,6 +343,7 @@ struct FloatCols {
   using T = float;
   float* img;
   __device__ __forceinline__ void load() {}
+  __device__ __forceinline__ void offset(int64_t o) { img += o; }
   __device__ __forceinline__ T term(float v) const { return v; }
   __device__ __forceinline__ void flush(int64_t i, float v) const {
     if (v != 0.f) atomicAdd(img + i, v);
@@ -354,6 +355,7 @@ struct FixedCols {
   const double* scale_ptr;  // 2^k of the fixed-point format, computed on the device
   double scale;
   __device__ __forceinline__ void load() { scale = *scale_ptr; }
+  __device__ __forceinline__ void offset(int64_t) {}  // one image per launch
   // the same rounding of each contribution as the per-basic-bin fixed-point kernel
   __device__ __forceinline__ T term(float v) const { return __double2ll_rn(static_cast<double>(v) * scale); }
   __device__ __forceinline__ void flush(int64_t i, long long v) const {
@@ -591,9 +593,18 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
 template <int NPA, int EPI>
 __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
     forward_paths_kernel(ProjParams p, PathParams pp, const int* __restrict__ list, const float* __restrict__ img,
-                         float* __restrict__ out, FwdEpilogue ep) {
+                         int64_t img_stride, float* __restrict__ out, int64_t out_stride, FwdEpilogue ep) {
   extern __shared__ __align__(16) unsigned char smem[];
   const PathItemDev it = pp.items[list[blockIdx.x]];
+  if (blockIdx.y > 0) {  // image blockIdx.y of a batch
+    const int64_t b = blockIdx.y;
+    img += b * img_stride;
+    if (out) out += b * out_stride;
+    ep.y += b * ep.y_stride;
+    if (ep.add) ep.add += b * ep.add_stride;
+    if (ep.mult) ep.mult += b * ep.mult_stride;
+    if (ep.small_value) ep.small_value += b * ep.sv_stride;
+  }
   double ll = 0.0;
   unsigned ncancel = 0;
   forward_path_item<NPA, EPI>(p, pp, it, smem, img, out, ep, ll, ncancel);
@@ -611,19 +622,23 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < kPathWarps; ++w) t += red[w];
-      ep.partials[blockIdx.x] = t;
+      ep.partials[static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x] = t;
     }
   }
 }
 
 template <typename Cols>
 __global__ void __launch_bounds__(kPathThreads, kPathMinCtasBack)
-    back_paths_kernel(ProjParams p, PathParams pp, const int* __restrict__ list, const float* __restrict__ pd, Cols acc,
-                      int zero_ends) {
+    back_paths_kernel(ProjParams p, PathParams pp, const int* __restrict__ list, const float* __restrict__ pd,
+                      int64_t pd_stride, Cols acc, int64_t img_stride, int zero_ends) {
   extern __shared__ __align__(16) unsigned char smem[];
   const PathItemDev it = pp.items[list[blockIdx.x]];
   Cols a = acc;
   a.load();
+  if (blockIdx.y > 0) {  // image blockIdx.y of a batch
+    if (pd) pd += static_cast<int64_t>(blockIdx.y) * pd_stride;
+    a.offset(static_cast<int64_t>(blockIdx.y) * img_stride);
+  }
   back_path_item<Cols>(p, pp, it, smem, pd, a, zero_ends);
 }
 
@@ -708,45 +723,68 @@ cudaError_t prepare_path_smem(const void* fn, int bytes) {
 }
 
 template <typename K, typename... A>
-cudaError_t launch_path(K kernel, int nitems, int smem_bytes, cudaStream_t st, A... args) {
-  if (nitems <= 0) return cudaSuccess;
+cudaError_t launch_path(K kernel, int nitems, int batch, int smem_bytes, cudaStream_t st, A... args) {
+  if (nitems <= 0 || batch <= 0) return cudaSuccess;
+  if (batch > 65535) return cudaErrorInvalidValue;
   cudaError_t e = prepare_path_smem(reinterpret_cast<const void*>(kernel), smem_bytes);
   if (e != cudaSuccess) return e;
-  kernel<<<nitems, kPathThreads, smem_bytes, st>>>(args...);
+  kernel<<<dim3(nitems, batch), kPathThreads, smem_bytes, st>>>(args...);
   return cudaGetLastError();
 }
 
 template <int EPI>
 cudaError_t launch_forward_paths_epi(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* image,
-                                     float* out, cudaStream_t st, const FwdEpilogue& ep) {
+                                     int64_t img_stride, float* out, int64_t out_stride, int batch, cudaStream_t st,
+                                     const FwdEpilogue& ep) {
   const int sm = path_smem_fwd(pp.K, p.nz, pp.zpad, pp.max_lines, pp.max_acc, pp.npa_max).total;
   switch (p.uniform_npa) {
-    case 1: return launch_path(forward_paths_kernel<1, EPI>, n, sm, st, p, pp, list, image, out, ep);
-    case 2: return launch_path(forward_paths_kernel<2, EPI>, n, sm, st, p, pp, list, image, out, ep);
-    default: return launch_path(forward_paths_kernel<0, EPI>, n, sm, st, p, pp, list, image, out, ep);
+    case 1:
+      return launch_path(forward_paths_kernel<1, EPI>, n, batch, sm, st, p, pp, list, image, img_stride, out, out_stride,
+                         ep);
+    case 2:
+      return launch_path(forward_paths_kernel<2, EPI>, n, batch, sm, st, p, pp, list, image, img_stride, out, out_stride,
+                         ep);
+    default:
+      return launch_path(forward_paths_kernel<0, EPI>, n, batch, sm, st, p, pp, list, image, img_stride, out, out_stride,
+                         ep);
   }
 }
 
 template <typename Cols>
 cudaError_t launch_back_paths(const ProjParams& p, const PathParams& pp, const int* list, int n, const float* pd,
-                              const Cols& acc, cudaStream_t st, int zero_ends) {
+                              int64_t pd_stride, const Cols& acc, int64_t img_stride, int batch, cudaStream_t st,
+                              int zero_ends) {
   const int sm = path_smem_back(p.nz, pp.max_lines, pp.max_members, pp.nax_max, pp.npa_max).total;
-  return launch_path(back_paths_kernel<Cols>, n, sm, st, p, pp, list, pd, acc, zero_ends);
+  return launch_path(back_paths_kernel<Cols>, n, batch, sm, st, p, pp, list, pd, pd_stride, acc, img_stride, zero_ends);
 }
 
 }  // namespace
 
-cudaError_t launch_forward_paths(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
-                                 const float* image, float* projdata, cudaStream_t st, const FwdEpilogue* ep) {
+cudaError_t launch_forward_paths_batch(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                       const float* images, int64_t img_stride, float* projdata, int64_t pd_stride,
+                                       int batch, cudaStream_t st, const FwdEpilogue* ep) {
   FwdEpilogue e{};
   if (ep) e = *ep;
   switch (e.mode) {
-    case kEpiNone: return launch_forward_paths_epi<kEpiNone>(p, pp, items, nitems, image, projdata, st, e);
-    case kEpiRatio: return launch_forward_paths_epi<kEpiRatio>(p, pp, items, nitems, image, projdata, st, e);
-    case kEpiGradient: return launch_forward_paths_epi<kEpiGradient>(p, pp, items, nitems, image, projdata, st, e);
-    case kEpiLoglik: return launch_forward_paths_epi<kEpiLoglik>(p, pp, items, nitems, image, projdata, st, e);
+    case kEpiNone:
+      return launch_forward_paths_epi<kEpiNone>(p, pp, items, nitems, images, img_stride, projdata, pd_stride, batch, st,
+                                                e);
+    case kEpiRatio:
+      return launch_forward_paths_epi<kEpiRatio>(p, pp, items, nitems, images, img_stride, projdata, pd_stride, batch,
+                                                 st, e);
+    case kEpiGradient:
+      return launch_forward_paths_epi<kEpiGradient>(p, pp, items, nitems, images, img_stride, projdata, pd_stride, batch,
+                                                    st, e);
+    case kEpiLoglik:
+      return launch_forward_paths_epi<kEpiLoglik>(p, pp, items, nitems, images, img_stride, projdata, pd_stride, batch,
+                                                  st, e);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_forward_paths(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                 const float* image, float* projdata, cudaStream_t st, const FwdEpilogue* ep) {
+  return launch_forward_paths_batch(p, pp, items, nitems, image, 0, projdata, 0, 1, st, ep);
 }
 
 cudaError_t launch_forward_batch_paths(const ProjParams* geoms, const PathParams* pgeoms, int npa, int smem_bytes,
@@ -784,13 +822,20 @@ int batch_paths_max_ctas_per_sm(int npa, int smem_bytes, bool forward) {
 
 cudaError_t launch_back_paths_atomic(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
                                      const float* projdata, float* image, cudaStream_t st, int zero_ends) {
-  return launch_back_paths(p, pp, items, nitems, projdata, FloatCols{image}, st, zero_ends);
+  return launch_back_paths(p, pp, items, nitems, projdata, 0, FloatCols{image}, 0, 1, st, zero_ends);
+}
+
+cudaError_t launch_back_paths_atomic_batch(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
+                                           const float* projdata, int64_t pd_stride, float* images, int64_t img_stride,
+                                           int batch, cudaStream_t st, int zero_ends) {
+  return launch_back_paths(p, pp, items, nitems, projdata, pd_stride, FloatCols{images}, img_stride, batch, st,
+                           zero_ends);
 }
 
 cudaError_t launch_back_paths_fixed(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
                                     const float* projdata, unsigned long long* acc, const double* scale,
                                     cudaStream_t st, int zero_ends) {
-  return launch_back_paths(p, pp, items, nitems, projdata, FixedCols{acc, scale, 0.0}, st, zero_ends);
+  return launch_back_paths(p, pp, items, nitems, projdata, 0, FixedCols{acc, scale, 0.0}, 0, 1, st, zero_ends);
 }
 
 }  // namespace b200

@@ -292,6 +292,66 @@ def reference_cuda_priors(p_dev_layout, shape, vox, device):
     return res
 
 
+def autograd_workload(device, batch=8):
+    """The differentiable projector's workload: a batch of 8 seeded smooth fields of 172x172x127 on the clinical
+    scanner (zoom 0.5), loss = Poisson log-likelihood (attenuation, 10 % background) + RelativeDifferencePrior (beta
+    0.1, gamma 2); one step = the loss's value and its gradient by torch.autograd (forward and back projections of the
+    batch, one launch per direction), against the same with one launch per image."""
+    import torch
+    from stir_b200 import geometry as G
+    from stir_b200 import phantoms, workloads
+    from stir_b200.autograd import PoissonLogLikelihood, Prior
+    from stir_b200.osmaposl import RelativeDifferencePrior
+    from stir_b200.projectors import RayTracingProjector
+    proj = RayTracingProjector(*G.clinical_3d_pet_half(), device=device)
+    imgs = [phantoms.smooth_random_field(proj.image, sigma_vox=3.0, seed=10 + k) for k in range(batch)]
+    x = torch.stack([proj.image_to_device_layout(torch.from_numpy(a).cuda(device)) for a in imgs])
+    mu = phantoms.attenuation_cylinder(proj.image, radius_mm=150.0, mu_per_mm=0.0096)
+    m = workloads._attenuation_factors(proj, mu)
+    ys, adds = [], []
+    for k in range(batch):
+        ybar = m * proj.forward_dev(x[k])
+        b = 0.1 * float(ybar.double().mean())
+        yk, _ = workloads._poisson(ybar + b, 3e7, 100 + k)
+        ys.append(yk)
+        adds.append(torch.full_like(yk, b) / m)
+    y, add = torch.stack(ys), torch.stack(adds)
+    R = Prior(proj, RelativeDifferencePrior(0.1, gamma=2.0, epsilon=0.0))
+    L = PoissonLogLikelihood(proj, y, add, m)
+    singles = [PoissonLogLikelihood(proj, y[k], add[k], m) for k in range(batch)]
+
+    def batched():
+        xg = x.detach().requires_grad_(True)
+        loss = -(L(xg) - R(xg))
+        loss.backward()
+        return float(loss)
+
+    def one_by_one():
+        total = 0.0
+        for k in range(batch):
+            xg = x[k].detach().requires_grad_(True)
+            loss = -(singles[k](xg) - R(xg))
+            loss.backward()
+            total += float(loss)
+        return total
+
+    ms_b = time_dev(batched, warm=2, reps=3)
+    ms_1 = time_dev(one_by_one, warm=1, reps=3)
+    v_b, v_1 = batched(), one_by_one()
+    res = {"metric": "differentiable projector loss+gradient steps/s", "value": 1e3 / ms_b, "unit": "steps/s",
+           "ms_per_step": ms_b, "images_per_s": batch * 1e3 / ms_b, "one_launch_per_image_ms": ms_1,
+           "speedup_vs_one_launch_per_image": ms_1 / ms_b, "batch": batch,
+           "loss_rel_diff_vs_one_by_one": abs(v_b - v_1) / abs(v_1),
+           "workload": "8 x 172x172x127 smooth fields (sigma 3 voxels, seeds 10..17) on the clinical scanner at zoom 0.5; "
+                       "loss -log-likelihood (3e7 counts each, attenuation, 10 % background) + RDP beta 0.1; value "
+                       "and gradient by torch.autograd, the projection recomputed in backward (wall clock around "
+                       "CUDA events: the value is read on the host)"}
+    proj.close()
+    del proj, x, y, add, m
+    torch.cuda.empty_cache()
+    return res
+
+
 def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5):
     """The TOF configuration's reconstructions: `frames` noise realisations (seeds 0..), OSMAPOSL with a
     QuadraticPrior (beta 0.5, 3x3x3 neighbourhood), 21 subsets x 3 iterations, batched in one graph against one
@@ -307,7 +367,7 @@ def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5)
     data = []
     for k in range(frames):
         g = torch.Generator(device=ybar.device).manual_seed(k)
-        scale = 5e6 / float((ybar + bg).sum())
+        scale = 3e8 / float((ybar + bg).sum())
         y = torch.poisson((ybar + bg) * scale, generator=g) / scale
         data.append((y, torch.full_like(y, bg)))
     n = nsub * iterations
@@ -347,7 +407,7 @@ def tof_batched_reconstructions(proj, frames=4, nsub=21, iterations=3, beta=0.5)
     return {"metric": "batched TOF OSMAPOSL reconstructions/s", "value": frames / t_b, "unit": "reconstructions/s",
             "per_frame_value": frames / t_pf, "speedup_vs_per_frame": t_pf / t_b, "frames": frames,
             "subsets": nsub, "sub_iterations": n, "prior": f"QuadraticPrior beta {beta}",
-            "workload": "noise realisations (torch Poisson, seeds 0..3, 5e6 counts) of a cylinder with 2 spheres, "
+            "workload": "noise realisations (torch Poisson, seeds 0..3, 3e8 counts) of a cylinder with 2 spheres, "
                         "additive background 10 %; wall clock with a device synchronisation on both sides"}
 
 
@@ -685,6 +745,23 @@ def b200_main(args):
             "l2_hit_rate": {FWD_KERNEL: profile_value("l2_hit_rate", FWD_KERNEL),
                             BACK_KERNEL: profile_value("l2_hit_rate", BACK_KERNEL)}}
 
+    roof["byte_model"] = ("algorithmic bytes (SURVEY 8d): every (row element, LOR) pair counted as a 4-byte image read "
+                          "(forward) or an 8-byte read-modify-write (back); the column staging serves them from shared "
+                          "memory and L2, so frac above 1 says the kernel avoids DRAM, not that it beats the copy "
+                          "bandwidth; the compulsory-bytes fractions (image and projection data once) and the on-chip "
+                          "limiter (ncu) say where the time goes")
+
+    # the deterministic back projection (64-bit fixed point, order-independent) on the same data, beside the atomic one
+    bk2 = proj.empty_image()
+    proj.back_dev(y, out=bk2, mode=_abi.BACKPROJECT_DETERMINISTIC)
+    det_ms = time_dev(lambda: proj.back_dev(y, out=bk2, mode=_abi.BACKPROJECT_DETERMINISTIC), warm=1, reps=3)
+    bk3 = proj.back_dev(y, mode=_abi.BACKPROJECT_DETERMINISTIC)
+    deterministic = {"back_ms": det_ms, "atomic_back_ms": back_ms, "bit_identical_across_runs": bool(torch.equal(bk2, bk3)),
+                     "rel_l2_vs_atomic": float((bk2 - bk).double().norm() / bk.double().norm()),
+                     "method": "each contribution rounded to a 64-bit fixed-point integer (scale from the data's bound "
+                               "and the largest column sum), integers added atomically, converted once"}
+    del bk2, bk3
+
     cpu = None
     cb = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -707,7 +784,8 @@ def b200_main(args):
             "e2e": {"value": e2e_value, "unit": "LORs/s", "h2d_bytes_per_step": img_bytes + pd_bytes,
                     "d2h_bytes_per_step": pd_bytes + img_bytes},
             "clocks": clocks.summary(),
-            "gpu_launches": 2 * K}
+            "gpu_launches": 2 * K,
+            "deterministic": deterministic}
     # the secondary workloads and the batched reconstructions are measured on one GPU only (the scaling runs
     # hold every GPU of the node; they report the headline alone)
     if not args.no_extras and ws == 1:
@@ -715,6 +793,11 @@ def b200_main(args):
             line.update(listmode_and_priors(proj, pdi, img, xd, cb))
         except Exception as e:  # reported, never hides the headline line
             line["listmode"] = {"error": f"{type(e).__name__}: {e}"}
+    if not args.no_extras and ws == 1:
+        try:
+            line["autograd"] = autograd_workload(local)
+        except Exception as e:  # reported, never hides the headline line
+            line["autograd"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_batch and ws == 1:
         proj.close()
         del pd, bk, flush, y, xd

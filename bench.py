@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "split"],
+                    help="replicas: an independent copy of the workload per GPU (weak scaling); split: one copy of the "
+                         "workload split across the GPUs by views, each holding its share of the projection data, "
+                         "the back projections summed by an NCCL all-reduce (strong scaling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched dynamic OSEM measurement")
     ap.add_argument("--batch-iterations", type=int, default=2, help="full OSEM iterations per dynamic frame")
@@ -453,6 +457,74 @@ def tof_workload(with_cpu, device):
         proj.close()
 
 
+def split_measure(pdi, img, x_host, rank, ws, local, dist, steps, warmup):
+    """The clinical workload's forward + back projection split across the ranks: rank r holds the projection data
+    of the views of subset r of ws (a view shard: 1/ws of the data) and projects them; the back projections are
+    summed by an NCCL all-reduce of the image (the exchange of the multi-GPU reconstruction).  Returns the whole
+    job's LORs/s over the slowest rank's device time."""
+    import torch
+    from stir_b200.distributed import rank_subset, rank_views, shard_projdata
+    from stir_b200.projectors import RayTracingProjector
+    dev = torch.device("cuda", local)
+    proj = RayTracingProjector(pdi, img, device=local)
+    nbins = proj.projdata_size
+    xd = proj.image_to_device_layout(torch.from_numpy(x_host).to(dev))
+    y_full = proj.forward_dev(xd)
+    y_full.add_(0.3 * float(y_full.mean()))
+    views = rank_views(proj.geometry, 1, rank, ws, proj.info.symmetries_used)
+    y = shard_projdata(pdi, y_full, views)
+    del y_full
+    proj.set_view_shard(views)
+    sub, nsub = rank_subset(0, 1, rank, ws)
+    pd = proj.empty_projdata()
+    bk = proj.empty_image()
+    flush = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step():
+        proj.forward_dev(xd, out=pd, subset_num=sub, num_subsets=nsub)
+        proj.back_dev(y, out=bk, subset_num=sub, num_subsets=nsub)
+        if dist:
+            dist.all_reduce(bk)
+
+    for _ in range(max(warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ar = []
+    e0.record()
+    for k in range(steps):
+        flush.fill_(float(k))
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    # the all-reduce alone, for the record
+    if dist:
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(5):
+            dist.all_reduce(bk)
+        a1.record()
+        torch.cuda.synchronize()
+        ar.append(a0.elapsed_time(a1) / 5)
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item()) / steps
+    res = {"value": nbins / (ms / 1e3), "unit": "LORs/s", "ms_per_step": ms, "scaling": "strong",
+           "views_per_rank": len(views), "projdata_bytes_per_rank": 4 * proj.projdata_size,
+           "allreduce_ms": ar[0] if ar else 0.0, "image_bytes": 4 * img.nz * img.ny * img.nx,
+           "workload": "forward + back projection of all 72.6 M LORs split by views (view shards), NCCL all-reduce "
+                       "of the back projection every step"}
+    proj.close()
+    del pd, bk, flush, y, xd
+    torch.cuda.empty_cache()
+    return res
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -788,6 +860,13 @@ def b200_main(args):
             "deterministic": deterministic}
     # the secondary workloads and the batched reconstructions are measured on one GPU only (the scaling runs
     # hold every GPU of the node; they report the headline alone)
+    if ws > 1 or args.mode == "split":
+        # the split of one reconstruction's projections across the GPUs (all ranks take part)
+        split = split_measure(pdi, img, x, rank, ws, local, dist, K, args.warmup)
+        if args.mode == "split":
+            line.update(value=split["value"], ms_per_step=split["ms_per_step"], scaling="strong")
+            line["config"]["parallelism"] = f"view split over {ws} GPU(s), NCCL all-reduce of the back projection"
+        line["split"] = split
     if not args.no_extras and ws == 1:
         try:
             line.update(listmode_and_priors(proj, pdi, img, xd, cb))

@@ -263,6 +263,18 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
 int b200rt_prior_value_dev(b200rt_projector* h, const b200rt_prior* prior, const float* image_dev, double* out,
                            void* stream);
 
+/* View shard: the projector holds the projection data of `views` only (slot i = views[i]), in the device layout
+ * [segment][slot][tangential][axial]; every projection-data array passed afterwards (y, additive, multiplicative
+ * factors, projections) has that shard's size (b200rt_projdata_size).  Projections, sensitivities, the OSMAPOSL
+ * numerator and update, the log-likelihood and its gradient, attenuation and normalisation then cover the bins of
+ * those views only (lines of other views are skipped, and path items without a line in the shard); summed over
+ * shards that partition the views they give the whole data's result.  For the multi-GPU reconstruction that keeps
+ * only its share of y, a and m on each GPU (the data partition of STIR's MPI build, distributed.cxx:161-225).
+ * Needs the column-staged kernels (non-TOF data; B200RT_ERR_UNSUPPORTED otherwise).  Entry points that address the
+ * whole data (host buffers, layout conversions, viewgrams, streams, list mode, OSSPS, batches, the allocation-free
+ * log-likelihood) return B200RT_ERR_STATE on a shard.  views = NULL or num_views = 0 restores the whole data. */
+int b200rt_set_view_shard(b200rt_projector* h, const int32_t* views, int num_views);
+
 /* A batch of images through one projector (no STIR counterpart: STIR projects one image at a time; the batches of
  * torch.autograd and of noise realisations).  Image b is at images_dev + b*image_stride (device layout), its
  * projection data at projdata_dev + b*projdata_stride; strides in floats, at least an image / the projection data.

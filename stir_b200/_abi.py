@@ -271,6 +271,7 @@ EXPORTS = [
     ("b200rt_projdata_to_stream_dev", _I, [_P, _P, ctypes.POINTER(StreamFormat), _P, _I64, _P]),
     ("b200rt_gibbs_create", _I, [ctypes.POINTER(GibbsParams), _I, ctypes.POINTER(_P)]),
     ("b200rt_gibbs_destroy", None, [_P]),
+    ("b200rt_set_view_shard", _I, [_P, _P, _I]),
     ("b200rt_forward_project_batch_dev", _I, [_P, _P, _I64, _P, _I64, _I, _I, _I, _P]),
     ("b200rt_back_project_batch_dev", _I, [_P, _P, _I64, _P, _I64, _I, _I, _I, _I, _P]),
     ("b200rt_log_likelihood_batch_dev", _I, [_P, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _I, _P, _P]),

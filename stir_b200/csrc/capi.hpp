@@ -95,6 +95,12 @@ struct b200rt_projector {
   std::vector<int> h_bin_view;  // basic view of each bin
   std::vector<int> h_bin_seg;
   std::vector<int> h_view_basic;  // basic view of each view (-1: none)
+  // view shard (b200rt_set_view_shard): the views held, in slot order (empty: every view), each view's slot (-1: not
+  // held) on the host and the device, the full layout's segment table, and the shard's data size and timing-bin stride
+  std::vector<int> shard_views, h_view_slot;
+  DevBuf<int> view_slot_dev;
+  std::vector<SegDev> h_segs_full;
+  int64_t shard_pd_size = 0, shard_tof_stride = 0;
   // basic views of h_bin_view, h_tof_basic_view, h_item_view and h_view_basic on the device (set-up)
   DevBuf<int> bin_view_dev, tof_basic_view_dev, item_view_dev, view_basic_dev;
   std::map<long long, int> bin_index;  // (view, seg, tang, tof) -> bin
@@ -199,5 +205,12 @@ void osmaposl_numerator(b200rt_projector& h, const float* x, const float* y, con
 void osmaposl_apply(b200rt_projector& h, float* x, float* u, const float* sens, int nsub, int subiter,
                     const b200rt_prior* prior, float min_rel, float max_rel, cudaStream_t st);
 int check_mode_prior(b200rt_projector* h, int mode, const b200rt_prior* prior);
+
+// the projection data's size and timing-bin stride in the projector's layout (a view shard's, or the full one)
+inline bool sharded(const b200rt_projector& h) { return !h.shard_views.empty(); }
+inline int64_t pd_size(const b200rt_projector& h) { return sharded(h) ? h.shard_pd_size : h.geo->projdata_size(); }
+inline int64_t pd_tof_stride(const b200rt_projector& h) { return sharded(h) ? h.shard_tof_stride : h.geo->tof_stride(); }
+// entry points that address the full projection data refuse a view shard
+int refuse_shard(b200rt_projector* h, const char* what);
 
 }  // namespace capi

@@ -358,6 +358,7 @@ int b200rt_batch_add_frame(b200rt_batch* b, b200rt_projector* h, float* estimate
                            const float* additive_dev, const float* const* sensitivity_devs, int num_subsets,
                            int start_subset, int num_subiterations, int zero_seg0_end_planes, const b200rt_prior* prior,
                            float min_relative_change, float max_relative_change, int* frame) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_batch_add_frame");
   if (!b) return B200RT_ERR_INVALID_ARGUMENT;
   if (!h || !estimate_dev || !y_dev || !sensitivity_devs) return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (h->device != b->device) return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "projector is on another device");

@@ -9,7 +9,7 @@ namespace {
 int check_batch(b200rt_projector* h, int batch, int64_t image_stride, int64_t pd_stride) {
   if (batch < 1 || batch > 65535) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "batch must be 1..65535");
   const Geometry& g = *h->geo;
-  if (batch > 1 && (image_stride < g.image_size() || pd_stride < g.projdata_size()))
+  if (batch > 1 && (image_stride < g.image_size() || pd_stride < pd_size(*h)))
     return fail(h, B200RT_ERR_INVALID_ARGUMENT, "batch strides smaller than an image / the projection data");
   return B200RT_OK;
 }
@@ -25,7 +25,7 @@ float* batch_thresholds(b200rt_projector& h, const float* y, int64_t y_stride, i
   const int* views = subset_views(h, subset, nsub, nv);
   for (int b = 0; b < nsets; ++b)
     ck(launch_viewgram_small_values(y + b * y_stride, h.segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_ends,
-                                    g.num_tof(), g.tof_stride(), h.small_value.p + b * nsv, st),
+                                    g.num_tof(), pd_tof_stride(h), h.small_value.p + b * nsv, st, h.params.view_slot),
        "viewgram thresholds");
   sv_stride = y_stride ? nsv : 0;
   return h.small_value.p;
@@ -97,7 +97,7 @@ int b200rt_log_likelihood_batch_dev(b200rt_projector* h, const float* images_dev
                                     void* stream) {
   if (!h || !images_dev || !y_dev || !values) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
-  if (int st = check_batch(h, batch, image_stride, h->geo->projdata_size())) return st;
+  if (int st = check_batch(h, batch, image_stride, pd_size(*h))) return st;
   if (!h->use_paths) {  // the per-basic-bin and TOF-grouped kernels take one image at a time
     for (int b = 0; b < batch; ++b)
       if (int st = b200rt_log_likelihood_dev(h, images_dev + b * image_stride, y_dev + b * y_stride,
@@ -147,7 +147,7 @@ int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* i
                                              void* stream) {
   if (!h || !images_dev || !y_dev || !gradients_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
-  if (int st = check_batch(h, batch, std::min(image_stride, gradient_stride), h->geo->projdata_size())) return st;
+  if (int st = check_batch(h, batch, std::min(image_stride, gradient_stride), pd_size(*h))) return st;
   if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
     return fail(h, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
   if (!h->use_paths || back_projection_mode != B200RT_BACKPROJECT_ATOMIC) {
@@ -167,7 +167,7 @@ int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* i
     int n = 0;
     const int* list = path_list(*h, subset_num, num_subsets, n);
     // the gradient ratios of every image: projection data outside the subset stay zero (never written)
-    const size_t need = static_cast<size_t>(g.projdata_size()) * batch;
+    const size_t need = static_cast<size_t>(pd_size(*h)) * batch;
     if (h->ratio_batch.n < need) {
       h->ratio_batch.alloc(need);
       ck(cudaMemsetAsync(h->ratio_batch.p, 0, sizeof(float) * need, st), "memset");
@@ -187,11 +187,11 @@ int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* i
     ep.small_value = batch_thresholds(*h, y_dev, y_stride, batch, subset_num, num_subsets, zero_seg0_end_planes, st,
                                       ep.sv_stride);
     ck(launch_forward_paths_batch(h->params, h->pparams, list, n, images_dev, image_stride, h->ratio_batch.p,
-                                  g.projdata_size(), batch, st, &ep),
+                                  pd_size(*h), batch, st, &ep),
        "forward projection");
     for (int b = 0; b < batch; ++b)
       ck(cudaMemsetAsync(gradients_dev + b * gradient_stride, 0, sizeof(float) * g.image_size(), st), "memset");
-    ck(launch_back_paths_atomic_batch(h->params, h->pparams, list, n, h->ratio_batch.p, g.projdata_size(),
+    ck(launch_back_paths_atomic_batch(h->params, h->pparams, list, n, h->ratio_batch.p, pd_size(*h),
                                       gradients_dev, gradient_stride, batch, st, 0),
        "back projection");
     return B200RT_OK;

@@ -84,6 +84,7 @@ int b200rt_listmode_gradient_dev(b200rt_projector* h, const b200rt_lm_event* eve
                                  const float* image_dev, int subset_num, int num_subsets, int has_add,
                                  const float* subset_sensitivity_dev, int accumulate, float* gradient_dev,
                                  void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_listmode_gradient_dev");
   if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
   if (!gradient_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   try {
@@ -115,6 +116,7 @@ int b200rt_listmode_gradient_dev(b200rt_projector* h, const b200rt_lm_event* eve
 int b200rt_listmode_value_dev(b200rt_projector* h, const b200rt_lm_event* events_dev, int64_t num_events,
                               const float* image_dev, int subset_num, int num_subsets, int has_add, double* value,
                               void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_listmode_value_dev");
   if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
   if (!value) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   try {
@@ -149,6 +151,7 @@ int b200rt_listmode_hessian_times_input_dev(b200rt_projector* h, const b200rt_lm
                                             int64_t num_events, const float* image_dev, const float* rhs_dev,
                                             int subset_num, int num_subsets, int has_add, float* output_dev,
                                             void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_listmode_hessian_times_input_dev");
   if (int st = lm_check(h, events_dev, num_events, image_dev, subset_num, num_subsets)) return st;
   if (!rhs_dev || !output_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   try {

@@ -78,6 +78,7 @@ extern "C" int b200rt_log_likelihood_dev_noalloc(b200rt_projector* h, const floa
                                                  const float* additive_dev, const float* mult_dev, int subset_num,
                                                  int num_subsets, int zero_seg0_end_planes, double* out_dev,
                                                  void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_log_likelihood_dev_noalloc");
   if (!h || !image_dev || !y_dev || !out_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
   try {

@@ -10,15 +10,15 @@ void osmaposl_numerator(b200rt_projector& h, const float* x, const float* y, con
                         int zero_ends, int mode, float* u, cudaStream_t st) {
   const Geometry& g = *h.geo;
   if (!h.ratio.p) {
-    h.ratio.alloc(g.projdata_size());
-    ck(cudaMemsetAsync(h.ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");  // bins outside the subset
+    h.ratio.alloc(pd_size(h));
+    ck(cudaMemsetAsync(h.ratio.p, 0, sizeof(float) * pd_size(h), st), "memset");  // bins outside the subset
   }
   h.small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
   h.cancelled.alloc(1);
   int nv = 0;
   const int* views = subset_views(h, subset, nsub, nv);
   ck(launch_viewgram_small_values(y, h.segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_ends, g.num_tof(),
-                                  g.tof_stride(), h.small_value.p, st),
+                                  pd_tof_stride(h), h.small_value.p, st, h.params.view_slot),
      "viewgram thresholds");
   ck(cudaMemsetAsync(h.cancelled.p, 0, sizeof(unsigned int), st), "memset");
   FwdEpilogue ep{};
@@ -148,7 +148,7 @@ int b200rt_log_likelihood_dev(b200rt_projector* h, const float* image_dev, const
     if (h->ll_partials.n < static_cast<size_t>(std::max(n, 1))) h->ll_partials.alloc(std::max(n, 1));
     h->ll_sum.alloc(1);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
-                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
+                                    g.num_tof(), pd_tof_stride(*h), h->small_value.p, st, h->params.view_slot),
        "viewgram thresholds");
     FwdEpilogue ep{};
     ep.mode = kEpiLoglik;
@@ -210,15 +210,15 @@ int b200rt_log_likelihood_gradient_dev(b200rt_projector* h, const float* image_d
     const Geometry& g = *h->geo;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!h->ratio.p) {
-      h->ratio.alloc(g.projdata_size());
-      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+      h->ratio.alloc(pd_size(*h));
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * pd_size(*h), st), "memset");
     }
     h->small_value.alloc(static_cast<size_t>(g.num_tof()) * (2 * g.S() + 1) * g.num_views());
     h->cancelled.alloc(1);
     int nv = 0;
     const int* views = subset_views(*h, subset_num, num_subsets, nv);
     ck(launch_viewgram_small_values(y_dev, h->segs.p, g.S(), g.num_views(), g.num_tang(), views, nv, zero_seg0_end_planes,
-                                    g.num_tof(), g.tof_stride(), h->small_value.p, st),
+                                    g.num_tof(), pd_tof_stride(*h), h->small_value.p, st, h->params.view_slot),
        "viewgram thresholds");
     ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
     FwdEpilogue ep{};
@@ -249,11 +249,11 @@ int b200rt_attenuation_dev(b200rt_projector* h, const float* mu_dev, float* proj
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     const Geometry& g = *h->geo;
     if (!h->ratio.p) {
-      h->ratio.alloc(g.projdata_size());
-      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+      h->ratio.alloc(pd_size(*h));
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * pd_size(*h), st), "memset");
     }
     forward_subset(*h, mu_dev, h->ratio.p, 0, 1, st);
-    ck(launch_attenuation(h->ratio.p, projdata_dev, g.projdata_size(), mode, st), "attenuation");
+    ck(launch_attenuation(h->ratio.p, projdata_dev, pd_size(*h), mode, st), "attenuation");
     return B200RT_OK;
   } catch (const std::exception& e) {
     return fail(h, status_of(e), e.what());
@@ -280,7 +280,7 @@ int b200rt_normalisation_dev(b200rt_projector* h, const b200rt_norm_term* terms,
   try {
     DeviceGuard dg(h->device);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int64_t n = g.projdata_size();
+    const int64_t n = pd_size(*h);
     int step = mode;
     if (mode == B200RT_NORM_FACTORS) {
       ck(launch_fill(projdata_dev, n, 1.f, st), "fill");
@@ -309,6 +309,7 @@ int b200rt_normalisation_dev(b200rt_projector* h, const b200rt_norm_term* terms,
 
 int b200rt_ossps_denominator_dev(b200rt_projector* h, const float* y_dev, const float* norm_dev, float* denominator_dev,
                                  int back_projection_mode, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_ossps_denominator_dev");
   if (!h || !y_dev || !denominator_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_mode_prior(h, back_projection_mode, nullptr)) return st;
   try {
@@ -316,8 +317,8 @@ int b200rt_ossps_denominator_dev(b200rt_projector* h, const float* y_dev, const 
     const Geometry& g = *h->geo;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!h->ratio.p) {
-      h->ratio.alloc(g.projdata_size());
-      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * g.projdata_size(), st), "memset");
+      h->ratio.alloc(pd_size(*h));
+      ck(cudaMemsetAsync(h->ratio.p, 0, sizeof(float) * pd_size(*h), st), "memset");
     }
     if (!h->ones.p) {
       h->ones.alloc(g.image_size());
@@ -346,6 +347,7 @@ int b200rt_ossps_subiteration_dev(b200rt_projector* h, float* estimate_dev, floa
                                   int subset_num, int num_subsets, int subiteration_num, int start_subiteration_num,
                                   int zero_seg0_end_planes, const b200rt_prior* prior, float relaxation_parameter,
                                   float relaxation_gamma, float upper_bound, int back_projection_mode, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_ossps_subiteration_dev");
   if (!h || !estimate_dev || !denominator_dev || !y_dev || !sens_dev)
     return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;

@@ -32,6 +32,7 @@ extern "C" {
 
 int b200rt_get_viewgram(b200rt_projector* h, const float* projdata_dev, int segment_num, int view_num,
                         int timing_pos_num, float* viewgram, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_get_viewgram");
   if (!h || !projdata_dev || !viewgram) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   int64_t off = 0;
   int nax = 0;
@@ -61,6 +62,7 @@ int b200rt_get_viewgram(b200rt_projector* h, const float* projdata_dev, int segm
 
 int b200rt_set_viewgram(b200rt_projector* h, float* projdata_dev, int segment_num, int view_num, int timing_pos_num,
                         const float* viewgram, int accumulate, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_set_viewgram");
   if (!h || !projdata_dev || !viewgram) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   int64_t off = 0;
   int nax = 0;
@@ -122,6 +124,7 @@ int b200rt_back_project_dev(b200rt_projector* h, const float* projdata_dev, floa
 
 int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* projdata_host, int subset_num,
                            int num_subsets) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_forward_project");
   if (!h || !image_host || !projdata_host) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
   try {
@@ -168,6 +171,7 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
 
 int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* image_host, int subset_num,
                         int num_subsets, int mode) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_back_project");
   if (!h || !image_host || !projdata_host) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (int st = check_subset(h, subset_num, num_subsets)) return st;
   if (mode != B200RT_BACKPROJECT_ATOMIC && mode != B200RT_BACKPROJECT_DETERMINISTIC)

@@ -13,6 +13,10 @@ int fail(b200rt_projector* h, int code, const std::string& msg) {
   return code;
 }
 
+int refuse_shard(b200rt_projector* h, const char* what) {
+  return fail(h, B200RT_ERR_STATE, std::string(what) + ": not available on a view shard (b200rt_set_view_shard)");
+}
+
 int status_of(const std::exception& e) {
   if (auto* ce = dynamic_cast<const CudaError*>(&e)) {
     return ce->code == cudaErrorMemoryAllocation ? B200RT_ERR_OUT_OF_MEMORY : B200RT_ERR_CUDA;
@@ -545,6 +549,7 @@ void setup_projector(b200rt_projector& h) {
     sd[s + g.S()].npa = g.npa(s);
   }
   h.segs.upload(sd, h.stream);
+  h.h_segs_full = sd;
 
   ProjParams& p = h.params;
   p.rows = h.rows.p;
@@ -655,8 +660,13 @@ const int* path_list(b200rt_projector& h, int subset, int nsub, int& count) {
     return it->second->p;
   }
   std::vector<int> list;
-  for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i)
-    if (h.h_item_view[i] % nsub == subset) list.push_back(i);
+  for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i) {
+    if (h.h_item_view[i] % nsub != subset) continue;
+    // a view shard skips the items whose lines all write views it does not hold
+    const int ov = h.h_item_out_view.empty() ? -1 : h.h_item_out_view[i];
+    if (sharded(h) && ov >= 0 && h.h_view_slot[ov] < 0) continue;
+    list.push_back(i);
+  }
   auto buf = std::make_unique<DevBuf<int>>();
   buf->upload(list, h.stream);
   ck(cudaStreamSynchronize(h.stream), "path list");
@@ -725,7 +735,7 @@ const int* subset_views(b200rt_projector& h, int subset, int nsub, int& count) {
   }
   std::vector<int> views;
   for (int v = 0; v < g.num_views(); ++v)
-    if (in[v]) views.push_back(v);
+    if (in[v] && (!sharded(h) || h.h_view_slot[v] >= 0)) views.push_back(v);  // a view shard: the views it holds
   auto buf = std::make_unique<DevBuf<int>>();
   buf->upload(views, h.stream);
   ck(cudaStreamSynchronize(h.stream), "subset views");
@@ -773,7 +783,7 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
       ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
     return;
   }
-  h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(g.projdata_size(), ni)), 1));
+  h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(pd_size(h), ni)), 1));
   if (!h.colmax_ready) {
     // largest column sum of A (A^T 1 over every bin): bounds every voxel's sum of |w d| / max|d|
     h.colmax.alloc(1);
@@ -801,7 +811,7 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
     }
     ck(launch_fixed_scale(h.det_bound.p, 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
   } else {
-    ck(launch_fixed_scale(pd, pd ? g.projdata_size() : 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
+    ck(launch_fixed_scale(pd, pd ? pd_size(h) : 1, h.colmax.p, h.det_partial.p, h.fixed_scale.p, st), "scale");
   }
   ck(cudaMemsetAsync(h.acc64.p, 0, sizeof(unsigned long long) * ni, st), "memset");
   if (h.use_paths)
@@ -1025,11 +1035,63 @@ const char* b200rt_last_error(const b200rt_projector* h) {
   return h->err.c_str();
 }
 
+int b200rt_set_view_shard(b200rt_projector* h, const int32_t* views, int num_views) {
+  if (!h) return B200RT_ERR_INVALID_ARGUMENT;
+  if (num_views < 0 || (num_views > 0 && !views)) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null view list");
+  const Geometry& g = *h->geo;
+  if (num_views > 0 && (!h->use_paths || g.num_tof() != 1))
+    return fail(h, B200RT_ERR_UNSUPPORTED, "a view shard needs the column-staged kernels (non-TOF data)");
+  std::vector<int> slot(g.num_views(), -1);
+  for (int i = 0; i < num_views; ++i) {
+    if (views[i] < 0 || views[i] >= g.num_views()) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "view out of range");
+    if (slot[views[i]] >= 0) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "a view listed twice");
+    slot[views[i]] = i;
+  }
+  try {
+    DeviceGuard dg(h->device);
+    ck(cudaStreamSynchronize(h->stream), "view shard");
+    std::vector<SegDev> sd = h->h_segs_full;
+    if (num_views > 0) {
+      int64_t off = 0;
+      for (int s = -g.S(); s <= g.S(); ++s) {
+        sd[s + g.S()].dev_offset = off;
+        off += static_cast<int64_t>(g.nax(s)) * num_views * g.num_tang();
+      }
+      h->shard_tof_stride = off;
+      h->shard_pd_size = off;  // non-TOF
+      h->view_slot_dev.upload(slot, h->stream);
+    } else {
+      h->view_slot_dev.release();
+    }
+    h->segs.upload(sd, h->stream);
+    ck(cudaStreamSynchronize(h->stream), "view shard");
+    h->shard_views.assign(views, views + num_views);
+    h->h_view_slot = slot;
+    h->params.segs = h->segs.p;
+    h->params.view_slot = num_views > 0 ? h->view_slot_dev.p : nullptr;
+    h->params.tof_stride = num_views > 0 ? h->shard_tof_stride : g.tof_stride();
+    // every cached list and scratch sized by the data's layout is rebuilt on first use
+    h->subset_lists.clear();
+    h->subset_counts.clear();
+    h->path_lists.clear();
+    h->path_counts.clear();
+    h->subset_views.clear();
+    h->subset_view_counts.clear();
+    h->view_groups.clear();
+    h->colmax_ready = false;
+    h->ratio.release();
+    h->ratio_batch.release();
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_get_info(const b200rt_projector* h, b200rt_info* out) {
   if (!h || !out) return B200RT_ERR_INVALID_ARGUMENT;
   const Geometry& g = *h->geo;
   std::memset(out, 0, sizeof(*out));
-  out->num_bins = g.projdata_size();
+  out->num_bins = pd_size(*h);
   out->num_image_voxels = g.image_size();
   out->num_basic_bins = static_cast<int64_t>(h->h_bins.size());
   out->num_row_elements = static_cast<int64_t>(h->rows.n);
@@ -1040,7 +1102,7 @@ int b200rt_get_info(const b200rt_projector* h, b200rt_info* out) {
   return B200RT_OK;
 }
 
-int64_t b200rt_projdata_size(const b200rt_projector* h) { return h ? h->geo->projdata_size() : -1; }
+int64_t b200rt_projdata_size(const b200rt_projector* h) { return h ? pd_size(*h) : -1; }
 int64_t b200rt_image_size(const b200rt_projector* h) { return h ? h->geo->image_size() : -1; }
 
 int b200rt_get_row(b200rt_projector* h, int segment, int view, int axial, int tangential, int timing, int32_t* coords_zyx,
@@ -1094,12 +1156,14 @@ int b200rt_image_from_device_layout(b200rt_projector* h, const float* dev, float
   return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
 }
 int b200rt_projdata_to_device_layout(b200rt_projector* h, const float* stir_dev, float* dev, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_to_device_layout");
   if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(h->device);
   const cudaError_t e = projdata_layout(*h->geo, stir_dev, dev, true, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
 }
 int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_from_device_layout");
   if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(h->device);
   const cudaError_t e = projdata_layout(*h->geo, dev, stir_dev, false, static_cast<cudaStream_t>(stream));

@@ -77,6 +77,7 @@ int b200rt_stream_bytes(b200rt_projector* h, const b200rt_stream_format* fmt, in
 
 int b200rt_projdata_from_stream_dev(b200rt_projector* h, const void* stream_dev, int64_t stream_bytes,
                                     const b200rt_stream_format* fmt, float* projdata_dev, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_from_stream_dev");
   if (!h || !stream_dev || !fmt || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   try {
     int64_t n = 0;
@@ -94,6 +95,7 @@ int b200rt_projdata_from_stream_dev(b200rt_projector* h, const void* stream_dev,
 
 int b200rt_projdata_to_stream_dev(b200rt_projector* h, const float* projdata_dev, const b200rt_stream_format* fmt,
                                   void* stream_dev, int64_t stream_bytes, void* stream) {
+  if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_to_stream_dev");
   if (!h || !stream_dev || !fmt || !projdata_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   if (fmt->number_type != B200RT_NUMBER_FLOAT && fmt->number_type != B200RT_NUMBER_DOUBLE)
     return fail(h, B200RT_ERR_UNSUPPORTED, "streams are written as float or double");

@@ -80,6 +80,10 @@ struct ProjParams {
   int min_z, min_y, min_x;
   int max_row_len;
   int uniform_npa;  // planes per axial position if equal for all segments, else 0
+  // a projector holding part of the views (b200rt_set_view_shard): the slot of every view in the device layout of
+  // the projection data (-1: not held), or null when every view is held (slot = view); segs[].dev_offset and
+  // tof_stride then describe the shard's layout [timing bin][segment][slot][tangential][axial]
+  const int* view_slot;
   int max_nax;      // most axial positions of any segment
   // TOF data by basic bin (the TOF-grouped packed kernels): the non-TOF basic rows, every element's weight for
   // each timing bin ([element][timing bin], 0 where the TOF row has no element) and one entry per basic bin
@@ -426,7 +430,7 @@ cudaError_t launch_max(const float* data, int64_t n, float* partial, float* out,
 // out index: ((tof bin - min) * (2S+1) + segment + S) * num_views + view
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
-                                         float* out, cudaStream_t st);
+                                         float* out, cudaStream_t st, const int* view_slot = nullptr);
 int update_num_blocks(int64_t n);
 cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const b200rt_prior* prior,
                           const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,

@@ -23,12 +23,15 @@ __device__ __forceinline__ float warp_max(float v) {
 // one block per (segment, view) of the subset: max over the viewgram of y with segment 0 end planes zeroed
 __global__ void viewgram_small_value_kernel(const float* __restrict__ y, const SegDev* __restrict__ segs, int S, int num_views,
                                             int num_tang, const int* __restrict__ views, int zero_ends, int64_t tof_stride,
-                                            float* __restrict__ out) {
+                                            float* __restrict__ out, const int* __restrict__ view_slot) {
   const int seg = static_cast<int>(blockIdx.y) - S;
   const int view = views[blockIdx.x];
   const int tofi = blockIdx.z;
   const SegDev sd = segs[seg + S];
-  const int64_t base = tofi * tof_stride + sd.dev_offset + static_cast<int64_t>(view) * num_tang * sd.nax;
+  // the viewgram's block in the data's layout (a view shard holds its views at their slots; the caller lists only
+  // held views)
+  const int slot = view_slot ? view_slot[view] : view;
+  const int64_t base = tofi * tof_stride + sd.dev_offset + static_cast<int64_t>(slot) * num_tang * sd.nax;
   const int n = num_tang * sd.nax;
   float m = -INFINITY;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -673,10 +676,10 @@ cudaError_t launch_ossps_update(float* x, float* den, const float* g, float* pg,
 
 cudaError_t launch_viewgram_small_values(const float* y, const SegDev* segs, int S, int num_views, int num_tang,
                                          const int* views, int nviews, int zero_ends, int num_tof, int64_t tof_stride,
-                                         float* out, cudaStream_t st) {
+                                         float* out, cudaStream_t st, const int* view_slot) {
   if (nviews <= 0) return cudaSuccess;
   viewgram_small_value_kernel<<<dim3(nviews, 2 * S + 1, num_tof), 256, 0, st>>>(y, segs, S, num_views, num_tang, views,
-                                                                                  zero_ends, tof_stride, out);
+                                                                                  zero_ends, tof_stride, out, view_slot);
   return cudaGetLastError();
 }
 

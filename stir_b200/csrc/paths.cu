@@ -42,13 +42,15 @@ __device__ __forceinline__ void setup_path_lines(const ProjParams& p, const Path
     const ProjBinDev pb = p.bins[pl.bin];
     PathLineSmem s{};
     const int tang = static_cast<int>(L.tang_sign) * pb.tang;
-    s.active = tang >= p.min_tang && tang <= p.max_tang;
+    // the line's view in the data's layout: a view shard holds some views only, the others' lines are inactive
+    const int slot = p.view_slot ? __ldg(p.view_slot + L.view) : L.view;
+    s.active = tang >= p.min_tang && tang <= p.max_tang && slot >= 0;
     const SegDev sd = p.segs[L.seg + p.S];
     s.nax = sd.nax;
     s.npa = sd.npa;
     s.tofi = pb.tof - p.min_tof;
     s.out_base = static_cast<int64_t>(s.tofi) * p.tof_stride + sd.dev_offset +
-                 (static_cast<int64_t>(L.view) * p.num_tang + (tang - p.min_tang)) * sd.nax;
+                 (static_cast<int64_t>(max(slot, 0)) * p.num_tang + (tang - p.min_tang)) * sd.nax;
     s.elem_off = pl.elem_off;
     s.chunk_off = pl.chunk_off;
     // z index in the image of element z (stored as z + 512): zq ? q - z : z, minus min_z

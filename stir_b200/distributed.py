@@ -3,12 +3,14 @@
 Two ways the hot path shards:
 * independent units (dynamic frames, gates, noise realisations): `shard` gives each rank its own units;
   no collective touches the data path;
-* one large reconstruction: every rank keeps the whole image and its own copy of the projection data,
-  and projects part of each subset.  Subset s of n is the union over ranks r of subset s + r*n of n*R
-  (the basic views v = s mod n split by v mod n*R), so rank r computes the numerator of its part, an
-  all-reduce (sum) combines the numerators (the image-sized exchange STIR's MPI version does with
-  MPI_Reduce, distributed_functions.cxx:933,977), and every rank applies the identical update
-  (no broadcast needed).  Sensitivities and log-likelihood values are combined the same way.
+* one large reconstruction: every rank keeps the whole image and projects part of each subset.  Subset s of n
+  is the union over ranks r of subset s + r*n of n*R (the basic views v = s mod n split by v mod n*R), so rank
+  r computes the numerator of its part, an all-reduce (sum) combines the numerators (the image-sized exchange
+  STIR's MPI version does with MPI_Reduce, distributed_functions.cxx:933,977), and every rank applies the
+  identical update (no broadcast needed).  Sensitivities and log-likelihood values are combined the same way.
+  Each rank holds the projection data (y, additive term, multiplicative factors) of its own views only: its
+  projector is a view shard (`RayTracingProjector.set_view_shard(rank_views(...))`) and its arrays the shard's
+  (`shard_projdata`), 1/R of the whole data.
 
 The per-rank compute is a backend with numerator / apply / sensitivity / log_likelihood methods;
 `B200Backend` runs them on the GPU through the C ABI.
@@ -30,6 +32,34 @@ def shard(units: Sequence, rank: int, world: int) -> List:
 def rank_subset(subset_num: int, num_subsets: int, rank: int, world: int):
     """(subset, number of subsets) of rank `rank`'s part of subset `subset_num` of `num_subsets`."""
     return subset_num + rank * num_subsets, num_subsets * world
+
+
+def rank_views(geometry, num_subsets: int, rank: int, world: int, bits: int = None) -> List[int]:
+    """The views whose projection data rank `rank` of `world` needs when every subset s of `num_subsets` is split as
+    subset s + rank * num_subsets of num_subsets * world: the union of those sub-subsets' views (their basic views
+    and every view related to them by the symmetries `bits`, b200rt_info.symmetries_used).  The ranks' view sets
+    partition the views."""
+    from .subsets import views_in_subset
+    out = set()
+    for s in range(num_subsets):
+        out.update(views_in_subset(geometry, *rank_subset(s, num_subsets, rank, world), bits=bits))
+    return sorted(out)
+
+
+def shard_projdata(pdi, data, views):
+    """The part of device-layout projection data `data` (non-TOF, [segment -S..S][view][tangential][axial]) that a
+    view shard holding `views` (in that order) uses: [segment][slot][tangential][axial]."""
+    import torch
+    S = pdi.max_segment_num
+    nv, nt = pdi.num_views, pdi.num_tangential_poss
+    idx = torch.as_tensor(list(views), dtype=torch.long, device=data.device)
+    parts, off = [], 0
+    for seg in range(-S, S + 1):
+        nax = pdi.get_num_axial_poss(seg)
+        n = nv * nt * nax
+        parts.append(data[off:off + n].view(nv, nt * nax).index_select(0, idx).reshape(-1))
+        off += n
+    return torch.cat(parts)
 
 
 def _p(t):

@@ -56,6 +56,25 @@ class RayTracingProjector:
         _abi.check(self.lib.b200rt_get_info(self.h, ctypes.byref(info)), self.h, "b200rt_get_info")
         self.info = info
         self._non_tof = None
+        self.shard_views = None
+
+    def set_view_shard(self, views=None):
+        """Hold the projection data of `views` only (b200rt_set_view_shard): projection-data arrays then have the
+        shard's size (`projdata_size`), in the device layout with the views in the order given; None restores the
+        whole data."""
+        import numpy as np
+        if views is None or len(views) == 0:
+            _abi.check(self.lib.b200rt_set_view_shard(self.h, None, 0), self.h, "b200rt_set_view_shard")
+            self.shard_views = None
+        else:
+            v = np.ascontiguousarray(views, np.int32)
+            _abi.check(self.lib.b200rt_set_view_shard(self.h, v.ctypes.data_as(ctypes.c_void_p), len(v)), self.h,
+                       "b200rt_set_view_shard")
+            self.shard_views = [int(a) for a in v]
+        info = _abi.Info()
+        _abi.check(self.lib.b200rt_get_info(self.h, ctypes.byref(info)), self.h, "b200rt_get_info")
+        self.info = info
+        return self
 
     def non_tof_projector(self) -> "RayTracingProjector":
         """This projector without timing bins (ProjDataInfo::create_non_tof_clone, the same matrix settings); itself

@@ -94,3 +94,16 @@ def test_two_ranks_gloo_match_single_process(tmp_path):
     ll = float(np.load(tmp_path / "ll0.npy")[0])
     ref = orc.log_likelihood(xr, y, add, None, 1, 6)
     assert abs(ll - ref) <= 1e-6 * abs(ref)
+
+
+def test_rank_views_partition_the_views():
+    """The views each rank holds under the view split of every subset are disjoint and cover every view."""
+    from stir_b200 import geometry as G
+    from stir_b200.distributed import rank_views
+    from stir_b200.subsets import SYM_180, SYM_90
+    for pdi, img, nsub, world in [(*G.small_3d_pet(), 6, 2), (*G.clinical_3d_pet(), 21, 4), (*G.clinical_3d_pet(), 7, 3)]:
+        geo = G.make_geometry(pdi, img)
+        parts = [rank_views(geo, nsub, r, world, SYM_90 | SYM_180) for r in range(world)]
+        allv = sorted(v for p in parts for v in p)
+        assert allv == list(range(pdi.num_views)), (nsub, world)
+        assert all(len(p) > 0 for p in parts)

@@ -297,15 +297,38 @@ def test_differentiable_projector_batch(half, oracle_lib):
             int(rng.integers(1, nz - 1))
         if xh[k, yy - 1:yy + 2, xx - 1:xx + 2, zz - 1:zz + 2].min() >= 0.05:
             picks.append((k, yy, xx, zz))
-    for k, yy, xx, zz in picks:
-        Lk = PoissonLogLikelihood(proj, y[k], add[k], m)
+    # The log-likelihood along a voxel's direction is evaluated in double from the float projections A x and A e_v
+    # (ybar(x +- h e_v) = m (A x +- h A e_v + a)), with STIR's clipping and thresholds: re-projecting x +- h in
+    # float would add rounding noise of about one unit in the last place of A x (~1e-5 of ~150) per LOR against a
+    # change of 2e-3, which over the ~1e4 LORs through a voxel is as large as the tolerance.
+    S, nvw, nt = proj.proj_data_info.max_segment_num, proj.proj_data_info.num_views, proj.proj_data_info.num_tangential_poss
+    def thresholds(yk):  # max over each viewgram x 1e-6 (divide_and_truncate's small value), per bin
+        parts, off = [], 0
+        for seg in range(-S, S + 1):
+            nax = proj.proj_data_info.get_num_axial_poss(seg)
+            blk = yk[off:off + nvw * nt * nax].view(nvw, nt * nax)
+            parts.append((blk.max(dim=1, keepdim=True).values * 1e-6).clamp(min=0).expand(-1, nt * nax).reshape(-1))
+            off += nvw * nt * nax
+        return torch.cat(parts)
 
-        def f(t):
-            return float(Lk(t)) - float(R(t))
+    def loglik(ybar, yk, sv):
+        ne = torch.maximum(ybar, yk / 1e4)
+        return float(torch.where(yk <= sv, -ne, yk * torch.log(ne) - ne).sum())
+    for k, yy, xx, zz in picks:
+        yk = y[k].double()
+        sv = thresholds(y[k]).double()
+        ax = proj.forward_dev(x[k]).double()
+        e = torch.zeros_like(x[k])
+        e[yy, xx, zz] = 1.0
+        col = proj.forward_dev(e).double()
+        sel = col != 0
+        md, ad = m.double()[sel], add[k].double()[sel]
+        lp = loglik(md * (ax[sel] + h * col[sel] + ad), yk[sel], sv[sel])
+        lm = loglik(md * (ax[sel] - h * col[sel] + ad), yk[sel], sv[sel])
         xp, xm = x[k].clone(), x[k].clone()
         xp[yy, xx, zz] += h
         xm[yy, xx, zz] -= h
-        num = (f(xp) - f(xm)) / (2 * h)
+        num = ((lp - lm) - (float(R(xp)) - float(R(xm)))) / (2 * h)
         assert abs(num - float(grad[k, yy, xx, zz])) <= tol, (k, yy, xx, zz, num, float(grad[k, yy, xx, zz]))
     # gradients against the oracle: the log-likelihood's on subset 0 of 42 (bounded CPU time), the prior's
     orc = oracle_lib.Oracle(proj.geometry)

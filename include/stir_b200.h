@@ -417,6 +417,11 @@ int b200rt_batch_add_frame(b200rt_batch* b, b200rt_projector* h, float* estimate
                            const float* additive_dev, const float* const* sensitivity_devs, int num_subsets,
                            int start_subset, int num_subiterations, int zero_seg0_end_planes, const b200rt_prior* prior,
                            float min_relative_change, float max_relative_change, int* frame);
+/* Back projection of a frame: B200RT_BACKPROJECT_ATOMIC (the default) or B200RT_BACKPROJECT_DETERMINISTIC, whose
+ * numerator is the same 64-bit fixed-point sum as b200rt_osmaposl_subiteration_dev's in that mode (scale from the
+ * ratio's bound 1e4), so the frame's reconstruction is bit-reproducible and equal to its own one-frame run.
+ * Deterministic frames need the column-staged kernels (non-TOF projectors; B200RT_ERR_UNSUPPORTED otherwise). */
+int b200rt_batch_set_frame_mode(b200rt_batch* b, int frame, int back_projection_mode);
 int b200rt_batch_num_frames(const b200rt_batch* b);
 /* Runs batched sub-iterations first..first+count-1 on `stream`.  use_graph != 0: the sequence is
  * captured once into a CUDA graph (kept per (first, count) until a frame is added or the

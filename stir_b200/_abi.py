@@ -252,6 +252,7 @@ EXPORTS = [
     ("b200rt_batch_create", _I, [_I, ctypes.POINTER(_P)]),
     ("b200rt_batch_destroy", None, [_P]),
     ("b200rt_batch_last_error", ctypes.c_char_p, [_P]),
+    ("b200rt_batch_set_frame_mode", _I, [_P, _I, _I]),
     ("b200rt_batch_add_frame", _I, [_P, _P, _P, _P, _P, ctypes.POINTER(_P), _I, _I, _I, _I, ctypes.POINTER(Prior),
                                     ctypes.c_float, ctypes.c_float, ctypes.POINTER(_I)]),
     ("b200rt_batch_num_frames", _I, [_P]),

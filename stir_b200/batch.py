@@ -8,8 +8,8 @@ k advances each frame that has k or more sub-iterations by its own sub-iteration
 runs one persistent forward launch and one persistent back projection over the subsets of all frames,
 optionally captured with the per-frame thresholds and updates into one CUDA graph.
 
-The result of each frame equals OSMAPOSLReconstruction.reconstruct with the atomic back projection up
-to the order of float additions in the back projection.
+The result of each frame equals OSMAPOSLReconstruction.reconstruct: with the atomic back projection up to the
+order of float additions in the back projection, with the deterministic one bit for bit.
 """
 from __future__ import annotations
 
@@ -38,11 +38,11 @@ class BatchedOSMAPOSL:
 
     def add(self, recon: OSMAPOSLReconstruction, x) -> int:
         """Adds recon with estimate x (device layout, updated in place).  recon runs its sub-iterations
-        1..num_subiterations; it must start at sub-iteration 1 and use the atomic back projection."""
+        1..num_subiterations; it must start at sub-iteration 1.  A deterministic back projection (recon's
+        back_projection_mode) makes the frame bit-reproducible and equal to its own one-frame run (non-TOF
+        projectors)."""
         if recon.start_subiteration_num != 1:
             raise ValueError("a batched frame starts at sub-iteration 1")
-        if recon.mode != _abi.BACKPROJECT_ATOMIC:
-            raise ValueError("batched reconstructions use the atomic back projection")
         if recon.sensitivities is None:
             recon.set_up()
         if recon.enforce_initial_positivity:
@@ -54,6 +54,8 @@ class BatchedOSMAPOSL:
             self.b, recon.proj.h, _ptr(x), _ptr(recon.y), _ptr(recon.additive), sens, recon.num_subsets,
             recon.start_subset_num, recon.num_subiterations, int(recon.zero_seg0_end_planes), prior,
             float(recon.min_rel), float(recon.max_rel), ctypes.byref(idx)), "b200rt_batch_add_frame")
+        if recon.mode != _abi.BACKPROJECT_ATOMIC:
+            self._check(self.lib.b200rt_batch_set_frame_mode(self.b, idx.value, recon.mode), "b200rt_batch_set_frame_mode")
         self.frames.append((recon, x, sens))
         return idx.value
 

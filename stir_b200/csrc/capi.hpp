@@ -193,6 +193,7 @@ void prior_weights(const Geometry& g, int only_2D, float w[27]);
 void back_project_into(b200rt_projector& h, const float* pd, float* image, int subset, int nsub, int mode, int zero_ends,
                        cudaStream_t st, float max_abs = 0.f);
 int check_subset(b200rt_projector* h, int subset, int nsub);
+void ensure_colmax(b200rt_projector& h, float* scratch, cudaStream_t st);
 cudaError_t projdata_layout(const Geometry& g, const float* in, float* out, bool to_dev, cudaStream_t st);
 cudaError_t projdata_layout_views(const Geometry& g, const float* in, float* out, bool to_dev, int v0, int v1,
                                   cudaStream_t st);

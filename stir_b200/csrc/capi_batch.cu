@@ -28,6 +28,12 @@ struct b200rt_batch {
     float min_rel = 0.f, max_rel = 0.f;
     DevBuf<float> ratio, u, grad, small_value, partial_max, umax;
     DevBuf<unsigned int> cancelled;
+    // B200RT_BACKPROJECT_DETERMINISTIC: fixed-point numerator, its scale (from the ratio's bound 1e4 and the
+    // projector's largest column sum, as the frame's own back projection), the bound and a reduction scratch
+    int mode = B200RT_BACKPROJECT_ATOMIC;
+    DevBuf<unsigned long long> acc64;
+    DevBuf<double> fixed_scale;
+    DevBuf<float> bound, det_partial;
   };
   int device = 0;
   std::string err;
@@ -126,11 +132,23 @@ void batch_finalize(b200rt_batch& b) {
       int nv = 0;
       subset_views(*f.h, 0, 1, nv);  // all views, for the thresholds
     }
+    if (f.mode == B200RT_BACKPROJECT_DETERMINISTIC) {
+      if (!b.paths) throw std::invalid_argument("deterministic batched frames need the column-staged kernels");
+      f.acc64.alloc(g.image_size());
+      f.fixed_scale.alloc(1);
+      f.det_partial.alloc(1);
+      const float bound = 10000.F;  // the ratio's clip (divide_and_truncate): the scale does not depend on data
+      f.bound.upload(std::vector<float>{bound}, st);
+      ensure_colmax(*f.h, f.u.p, st);
+      ck(launch_fixed_scale(f.bound.p, 1, f.h->colmax.p, f.det_partial.p, f.fixed_scale.p, st), "scale");
+    }
     BatchFrameDev d{};
     d.geom = f.geom;
     d.x = f.x;
     d.ratio = f.ratio.p;
     d.u = f.u.p;
+    d.acc64 = f.mode == B200RT_BACKPROJECT_DETERMINISTIC ? f.acc64.p : nullptr;
+    d.fixed_scale = f.mode == B200RT_BACKPROJECT_DETERMINISTIC ? f.fixed_scale.p : nullptr;
     d.ep.mode = b200::kEpiRatio;
     d.ep.zero_ends = f.zero_ends;
     d.ep.y = f.y;
@@ -237,7 +255,10 @@ void batch_zero(b200rt_batch& b, int k, cudaStream_t st) {
     auto& f = *fp;
     if (k > f.num_subiters) continue;
     ck(cudaMemsetAsync(f.cancelled.p, 0, sizeof(unsigned int), st), "memset");
-    ck(cudaMemsetAsync(f.u.p, 0, sizeof(float) * f.h->geo->image_size(), st), "memset");
+    if (f.mode == B200RT_BACKPROJECT_DETERMINISTIC)
+      ck(cudaMemsetAsync(f.acc64.p, 0, sizeof(unsigned long long) * f.h->geo->image_size(), st), "memset");
+    else
+      ck(cudaMemsetAsync(f.u.p, 0, sizeof(float) * f.h->geo->image_size(), st), "memset");
   }
 }
 
@@ -303,6 +324,9 @@ const b200::BatchUpdateDev* batch_updates(b200rt_batch& b, int k, int& count, in
 void batch_subiteration(b200rt_batch& b, int k, cudaStream_t st) {
   batch_zero(b, k, st);
   batch_projections(b, k, st);
+  for (auto& fp : b.frames)  // deterministic frames: their fixed-point numerators to float
+    if (k <= fp->num_subiters && fp->mode == B200RT_BACKPROJECT_DETERMINISTIC)
+      ck(launch_fixed_to_float(fp->acc64.p, fp->fixed_scale.p, fp->u.p, fp->h->geo->image_size(), st), "numerator");
   // every frame's update (OSMAPOSLReconstruction.cxx:394-510) in three launches
   int n = 0, max_blocks = 1;
   const b200::BatchUpdateDev* upd = batch_updates(b, k, n, max_blocks);
@@ -353,6 +377,19 @@ void b200rt_batch_destroy(b200rt_batch* b) {
 const char* b200rt_batch_last_error(const b200rt_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 int b200rt_batch_num_frames(const b200rt_batch* b) { return b ? static_cast<int>(b->frames.size()) : 0; }
+
+int b200rt_batch_set_frame_mode(b200rt_batch* b, int frame, int back_projection_mode) {
+  if (!b) return B200RT_ERR_INVALID_ARGUMENT;
+  if (frame < 0 || frame >= static_cast<int>(b->frames.size())) return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "no such frame");
+  if (back_projection_mode != B200RT_BACKPROJECT_ATOMIC && back_projection_mode != B200RT_BACKPROJECT_DETERMINISTIC)
+    return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "unknown back-projection mode");
+  if (back_projection_mode == B200RT_BACKPROJECT_DETERMINISTIC && !b->frames[frame]->h->use_paths)
+    return bfail(b, B200RT_ERR_UNSUPPORTED, "deterministic batched frames need the column-staged kernels (non-TOF)");
+  b->frames[frame]->mode = back_projection_mode;
+  drop_graphs(*b);
+  b->ready = false;
+  return B200RT_OK;
+}
 
 int b200rt_batch_add_frame(b200rt_batch* b, b200rt_projector* h, float* estimate_dev, const float* y_dev,
                            const float* additive_dev, const float* const* sensitivity_devs, int num_subsets,

@@ -764,6 +764,30 @@ void prior_weights(const Geometry& g, int only_2D, float w[27]) {
 // Back projection of the subset into image_dev (overwritten), atomic or deterministic.
 // max_abs > 0: a bound on |pd| known in advance (the OSMAPOSL ratio is at most 1e4), which keeps the
 // fixed-point scale independent of bins outside the subset
+// the largest column sum of A (A^T 1 over every bin), which bounds every voxel's sum of |w d| / max|d| (the fixed-point
+// scale of the deterministic back projection); `scratch` is an image-sized buffer
+void ensure_colmax(b200rt_projector& h, float* scratch, cudaStream_t st) {
+  const Geometry& g = *h.geo;
+  const int64_t ni = g.image_size();
+  h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(pd_size(h), ni)), 1));
+  if (h.colmax_ready) return;
+  const bool grouped = !h.use_paths && h.params.tof_w;
+  h.colmax.alloc(1);
+  int nall = 0;
+  const int* all = h.use_paths ? path_list(h, 0, 1, nall)
+                   : grouped   ? tof_group_list(h, 0, 1, nall)
+                               : subset_list(h, 0, 1, nall);
+  ck(cudaMemsetAsync(scratch, 0, sizeof(float) * ni, st), "memset");
+  if (h.use_paths)
+    ck(launch_back_paths_atomic(h.params, h.pparams, all, nall, nullptr, scratch, st, 0), "column sums");
+  else if (grouped)
+    ck(launch_back_tof_grouped(h.params, all, nall, nullptr, scratch, nullptr, nullptr, st, 0), "column sums");
+  else
+    ck(launch_back_atomic(h.params, all, nall, nullptr, scratch, st, 0), "column sums");
+  ck(launch_max(scratch, ni, h.det_partial.p, h.colmax.p, st), "column sums");
+  h.colmax_ready = true;
+}
+
 void back_project_into(b200rt_projector& h, const float* pd, float* image, int subset, int nsub, int mode, int zero_ends,
                        cudaStream_t st, float max_abs) {
   const Geometry& g = *h.geo;
@@ -783,24 +807,7 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
       ck(launch_back_atomic(h.params, list, n, pd, image, st, zero_ends), "back projection");
     return;
   }
-  h.det_partial.alloc(std::max<int>(update_num_blocks(std::max<int64_t>(pd_size(h), ni)), 1));
-  if (!h.colmax_ready) {
-    // largest column sum of A (A^T 1 over every bin): bounds every voxel's sum of |w d| / max|d|
-    h.colmax.alloc(1);
-    int nall = 0;
-    const int* all = h.use_paths ? path_list(h, 0, 1, nall)
-                     : grouped   ? tof_group_list(h, 0, 1, nall)
-                                 : subset_list(h, 0, 1, nall);
-    ck(cudaMemsetAsync(image, 0, sizeof(float) * ni, st), "memset");
-    if (h.use_paths)
-      ck(launch_back_paths_atomic(h.params, h.pparams, all, nall, nullptr, image, st, 0), "column sums");
-    else if (grouped)
-      ck(launch_back_tof_grouped(h.params, all, nall, nullptr, image, nullptr, nullptr, st, 0), "column sums");
-    else
-      ck(launch_back_atomic(h.params, all, nall, nullptr, image, st, 0), "column sums");
-    ck(launch_max(image, ni, h.det_partial.p, h.colmax.p, st), "column sums");
-    h.colmax_ready = true;
-  }
+  ensure_colmax(h, image, st);
   h.acc64.alloc(ni);
   h.fixed_scale.alloc(1);
   if (max_abs > 0) {

@@ -128,6 +128,9 @@ struct BatchFrameDev {
   float* ratio;
   float* u;
   FwdEpilogue ep;
+  // deterministic back projection of this frame: 64-bit fixed-point sums and their scale (null: float atomics)
+  unsigned long long* acc64;
+  const double* fixed_scale;
 };
 struct BatchItem {
   int frame;

@@ -709,8 +709,15 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtasBack)
                             unsigned* counter) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ BatchPathStage st;
-  while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st))
-    back_path_item<FloatCols>(st.p, st.pp, st.it, smem, st.f.ratio, FloatCols{st.f.u}, 0);
+  while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st)) {
+    if (st.f.acc64) {  // a deterministic frame: the same fixed-point integers as its own back projection
+      FixedCols acc{st.f.acc64, st.f.fixed_scale, 0.0};
+      acc.load();
+      back_path_item<FixedCols>(st.p, st.pp, st.it, smem, st.f.ratio, acc, 0);
+    } else {
+      back_path_item<FloatCols>(st.p, st.pp, st.it, smem, st.f.ratio, FloatCols{st.f.u}, 0);
+    }
+  }
 }
 
 const void* forward_batch_paths_fn(int npa) {

@@ -145,9 +145,6 @@ def test_batch_rejects_bad_frames(frames):
     batch = BatchedOSMAPOSL()
     proj = frames[sp["geom"]][0]
     x = proj.empty_image().fill_(1.0)
-    rec = _recon(frames, sp, back_projection_mode=_abi.BACKPROJECT_DETERMINISTIC)
-    with pytest.raises(ValueError):
-        batch.add(rec, x)
     rec = _recon(frames, sp, start_subiteration_num=2)
     with pytest.raises(ValueError):
         batch.add(rec, x)
@@ -192,3 +189,41 @@ def test_batch_tof_frames_equal_frame_by_frame(cuda_device):
     for x, xr in runs:
         assert rel_l2(x.cpu().numpy(), xr.cpu().numpy()) < BATCH_TOL
     batch.close()
+
+
+def test_batch_deterministic_strong_prior_is_bit_reproducible(frames):
+    """Frames with a strong one-step-late prior (QP beta 0.5, which multiplies float-rounding differences about
+    tenfold per sub-iteration) and the deterministic back projection: the batched reconstruction equals each frame's
+    own deterministic reconstruction bit for bit, and a second batched run repeats it."""
+    import torch
+    from stir_b200 import _abi
+    from stir_b200.batch import BatchedOSMAPOSL
+    from stir_b200.osmaposl import OSMAPOSLReconstruction, QuadraticPrior
+    mode = _abi.BACKPROJECT_DETERMINISTIC
+    specs = [("fine", 3, 6), ("coarse", 4, 5), ("fine", 2, 4)]
+    refs, recs = [], []
+    for geom, nsub, n in specs:
+        proj, y, add = frames[geom]
+        ref = OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n,
+                                     prior=QuadraticPrior(0.5), back_projection_mode=mode).set_up()
+        xr = proj.empty_image().fill_(1.0)
+        ref.reconstruct(xr)
+        refs.append(xr)
+        recs.append((proj, OSMAPOSLReconstruction(proj, y, additive=add, num_subsets=nsub, num_subiterations=n,
+                                                  prior=QuadraticPrior(0.5), back_projection_mode=mode), ref))
+    outs = []
+    for run in range(2):
+        batch = BatchedOSMAPOSL()
+        xs = []
+        for proj, rec, ref in recs:
+            rec.sensitivities = ref.sensitivities
+            x = proj.empty_image().fill_(1.0)
+            batch.add(rec, x)
+            xs.append(x)
+        batch.reconstruct(use_graph=bool(run))
+        torch.cuda.synchronize()
+        outs.append([x.clone() for x in xs])
+        batch.close()
+    for a, b, r in zip(outs[0], outs[1], refs):
+        assert torch.equal(a, b)
+        assert torch.equal(a, r)

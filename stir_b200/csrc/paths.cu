@@ -441,8 +441,7 @@ __device__ __forceinline__ void back_span(const ProjParams& p, const PathParams&
       eb[lane] = make_int4(__float_as_int(v), off1, off2, static_cast<int>(pk));
     }
     __syncwarp();
-    for (int i = 0; i < cnt; ++i) {
-      const int4 w = eb[i];
+    auto element = [&](const int4 w, int i) {
       const unsigned pk = static_cast<unsigned>(w.w);
       if (pk & 4u) {
         flush();
@@ -465,7 +464,24 @@ __device__ __forceinline__ void back_span(const ProjParams& p, const PathParams&
       } else if (n == 1) {
         line(ev, w.y);
       }
+    };
+    // two elements at a time: when neither starts a column and each has its basic bin's two lines (the common
+    // case) their four lines run without branches between them; the order of the terms is unchanged
+    int i = 0;
+    for (; i + 1 < cnt; i += 2) {
+      const int4 w0 = eb[i], w1 = eb[i + 1];
+      if ((static_cast<unsigned>(w0.w) & 7u) == 2u && (static_cast<unsigned>(w1.w) & 7u) == 2u) {
+        const float v0 = __int_as_float(w0.x), v1 = __int_as_float(w1.x);
+        line(v0, w0.y);
+        line(v0, w0.z);
+        line(v1, w1.y);
+        line(v1, w1.z);
+      } else {
+        element(w0, i);
+        element(w1, i + 1);
+      }
     }
+    if (i < cnt) element(eb[i], i);
   }
   flush();
 }

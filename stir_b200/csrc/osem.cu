@@ -297,7 +297,8 @@ __global__ void absmax_kernel(const float* __restrict__ data, int64_t n, float* 
 }
 
 // scale = 2^floor(62 - log2(bound)): every partial sum of |w d| over a voxel is at most
-// max|d| * max column sum of A, so the int64 accumulator cannot overflow
+// max|d| * max column sum of A, so the int64 accumulator cannot overflow.  The exponent is capped at 126 so that
+// the scale is also a normal float (data whose bound is under 2^-64 keep 62 bits above 2^-126)
 __global__ void fixed_scale_kernel(const float* __restrict__ partial, int n, const float* __restrict__ colmax,
                                    double* __restrict__ scale) {
   float m = 0.f;
@@ -310,7 +311,7 @@ __global__ void fixed_scale_kernel(const float* __restrict__ partial, int n, con
     float t = 0.f;
     for (int w = 0; w < (blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
     const double bound = static_cast<double>(t) * static_cast<double>(*colmax) * 1.01 + 1e-30;
-    *scale = exp2(fmin(floor(62.0 - log2(bound)), 1000.0));
+    *scale = exp2(fmin(floor(62.0 - log2(bound)), 126.0));
   }
 }
 

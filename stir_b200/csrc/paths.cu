@@ -356,10 +356,16 @@ struct FixedCols {
   unsigned long long* acc;
   const double* scale_ptr;  // 2^k of the fixed-point format, computed on the device
   double scale;
-  __device__ __forceinline__ void load() { scale = *scale_ptr; }
+  float scale_f;  // the same power of two as a float
+  __device__ __forceinline__ void load() {
+    scale = *scale_ptr;
+    scale_f = static_cast<float>(scale);
+  }
   __device__ __forceinline__ void offset(int64_t) {}  // one image per launch
-  // the same rounding of each contribution as the per-basic-bin fixed-point kernel
-  __device__ __forceinline__ T term(float v) const { return __double2ll_rn(static_cast<double>(v) * scale); }
+  // the same rounding of each contribution as the per-basic-bin fixed-point kernel: the scale is a power of two of
+  // at most 2^126 and |v| x scale <= 2^62, so v x scale is exact in float as in double and rounds to the same
+  // integer, without the double multiply
+  __device__ __forceinline__ T term(float v) const { return __float2ll_rn(v * scale_f); }
   __device__ __forceinline__ void flush(int64_t i, long long v) const {
     if (v != 0) atomicAdd(acc + i, static_cast<unsigned long long>(v));
   }
@@ -727,7 +733,7 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtasBack)
   __shared__ BatchPathStage st;
   while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st)) {
     if (st.f.acc64) {  // a deterministic frame: the same fixed-point integers as its own back projection
-      FixedCols acc{st.f.acc64, st.f.fixed_scale, 0.0};
+      FixedCols acc{st.f.acc64, st.f.fixed_scale, 0.0, 0.f};
       acc.load();
       back_path_item<FixedCols>(st.p, st.pp, st.it, smem, st.f.ratio, acc, 0);
     } else {
@@ -860,7 +866,7 @@ cudaError_t launch_back_paths_atomic_batch(const ProjParams& p, const PathParams
 cudaError_t launch_back_paths_fixed(const ProjParams& p, const PathParams& pp, const int* items, int nitems,
                                     const float* projdata, unsigned long long* acc, const double* scale,
                                     cudaStream_t st, int zero_ends) {
-  return launch_back_paths(p, pp, items, nitems, projdata, 0, FixedCols{acc, scale, 0.0}, 0, 1, st, zero_ends);
+  return launch_back_paths(p, pp, items, nitems, projdata, 0, FixedCols{acc, scale, 0.0, 0.f}, 0, 1, st, zero_ends);
 }
 
 }  // namespace b200

@@ -817,7 +817,7 @@ def b200_main(args):
             "l2_hit_rate": {FWD_KERNEL: profile_value("l2_hit_rate", FWD_KERNEL),
                             BACK_KERNEL: profile_value("l2_hit_rate", BACK_KERNEL)}}
 
-    roof["byte_model"] = ("algorithmic bytes (SURVEY 8d): every (row element, LOR) pair counted as a 4-byte image read "
+    roof["byte_model"] = ("algorithmic bytes: every (row element, LOR) pair counted as a 4-byte image read "
                           "(forward) or an 8-byte read-modify-write (back); the column staging serves them from shared "
                           "memory and L2, so frac above 1 says the kernel avoids DRAM, not that it beats the copy "
                           "bandwidth; the compulsory-bytes fractions (image and projection data once) and the on-chip "

@@ -436,7 +436,18 @@ def tof_workload(with_cpu, device):
         res = {"metric": "TOF fwd+back TOF-bin LORs/s", "value": n / ((fms + bms) / 1e3), "unit": "LORs/s",
                "tof_bins_per_step": n, "forward_ms": fms, "back_ms": bms, "setup_s": setup_s, "gpu_launches": 2,
                "workload": "8 rings x 288 det (R 300 mm), span 1, 144 views x 64 tang, 33 timing bins of 50 ps, "
-                           "Gaussian 550 ps FWHM (STIR truncation), image 64x64x15; per-basic-bin TOF kernels"}
+                           "Gaussian 550 ps FWHM (STIR's kernel cut-off), image 64x64x15; TOF-grouped kernels",
+               "row_elements": int(proj.info.total_nnz)}
+        # the same with the Gaussian truncated at +-3 sigma (the kernel of the TOF configuration) beside STIR's cut-off
+        p3 = RayTracingProjector(pdi, img, device=device, tof_kernel_truncation_sigmas=3.0)
+        try:
+            f3 = time_dev(lambda: p3.forward_dev(x, pd))
+            b3 = time_dev(lambda: p3.back_dev(y, bk))
+            res["truncated_3_sigma"] = {"value": n / ((f3 + b3) / 1e3), "unit": "LORs/s", "forward_ms": f3,
+                                        "back_ms": b3, "row_elements": int(p3.info.total_nnz),
+                                        "kernel": "Gaussian truncated at +-3 sigma, bins integrate its inner part"}
+        finally:
+            p3.close()
         res["batched"] = tof_batched_reconstructions(proj)
         if with_cpu:
             from oracle.oracle import Oracle

@@ -116,6 +116,11 @@ typedef struct b200rt_geometry {
   int32_t do_symmetry_swap_segment;
   int32_t do_symmetry_swap_s;
   int32_t do_symmetry_shift_z;
+  /* TOF kernel cut-off.  0: STIR's (ProjMatrixByBin.inl:187-197: a timing bin gets 0 when both its ends lie at
+   * least 4 sqrt(2) sigma = 5.66 sigma from the voxel on the same side, otherwise the whole Gaussian's integral over
+   * the bin).  k > 0 (no STIR counterpart): the Gaussian truncated at +-k sigma, each timing bin getting the integral
+   * of the kernel over its part of [-k sigma, k sigma], not renormalised. */
+  float tof_kernel_truncation_sigmas;
 } b200rt_geometry;
 
 /* sizes and statistics of a set-up projector */
@@ -238,6 +243,13 @@ int b200rt_osmaposl_apply_update_dev(b200rt_projector* h, float* estimate_dev, f
 
 /* singularities cancelled by divide_and_truncate in the last sub-iteration (distributable.cxx:590-594); synchronises */
 int b200rt_get_num_cancelled(b200rt_projector* h, int64_t* out);
+
+/* The projector's device status word since creation or the last clear (no STIR counterpart: STIR's projectors run
+ * on the host).  B200RT_STATUS_STAGING_TIMEOUT: a forward projection's bulk copy of image columns into shared memory
+ * was not seen to complete within the kernel's wait limit, so that launch abandoned some path items and its
+ * results are incomplete.  Synchronises; clear != 0 resets the word after reading it. */
+#define B200RT_STATUS_STAGING_TIMEOUT 1u
+int b200rt_get_device_status(b200rt_projector* h, uint32_t* status, int clear);
 
 /* Poisson log-likelihood of one subset (accumulate_loglikelihood, src/buildblock/recon_array_functions.cxx:335-377,
  * RPC_process_related_viewgrams_accumulate_loglikelihood, ...AndProjData.cxx:1483-1515):

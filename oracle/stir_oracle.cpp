@@ -237,6 +237,7 @@ template <typename T> struct Geometry {
   /* TOF */
   std::vector<T> tof_low, tof_high; /* bin boundaries in mm */
   T r_sqrt2_gauss_sigma = 0;
+  T tof_trunc_n = 0; /* kernel truncated at +-k sigma: k / sqrt(2); 0: STIR's cut-off */
 
   int nax(int seg) const { return d.num_axial_poss[seg + S]; }
   int min_rd(int seg) const { return d.min_ring_diff[seg + S]; }
@@ -352,6 +353,8 @@ template <typename T> void setup_geometry(Geometry<T>& g, const b200rt_geometry&
     /* ProjMatrixByBin::enable_tof (ProjMatrixByBin.cxx:66-75) */
     const T sigma = static_cast<T>(static_cast<float>(static_cast<double>(d.timing_resolution_ps) * c_half)) / T(2.355f);
     g.r_sqrt2_gauss_sigma = T(1.0f) / (sigma * static_cast<T>(std::sqrt(2.0)));
+    if (!(d.tof_kernel_truncation_sigmas >= 0.f)) throw std::runtime_error("tof_kernel_truncation_sigmas must be >= 0");
+    g.tof_trunc_n = static_cast<T>(static_cast<double>(d.tof_kernel_truncation_sigmas) / std::sqrt(2.0));
   }
   g.projdata_size = g.tof_stride * g.num_tof;
 
@@ -749,10 +752,17 @@ const FastErf& fast_erf() {
   return f;
 }
 
-/* ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197) */
+/* ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197).  With a truncation (tof_trunc_n > 0, no STIR
+ * counterpart) the Gaussian is cut at +-k sigma: the bin's ends are clamped to [-k/sqrt2, k/sqrt2] in the kernel's
+ * units, so a bin wholly outside gets 0 and a straddling bin the kernel's integral over its inner part. */
 template <typename T> T tof_value(const Geometry<T>& g, T d1, T d2) {
-  const T d1n = d1 * g.r_sqrt2_gauss_sigma, d2n = d2 * g.r_sqrt2_gauss_sigma;
-  if ((d1n >= T(4.f) && d2n >= T(4.f)) || (d1n <= T(-4.f) && d2n <= T(-4.f))) return T(0);
+  T d1n = d1 * g.r_sqrt2_gauss_sigma, d2n = d2 * g.r_sqrt2_gauss_sigma;
+  if (g.tof_trunc_n > T(0)) {
+    d1n = std::min(std::max(d1n, -g.tof_trunc_n), g.tof_trunc_n);
+    d2n = std::min(std::max(d2n, -g.tof_trunc_n), g.tof_trunc_n);
+  } else if ((d1n >= T(4.f) && d2n >= T(4.f)) || (d1n <= T(-4.f) && d2n <= T(-4.f))) {
+    return T(0);
+  }
   return static_cast<T>(0.5 * (fast_erf()(static_cast<double>(d2n)) - fast_erf()(static_cast<double>(d1n))));
 }
 

@@ -22,6 +22,7 @@ ERR_TOO_LARGE = -7
 
 BACKPROJECT_ATOMIC = 0
 BACKPROJECT_DETERMINISTIC = 1
+STATUS_STAGING_TIMEOUT = 1  # b200rt_get_device_status: a forward staging copy's wait ran out
 
 ATTENUATION_FACTORS = 0
 ATTENUATION_APPLY = 1
@@ -80,6 +81,7 @@ class Geometry(ctypes.Structure):
         ("do_symmetry_swap_segment", ctypes.c_int32),
         ("do_symmetry_swap_s", ctypes.c_int32),
         ("do_symmetry_shift_z", ctypes.c_int32),
+        ("tof_kernel_truncation_sigmas", ctypes.c_float),
     ]
 
 
@@ -237,6 +239,7 @@ EXPORTS = [
     ("b200rt_osmaposl_apply_update_dev", _I, [_P, _P, _P, _P, _I, _I, ctypes.POINTER(Prior), ctypes.c_float, ctypes.c_float,
                                               _P]),
     ("b200rt_get_num_cancelled", _I, [_P, ctypes.POINTER(_I64)]),
+    ("b200rt_get_device_status", _I, [_P, ctypes.POINTER(ctypes.c_uint32), _I]),
     ("b200rt_log_likelihood_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(ctypes.c_double), _P]),
     ("b200rt_log_likelihood_gradient_dev", _I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P]),
     ("b200rt_prior_value_dev", _I, [_P, ctypes.POINTER(Prior), _P, ctypes.POINTER(ctypes.c_double), _P]),

@@ -115,6 +115,7 @@ struct b200rt_projector {
   DevBuf<float> ratio, upd, grad, small_value, partial_max, umax;
   DevBuf<float> ratio_batch;  // gradient ratios of an image batch (b200rt_log_likelihood_gradient_batch_dev)
   DevBuf<unsigned int> cancelled;
+  DevBuf<unsigned int> dev_status;  // kernels' status word (PathParams::status)
   DevBuf<double> ll_partials, ll_sum;
   // deterministic back projection
   DevBuf<unsigned long long> acc64;

@@ -115,6 +115,22 @@ int b200rt_osmaposl_apply_update_dev(b200rt_projector* h, float* estimate_dev, f
   }
 }
 
+int b200rt_get_device_status(b200rt_projector* h, uint32_t* status, int clear) {
+  if (!h || !status) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  try {
+    DeviceGuard dg(h->device);
+    unsigned int s = 0;
+    if (h->dev_status.p) {
+      ck(cudaMemcpy(&s, h->dev_status.p, sizeof(s), cudaMemcpyDeviceToHost), "D2H");
+      if (clear && s) ck(cudaMemset(h->dev_status.p, 0, sizeof(s)), "memset");
+    }
+    *status = s;
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_get_num_cancelled(b200rt_projector* h, int64_t* out) {
   if (!h || !out) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
   try {

@@ -242,6 +242,9 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   h.path_cmaj.upload(cmaj, h.stream);
   h.path_col_starts.upload(col_starts, h.stream);
   ck(cudaStreamSynchronize(h.stream), "path tables");
+  h.dev_status.alloc(1);
+  ck(cudaMemsetAsync(h.dev_status.p, 0, sizeof(unsigned), h.stream), "memset");
+  ck(cudaStreamSynchronize(h.stream), "status word");
   PathParams& pp = h.pparams;
   pp.elems = h.path_elems.p;
   pp.cols = h.path_cols.p;
@@ -258,6 +261,7 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   pp.max_members = nsegs;
   pp.max_acc = max_acc;
   pp.zpad = zpad;
+  pp.status = h.dev_status.p;
   h.h_item_view = item_view;
   h.h_item_out_view = item_out_view;
   h.paths_view_split = std::find(item_out_view.begin(), item_out_view.end(), -1) == item_out_view.end();
@@ -470,6 +474,7 @@ void setup_projector(b200rt_projector& h) {
     tp.origin[2] = g.desc().origin_x;
     tp.scanner_z_offset = g.scanner_z_offset();
     tp.r_sqrt2_sigma = g.r_sqrt2_gauss_sigma();
+    tp.trunc_n = g.tof_truncation_n();
     tp.low = d_low.p;
     tp.high = d_high.p;
     tp.erf_table = d_table.p;

@@ -104,6 +104,9 @@ Geometry::Geometry(const b200rt_geometry& d) : d_(d) {
     }
     const float sigma = static_cast<float>(static_cast<double>(d.timing_resolution_ps) * c_half) / 2.355f;
     r_sqrt2_sigma_ = 1.0f / (sigma * static_cast<float>(std::sqrt(2.0)));
+    if (!(d.tof_kernel_truncation_sigmas >= 0.f)) fail("tof_kernel_truncation_sigmas must be 0 (STIR's cut-off) or > 0");
+    // +-k sigma in the kernel's units (distance times 1 / (sqrt(2) sigma))
+    tof_trunc_n_ = static_cast<float>(static_cast<double>(d.tof_kernel_truncation_sigmas) / std::sqrt(2.0));
   }
   projdata_size_ = tof_stride_ * num_tof_;
 

@@ -93,6 +93,8 @@ class Geometry {
   float tof_low(int k) const { return tof_low_[k - min_tof_]; }
   float tof_high(int k) const { return tof_high_[k - min_tof_]; }
   float r_sqrt2_gauss_sigma() const { return r_sqrt2_sigma_; }
+  // TOF kernel cut-off k / sqrt(2) for truncation at +-k sigma; 0: STIR's cut-off
+  float tof_truncation_n() const { return tof_trunc_n_; }
   // LOR mid point and unit direction of a basic bin, in scanner coordinates (mm) (ProjMatrixByBin.inl:117-133)
   void lor_middle_and_direction(int seg, int view, int tang, float mid[3], float unit[3]) const;
   float scanner_z_offset() const;
@@ -120,6 +122,7 @@ class Geometry {
   int64_t tof_stride_ = 0, projdata_size_ = 0;
   std::vector<float> tof_low_, tof_high_;
   float r_sqrt2_sigma_ = 0;
+  float tof_trunc_n_ = 0;
 
   float average_ring_difference(int seg) const;
   int transform_z(int abs_seg, int ax) const;

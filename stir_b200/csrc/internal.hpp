@@ -184,8 +184,10 @@ struct PathParams {
   const int* col_starts;  // per path: first element of each column in cmaj (relative), ncols + 1 entries
   int max_members;        // basic bins per path (basic segments)
   int max_acc;            // forward accumulators of the largest item: path_parts(lines) x sum of the lines' nax
-  int zpad;               // >= 0: the staged columns are nz + zpad apart with zeros between them, enough for every
+  int zpad;               // >= 0: zeros of at least zpad planes between the staged columns, enough for every
                           // forward pass to read all its planes without range tests; -1: tests per lane
+  unsigned* status;       // device word of the projector: bit 0 set when a staging copy was not seen to complete
+                          // within the forward kernel's wait limit (that item's sums are then incomplete)
 };
 
 // parts each line's elements are split into (forward): an item's lines are processed in pairs (the two
@@ -226,8 +228,11 @@ __host__ __device__ inline int path_dl_len(int nz, int nax_max, int npa_max) {
 struct PathSmemFwd {
   int colbase, lines, pairs, rowoff, xbuf, acc, total;
 };
-// staged column ci, plane z at ci * path_col_stride + path_col_offset + z
-__host__ __device__ inline int path_col_stride(int nz, int zpad) { return zpad >= 0 ? nz + zpad : nz; }
+// staged column ci starts at ci * path_col_stride + path_col_offset (a 16-byte boundary with padded staging), plane
+// z at that start + z, plus, with padded staging, the column's 16-byte phase in global memory (0..3 floats): the
+// padded columns are copied as whole 16-byte blocks, so the stride leaves zpad zero planes between columns
+// whatever the phases
+__host__ __device__ inline int path_col_stride(int nz, int zpad) { return zpad >= 0 ? (nz + zpad + 6) & ~3 : nz; }
 __host__ __device__ inline int path_col_offset(int zpad) { return zpad > 0 ? zpad : 0; }
 __host__ __device__ inline PathSmemFwd path_smem_fwd(int K, int nz, int zpad, int max_lines, int max_acc, int npa_max) {
   PathSmemFwd s;
@@ -465,6 +470,7 @@ struct TofParams {
   float vox[3], origin[3];  // z,y,x
   float scanner_z_offset;
   float r_sqrt2_sigma;
+  float trunc_n;            // 0: STIR's kernel cut-off; > 0: kernel truncated at +-trunc_n (in units of sqrt(2) sigma)
   const float* low;         // per timing bin
   const float* high;
   const double* erf_table;  // FastErf samples

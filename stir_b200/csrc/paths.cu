@@ -102,6 +102,52 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
 }
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// ---- bulk staging: one cp.async.bulk (the TMA unit's 1-D copy) per image column, completed on an mbarrier ----
+// Source and destination are this GPU's memory only (the image and the CTA's shared memory); no multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n .reg .b64 state;\n mbarrier.arrive.shared::cta.b64 state, [%0];\n}\n" ::"r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for the phase with the given parity to complete, at most kStageWaitLimit polls (each poll may itself
+// suspend the thread for a while); false when the limit ran out.
+constexpr int kStageWaitLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (int i = 0; i < kStageWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_copy_to_smem(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// orders this thread's earlier generic-proxy accesses to shared memory before later async-proxy (bulk copy) ones
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
 // one packed element of the padded path: staged indices (16-bit, signed) of axial position 0 for both lines
 template <int NJ, bool TWO>
 __device__ __forceinline__ void padded_fma(const float* cols, uint32_t idx, float v, int zo0, int npa, float* acc1,
@@ -118,9 +164,11 @@ __device__ __forceinline__ void padded_fma(const float* cols, uint32_t idx, floa
 // One pass of one unit over elements [e0, e1) of its row: NJ groups of 32 axial positions from a0.
 // The warp's lanes transform 32 elements at a time (column slot -> staged index, z reflection) into
 // the warp's buffer; then every element costs one broadcast read and NJ shared loads and FMAs.
+// colstart: with padded staging, the staged index of plane 0 of each column of the chunk.
 template <int NPA, int NJ, bool TWO, bool PADDED>
 __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int e0, int e1, int c0, const float* cols,
-                                            int nz, int cstride, int coff, const PathLineSmem& L1,
+                                            const int* colstart, int nz, int cstride, int coff,
+                                            const PathLineSmem& L1,
                                             const PathLineSmem& L2, int a0, int nact, int lane, float* acc_row1,
                                             float* acc_row2, PathXElem* xb) {
   const int npa = NPA ? NPA : L1.npa;
@@ -151,7 +199,8 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
       const int zt1 = L1.zsign * zr + L1.zadd;
       const int zt2 = TWO ? L2.zsign * zr + L2.zadd : 0;
       if (PADDED) {
-        const int b1 = sl * cstride + coff + zt1, b2 = TWO ? sl * cstride + coff + zt2 : 0;
+        const int s0 = colstart[sl];
+        const int b1 = s0 + zt1, b2 = TWO ? s0 + zt2 : 0;
         xp[lane] = make_uint2((static_cast<uint32_t>(b1) & 0xffffu) | (static_cast<uint32_t>(b2) << 16),
                               __float_as_uint(m.v));
       } else {
@@ -166,7 +215,7 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
       }
     }
     __syncwarp();
-    if (PADDED) {
+    if constexpr (PADDED) {
       const uint4* xq = reinterpret_cast<const uint4*>(xb);
       int i = 0;
       for (; i + 1 < cnt; i += 2) {
@@ -178,27 +227,27 @@ __device__ __forceinline__ void gather_pass(const PathElem* __restrict__ E, int 
         const uint2 w = xp[i];
         padded_fma<NJ, TWO>(cols, w.x, __uint_as_float(w.y), zo0, npa, acc1, acc2);
       }
-      continue;
-    }
-    for (int i = 0; i < cnt; ++i) {
-      const PathXElem e = xb[i];
-      const float* q1 = cols + (e.base + zo0);
-      const float* q2 = cols + (e.zt + zo0);
-      if (PADDED || (e.full >> 30)) {
+    } else {
+      for (int i = 0; i < cnt; ++i) {
+        const PathXElem e = xb[i];
+        const float* q1 = cols + (e.base + zo0);
+        const float* q2 = cols + (e.zt + zo0);
+        if (e.full >> 30) {
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-          acc1[j] += q1[j * 32 * npa] * e.v;
-          if (TWO) acc2[j] += q2[j * 32 * npa] * e.v;
-        }
-      } else {
-        const int sb = (e.full & 0xffff) * cstride + coff;  // column start in the staging buffer
+          for (int j = 0; j < NJ; ++j) {
+            acc1[j] += q1[j * 32 * npa] * e.v;
+            if (TWO) acc2[j] += q2[j * 32 * npa] * e.v;
+          }
+        } else {
+          const int sb = (e.full & 0xffff) * cstride + coff;  // column start in the staging buffer
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-          const int zz1 = e.base - sb + zo0 + j * 32 * npa;
-          if (act[j] && static_cast<unsigned>(zz1) < static_cast<unsigned>(nz)) acc1[j] += q1[j * 32 * npa] * e.v;
-          if (TWO) {
-            const int zz2 = e.zt - sb + zo0 + j * 32 * npa;
-            if (act[j] && static_cast<unsigned>(zz2) < static_cast<unsigned>(nz)) acc2[j] += q2[j * 32 * npa] * e.v;
+          for (int j = 0; j < NJ; ++j) {
+            const int zz1 = e.base - sb + zo0 + j * 32 * npa;
+            if (act[j] && static_cast<unsigned>(zz1) < static_cast<unsigned>(nz)) acc1[j] += q1[j * 32 * npa] * e.v;
+            if (TWO) {
+              const int zz2 = e.zt - sb + zo0 + j * 32 * npa;
+              if (act[j] && static_cast<unsigned>(zz2) < static_cast<unsigned>(nz)) acc2[j] += q2[j * 32 * npa] * e.v;
+            }
           }
         }
       }
@@ -231,14 +280,18 @@ __device__ __forceinline__ int pair_lines(const PathLineSmem* ls, int nl, int2* 
 
 // one gather pass, with the padded staging or with per-lane range tests
 #define GATHER(NJ, TWO, LA, LB, ...)                                                                             \
-  (pp.zpad >= 0 ? gather_pass<NPA, NJ, TWO, true>(E, e0, e1, c0, cols, nz, cstride, coff, LA, LB, __VA_ARGS__)   \
-                : gather_pass<NPA, NJ, TWO, false>(E, e0, e1, c0, cols, nz, cstride, coff, LA, LB, __VA_ARGS__))
+  (pp.zpad >= 0                                                                                                  \
+       ? gather_pass<NPA, NJ, TWO, true>(E, e0, e1, c0, cols, colbase, nz, cstride, coff, LA, LB, __VA_ARGS__)    \
+       : gather_pass<NPA, NJ, TWO, false>(E, e0, e1, c0, cols, colbase, nz, cstride, coff, LA, LB, __VA_ARGS__))
 
+// One path item.  With padded staging the columns are copied by bulk copies completed on `bar` (phase parity
+// `phase`, flipped once per chunk); false when a copy was not seen to complete within the wait limit: the item is
+// then abandoned (no output written) and the projector's status word records it.
 template <int NPA, int EPI>
-__device__ __forceinline__ void forward_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+__device__ __forceinline__ bool forward_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
                                                   unsigned char* smem, const float* __restrict__ img,
                                                   float* __restrict__ out, const FwdEpilogue& ep, double& ll,
-                                                  unsigned& ncancel) {
+                                                  unsigned& ncancel, uint64_t* bar, unsigned& phase) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nz = p.nz;
   const PathSmemFwd lay = path_smem_fwd(pp.K, nz, pp.zpad, pp.max_lines, pp.max_acc, pp.npa_max);
@@ -271,22 +324,72 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
   // the staging buffer starts as zeros: with padded staging the planes between the columns stay zero
   if (pp.zpad > 0)
     for (int i = threadIdx.x; i < lay.colbase / 4; i += blockDim.x) cols[i] = 0.f;
+  const bool bulk = pp.zpad >= 0;
   const int nch = (it.ncols + pp.K - 1) / pp.K;
   for (int c = 0; c < nch; ++c) {
     const int c0 = c * pp.K, kc = min(pp.K, it.ncols - c0);
+    // the previous chunk's reads and the zeroing come before this chunk's bulk copies into the same slots
+    if (bulk) fence_proxy_async_smem();
     __syncthreads();  // previous chunk done (and the zeroing visible)
     chunk_columns(p, pp, it, c0, kc, colbase);
     __syncthreads();
-    for (int ci = warp; ci < kc; ci += kPathWarps) {
-      const int b = colbase[ci];
-      float* dst = cols + ci * cstride + coff;
-      if (b >= 0) {
-        for (int z = lane; z < nz; z += 32) cp_async4(dst + z, img + b + z);
-      } else {
-        for (int z = lane; z < nz; z += 32) dst[z] = 0.f;
+    if (bulk) {
+      // one bulk copy per column: the whole 16-byte blocks that hold its nz planes, to its slot's 16-byte
+      // boundary, so plane 0 lands at the column's phase (its address mod 16, in floats), which colbase[ci]
+      // records as the column's staged start; columns outside the image are zeroed instead
+      for (int ci = threadIdx.x; ci < kc; ci += blockDim.x) {
+        const int b = colbase[ci];
+        const int d = ci * cstride + coff;
+        float* slot = cols + d;
+        int start = d;
+        if (b >= 0) {
+          const float* src = img + b;
+          const int ph = static_cast<int>((reinterpret_cast<uintptr_t>(src) >> 2) & 3u);
+          const unsigned bytes = static_cast<unsigned>((ph + nz + 3) & ~3) * 4u;
+          mbar_expect_tx(bar, bytes);
+          bulk_copy_to_smem(slot, src - ph, bytes, bar);
+          start += ph;
+        } else {
+          for (int z = 0; z < ((nz + 6) & ~3); ++z) slot[z] = 0.f;
+        }
+        colbase[ci] = start;
       }
+      __syncthreads();  // every byte count is on the barrier before its arrival
+      if (threadIdx.x == 0) mbar_arrive(bar);
+      const bool done = mbar_wait_bounded(bar, phase);
+      if (!__syncthreads_and(done)) {
+        // not seen to complete: record it, give the copies in flight one more bounded wait, abandon the item
+        if (threadIdx.x == 0 && pp.status) atomicOr(pp.status, 1u);
+        mbar_wait_bounded(bar, phase);
+        return false;
+      }
+      phase ^= 1u;
+      // a slot's copies reach at most ext = round_up4(nz + 3) floats from its start: everything of [0, ext) that is
+      // not this chunk's column (the neighbouring planes copied with the blocks, and what an earlier chunk's
+      // column with another phase left there) back to zeros -- at most 3 planes below plane 0, 6 above nz - 1
+      const int ext = (nz + 6) & ~3;
+      for (int i = threadIdx.x; i < kc * 16; i += blockDim.x) {
+        const int ci = i >> 4, k = i & 15;
+        const int d = ci * cstride + coff, ph = colbase[ci] - d;
+        if (k < 4) {
+          if (k < ph) cols[d + k] = 0.f;
+        } else {
+          const int z = ph + nz + (k - 4);
+          if (z < ext) cols[d + z] = 0.f;
+        }
+      }
+    } else {
+      for (int ci = warp; ci < kc; ci += kPathWarps) {
+        const int b = colbase[ci];
+        float* dst = cols + ci * cstride + coff;
+        if (b >= 0) {
+          for (int z = lane; z < nz; z += 32) cp_async4(dst + z, img + b + z);
+        } else {
+          for (int z = lane; z < nz; z += 32) dst[z] = 0.f;
+        }
+      }
+      cp_async_wait();
     }
-    cp_async_wait();
     __syncthreads();
     for (int u = warp; u < U; u += kPathWarps) {
       const int pr = u >> lgP, part = u & (P - 1);
@@ -333,6 +436,7 @@ __device__ __forceinline__ void forward_path_item(const ProjParams& p, const Pat
       forward_store<EPI>(p, L.seg, L.view, L.tofi, L.nax, L.out_base + a, a, v, out, ep, ll, ncancel);
     }
   }
+  return true;
 }
 
 // Back projection as a gather over the voxels of each column: image[col][z] += the sum, over the path's
@@ -629,9 +733,18 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
     if (ep.mult) ep.mult += b * ep.mult_stride;
     if (ep.small_value) ep.small_value += b * ep.sv_stride;
   }
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar);
+  __syncthreads();
   double ll = 0.0;
   unsigned ncancel = 0;
-  forward_path_item<NPA, EPI>(p, pp, it, smem, img, out, ep, ll, ncancel);
+  unsigned phase = 0;
+  if (!forward_path_item<NPA, EPI>(p, pp, it, smem, img, out, ep, ll, ncancel, &bar, phase)) {
+    // abandoned (the status word says so): the item's log-likelihood partial is NaN rather than stale
+    if (EPI == kEpiLoglik && threadIdx.x == 0)
+      ep.partials[static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x] = __longlong_as_double(-1ll);
+    return;
+  }
   if (EPI == kEpiRatio || EPI == kEpiGradient) {
     // cancelled singularities (distributable.cxx:590-594)
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
@@ -716,10 +829,16 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
                                unsigned* counter) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ BatchPathStage st;
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar);
+  unsigned phase = 0;  // next_path_item synchronises the CTA before the barrier's first use
   while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st)) {
     double ll = 0.0;
     unsigned ncancel = 0;
-    forward_path_item<NPA, kEpiRatio>(st.p, st.pp, st.it, smem, st.f.x, st.f.ratio, st.f.ep, ll, ncancel);
+    // an abandoned item (status word set) ends this CTA: its copies may still be in flight
+    if (!forward_path_item<NPA, kEpiRatio>(st.p, st.pp, st.it, smem, st.f.x, st.f.ratio, st.f.ep, ll, ncancel, &bar,
+                                           phase))
+      return;
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if ((threadIdx.x & 31) == 0 && ncancel && st.f.ep.cancelled) atomicAdd(st.f.ep.cancelled, ncancel);
   }

@@ -296,10 +296,16 @@ __device__ __forceinline__ double fast_erf(const TofParams& tp, double xp) {
   return tp.erf_table[lower] + (xi - lower) * (tp.erf_table[lower + 1] - tp.erf_table[lower]);
 }
 
-// ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197)
+// ProjMatrixByBin::get_tof_value (ProjMatrixByBin.inl:187-197); with trunc_n > 0 the kernel truncated at
+// +-trunc_n: the bin's ends clamped to that range (a bin wholly outside it gets 0)
 __device__ __forceinline__ float tof_value(const TofParams& tp, float d1, float d2) {
-  const float d1n = d1 * tp.r_sqrt2_sigma, d2n = d2 * tp.r_sqrt2_sigma;
-  if ((d1n >= 4.f && d2n >= 4.f) || (d1n <= -4.f && d2n <= -4.f)) return 0.f;
+  float d1n = d1 * tp.r_sqrt2_sigma, d2n = d2 * tp.r_sqrt2_sigma;
+  if (tp.trunc_n > 0.f) {
+    d1n = fminf(fmaxf(d1n, -tp.trunc_n), tp.trunc_n);
+    d2n = fminf(fmaxf(d2n, -tp.trunc_n), tp.trunc_n);
+  } else if ((d1n >= 4.f && d2n >= 4.f) || (d1n <= -4.f && d2n <= -4.f)) {
+    return 0.f;
+  }
   return static_cast<float>(0.5 * (fast_erf(tp, static_cast<double>(d2n)) - fast_erf(tp, static_cast<double>(d1n))));
 }
 

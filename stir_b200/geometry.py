@@ -189,7 +189,10 @@ def image_from_projdata(pdi: ProjDataInfo, zoom: float = 1.0, xy_size: int = -1,
 
 
 def make_geometry(pdi: ProjDataInfo, img: ImageGeometry, num_tangential_LORs: int = 1,
-                  restrict_to_cylindrical_FOV: bool = True, symmetries: Sequence[bool] = (True,) * 5) -> _abi.Geometry:
+                  restrict_to_cylindrical_FOV: bool = True, symmetries: Sequence[bool] = (True,) * 5,
+                  tof_kernel_truncation_sigmas: float = 0.0) -> _abi.Geometry:
+    """The C ABI's geometry.  tof_kernel_truncation_sigmas: 0 keeps STIR's TOF kernel cut-off; k > 0 truncates the
+    Gaussian at +-k sigma (no STIR counterpart)."""
     g = _abi.Geometry()
     sc = pdi.scanner
     g.num_rings = sc.num_rings
@@ -222,6 +225,7 @@ def make_geometry(pdi: ProjDataInfo, img: ImageGeometry, num_tangential_LORs: in
     g.restrict_to_cylindrical_FOV = 1 if restrict_to_cylindrical_FOV else 0
     (g.do_symmetry_90degrees_min_phi, g.do_symmetry_180degrees_min_phi, g.do_symmetry_swap_segment,
      g.do_symmetry_swap_s, g.do_symmetry_shift_z) = [1 if s else 0 for s in symmetries]
+    g.tof_kernel_truncation_sigmas = float(tof_kernel_truncation_sigmas)
     return g
 
 

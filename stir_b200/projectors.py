@@ -40,12 +40,13 @@ class RayTracingProjector:
 
     def __init__(self, proj_data_info: ProjDataInfo, image: ImageGeometry, num_tangential_LORs: int = 1,
                  restrict_to_cylindrical_FOV: bool = True, symmetries=(True,) * 5, device: int = 0,
-                 geometry: Optional[_abi.Geometry] = None):
+                 geometry: Optional[_abi.Geometry] = None, tof_kernel_truncation_sigmas: float = 0.0):
         self.lib = _abi.load_library()
         self.proj_data_info = proj_data_info
         self.image = image
         self.geometry = geometry if geometry is not None else make_geometry(
-            proj_data_info, image, num_tangential_LORs, restrict_to_cylindrical_FOV, symmetries)
+            proj_data_info, image, num_tangential_LORs, restrict_to_cylindrical_FOV, symmetries,
+            tof_kernel_truncation_sigmas)
         self.device = device
         h = ctypes.c_void_p()
         st = self.lib.b200rt_create(ctypes.byref(self.geometry), device, ctypes.byref(h))
@@ -111,6 +112,14 @@ class RayTracingProjector:
     @property
     def device_image_shape(self):
         return (self.geometry.ny, self.geometry.nx, self.geometry.nz)
+
+    def device_status(self, clear: bool = False) -> int:
+        """The projector's device status word (0: every kernel completed its work; bit STATUS_STAGING_TIMEOUT: a
+        forward projection abandoned path items whose staging copies were not seen to complete).  Synchronises."""
+        s = ctypes.c_uint32(0)
+        _abi.check(self.lib.b200rt_get_device_status(self.h, ctypes.byref(s), int(clear)), self.h,
+                   "b200rt_get_device_status")
+        return int(s.value)
 
     def get_row(self, segment, view, axial, tangential, timing=0):
         n = ctypes.c_int64(0)

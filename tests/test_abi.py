@@ -33,8 +33,8 @@ def test_python_binding_covers_header():
 
 
 def test_struct_layout_matches_header():
-    # b200rt_geometry: 10 scalars, 6 ints, 3 arrays of 255, 6 ints, 6 floats, 7 ints
-    assert ctypes.sizeof(_abi.Geometry) == 4 * (10 + 6 + 3 * 255 + 6 + 6 + 7)
+    # b200rt_geometry: 10 scalars, 6 ints, 3 arrays of 255, 6 ints, 6 floats, 7 ints, the TOF cut-off
+    assert ctypes.sizeof(_abi.Geometry) == 4 * (10 + 6 + 3 * 255 + 6 + 6 + 7 + 1)
     assert ctypes.sizeof(_abi.Info) == 5 * 8 + 4 * 4
     assert ctypes.sizeof(_abi.Prior) == 6 * 4 + 8
 

@@ -65,3 +65,21 @@ def test_clinical_adjoint_linearity_determinism(clinical):
     # the host entry points (copies overlapped with the projection, group by group of views)
     xs = proj.image_from_device_layout(xd.view(proj.device_image_shape)).cpu().numpy()
     assert np.array_equal(proj.forward_host(xs), proj.projdata_from_device_layout(ax).cpu().numpy())
+
+
+def test_clinical_forward_independent_of_image_alignment(clinical):
+    """The forward kernel copies each image column to shared memory as whole 16-byte blocks, so where a column
+    starts within its block (127 planes: every phase occurs) must not change a single bin: an image that starts
+    1, 2 or 3 floats past a 16-byte boundary projects bit for bit as the aligned one, and every launch completes."""
+    import torch
+    pdi, img, proj, orc, x = clinical
+    n = proj.geometry.nz * proj.geometry.ny * proj.geometry.nx
+    xd = proj.image_to_device_layout(torch.from_numpy(x).cuda()).reshape(-1)
+    proj.device_status(clear=True)
+    ref = proj.forward_dev(xd, proj.empty_projdata())
+    buf = torch.zeros(n + 4, device="cuda")
+    for k in range(1, 4):
+        buf.zero_()
+        buf[k:k + n].copy_(xd)
+        assert torch.equal(proj.forward_dev(buf[k:k + n], proj.empty_projdata()), ref), k
+    assert proj.device_status() == 0

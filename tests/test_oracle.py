@@ -128,3 +128,34 @@ def test_prior_gradient_vs_numerical(oracle_lib, ptype):
         xm[idx] -= h
         num = (oracle_lib.prior_value(p, xp.astype(np.float32), vox) - oracle_lib.prior_value(p, xm.astype(np.float32), vox)) / (2 * h)
         assert abs(num - g[idx]) <= 2e-3 * max(1.0, abs(g).max())
+
+
+@pytest.mark.parametrize("k", [0.0, 3.0])
+def test_oracle_tof_kernel_cut_off(oracle_lib, k):
+    """The TOF rows of a LOR through the centre summed over the 33 timing bins (50 ps each: they cover +-3.53 sigma
+    of the 550 ps kernel): with STIR's cut-off (5.66 sigma, beyond the bins) the voxel at the LOR's middle keeps
+    erf(3.53 / sqrt 2) of its non-TOF value; with the kernel truncated at +-3 sigma it keeps erf(3 / sqrt 2) = 0.9973,
+    no voxel keeps more, and the rows are shorter."""
+    import math
+    pdi, img = G.tof_small_3d_pet()
+    orc = oracle_lib.Oracle(G.make_geometry(pdi, img, tof_kernel_truncation_sigmas=k))
+    nt = oracle_lib.Oracle(G.make_geometry(G.non_tof(pdi), img))
+    c0, v0 = nt.row(0, 0, 4, 0)
+    key = lambda c: [tuple(r) for r in c]
+    total = dict.fromkeys(key(c0), 0.0)
+    nnz = 0
+    for t in range(-16, 17):
+        c, v = orc.row(0, 0, 4, 0, t)
+        nnz += len(v)
+        for kk, vv in zip(key(c), v):
+            total[kk] += vv
+    ratio = np.array([total[kk] / vv for kk, vv in zip(key(c0), v0)])
+    c_half = 0.299792458 * 0.5  # mm per ps of timing difference
+    sigma = 550.0 * c_half / 2.355
+    reach = 16.5 * 50.0 * c_half / sigma  # the bins' half range, in sigmas
+    expect = math.erf((reach if k == 0 else min(k, reach)) / math.sqrt(2.0))
+    assert abs(ratio.max() - expect) < 2e-4
+    assert ratio.max() <= expect + 2e-4
+    if k:
+        full = oracle_lib.Oracle(G.make_geometry(pdi, img))
+        assert nnz < sum(len(full.row(0, 0, 4, 0, t)[1]) for t in range(-16, 17))

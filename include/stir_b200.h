@@ -418,7 +418,21 @@ typedef struct {
   int ctas_per_sm_forward; /* persistent CTAs per SM; 0 = as many as fit */
   int ctas_per_sm_back;
   int order;               /* work order inside a frame: 0 = basic-bin order, 1 = longest rows first */
+  int kernels;             /* kernel family, B200RT_BATCH_KERNELS_* */
 } b200rt_batch_config;
+/* Kernel families of the batched projectors (how the work of a frame is cut into work items):
+ * AUTO: the first the frames allow of PATHS, TOF_GROUPED, PACKED, BASIC_BINS;
+ * PATHS: one CTA per (frame, path item), the image columns of the path staged in shared memory, lanes on axial
+ *   positions (every frame's projector has path tables; the only family for deterministic frames);
+ * TOF_GROUPED: one warp per (frame, basic bin) with all its timing bins in registers, lanes on (line, axial
+ *   position) (TOF frames with one timing-bin count);
+ * PACKED: one warp per (frame, basic bin or TOF bin), lanes on (line, axial position) (at most 16 axial positions);
+ * BASIC_BINS: one CTA per (frame, basic bin or TOF bin), one warp per related line, lanes on axial positions. */
+#define B200RT_BATCH_KERNELS_AUTO 0
+#define B200RT_BATCH_KERNELS_PATHS 1
+#define B200RT_BATCH_KERNELS_TOF_GROUPED 2
+#define B200RT_BATCH_KERNELS_PACKED 3
+#define B200RT_BATCH_KERNELS_BASIC_BINS 4
 
 int b200rt_batch_create(int device, b200rt_batch** out);
 void b200rt_batch_destroy(b200rt_batch* b);
@@ -439,9 +453,9 @@ int b200rt_batch_num_frames(const b200rt_batch* b);
  * captured once into a CUDA graph (kept per (first, count) until a frame is added or the
  * configuration changes) and launched as one graph. */
 int b200rt_batch_run(b200rt_batch* b, int first_subiteration, int count, int use_graph, void* stream);
-/* Times the batched projectors of sub-iteration `subiteration` for each configuration (CTAs per SM,
- * work order), keeps the fastest and writes it to *out (may be NULL).  Estimates are not changed;
- * synchronises. */
+/* Times the batched projectors of sub-iteration `subiteration` for each configuration the frames allow (kernel
+ * family, CTAs per SM, work order), keeps the fastest and writes it to *out (may be NULL).  Estimates are not
+ * changed; synchronises. */
 int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config* out);
 int b200rt_batch_set_config(b200rt_batch* b, const b200rt_batch_config* config);
 int b200rt_batch_get_config(const b200rt_batch* b, b200rt_batch_config* out);

@@ -22,6 +22,11 @@ ERR_TOO_LARGE = -7
 
 BACKPROJECT_ATOMIC = 0
 BACKPROJECT_DETERMINISTIC = 1
+BATCH_KERNELS_AUTO = 0
+BATCH_KERNELS_PATHS = 1
+BATCH_KERNELS_TOF_GROUPED = 2
+BATCH_KERNELS_PACKED = 3
+BATCH_KERNELS_BASIC_BINS = 4
 STATUS_STAGING_TIMEOUT = 1  # b200rt_get_device_status: a forward staging copy's wait ran out
 
 ATTENUATION_FACTORS = 0
@@ -122,6 +127,7 @@ class BatchConfig(ctypes.Structure):
         ("ctas_per_sm_forward", ctypes.c_int32),
         ("ctas_per_sm_back", ctypes.c_int32),
         ("order", ctypes.c_int32),
+        ("kernels", ctypes.c_int32),
     ]
 
 

@@ -68,17 +68,19 @@ class BatchedOSMAPOSL:
         self._check(self.lib.b200rt_batch_autotune(self.b, int(subiteration), ctypes.byref(cfg)),
                     "b200rt_batch_autotune")
         return dict(ctas_per_sm_forward=cfg.ctas_per_sm_forward, ctas_per_sm_back=cfg.ctas_per_sm_back,
-                    order=cfg.order)
+                    order=cfg.order, kernels=cfg.kernels)
 
-    def set_config(self, ctas_per_sm_forward: int = 0, ctas_per_sm_back: int = 0, order: int = 0):
-        cfg = _abi.BatchConfig(ctas_per_sm_forward, ctas_per_sm_back, order)
+    def set_config(self, ctas_per_sm_forward: int = 0, ctas_per_sm_back: int = 0, order: int = 0,
+                   kernels: int = _abi.BATCH_KERNELS_AUTO):
+        """kernels: the kernel family (_abi.BATCH_KERNELS_*); AUTO takes the first the frames allow."""
+        cfg = _abi.BatchConfig(ctas_per_sm_forward, ctas_per_sm_back, order, kernels)
         self._check(self.lib.b200rt_batch_set_config(self.b, ctypes.byref(cfg)), "b200rt_batch_set_config")
 
     def get_config(self) -> dict:
         cfg = _abi.BatchConfig()
         self._check(self.lib.b200rt_batch_get_config(self.b, ctypes.byref(cfg)), "b200rt_batch_get_config")
         return dict(ctas_per_sm_forward=cfg.ctas_per_sm_forward, ctas_per_sm_back=cfg.ctas_per_sm_back,
-                    order=cfg.order)
+                    order=cfg.order, kernels=cfg.kernels)
 
     def run(self, first: int = 1, count: int | None = None, use_graph: bool = True, stream=None):
         """Batched sub-iterations first..first+count-1 (default: to the last frame's end)."""

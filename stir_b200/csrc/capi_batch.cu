@@ -41,10 +41,12 @@ struct b200rt_batch {
   std::vector<b200rt_projector*> geoms;
   DevBuf<b200::ProjParams> d_geoms;
   DevBuf<b200::PathParams> d_pgeoms;
-  bool paths = false;  // every frame's projector has path items: the column-staged batched kernels
-  bool tof_grouped = false;  // otherwise, TOF frames with the timing bins of a basic bin grouped: TOF kernels
+  // kernel families (index B200RT_BATCH_KERNELS_*) the frames allow, the one in use, and each one's most
+  // persistent CTAs per SM (forward, back)
+  bool avail[5] = {false, false, false, false, false};
+  int family = B200RT_BATCH_KERNELS_PATHS;
+  int max_f[5] = {0, 0, 0, 0, 0}, max_b[5] = {0, 0, 0, 0, 0};
   int num_tof = 1;
-  bool packed = false;  // otherwise, every segment of every frame has few axial positions: the packed kernels
   int smem_f = 0, smem_b = 0;
   DevBuf<b200::BatchFrameDev> d_frames;
   DevBuf<unsigned int> counters;  // work-queue heads of the forward and back launches
@@ -52,7 +54,7 @@ struct b200rt_batch {
   int npa = 0;
   size_t smem = 0;
   int num_sms = 0, max_fwd = 0, max_back = 0;
-  b200rt_batch_config cfg{0, 0, 0};
+  b200rt_batch_config cfg{0, 0, 0, B200RT_BATCH_KERNELS_AUTO};
   // item lists by (order, subset of each frame or -1)
   std::map<std::vector<int>, std::unique_ptr<DevBuf<b200::BatchItem>>> items;
   std::map<std::vector<int>, int> item_counts;
@@ -78,6 +80,24 @@ void drop_graphs(b200rt_batch& b) {
 
 int frame_subset(const b200rt_batch::Frame& f, int k) { return (f.start_subset + k - 1) % f.nsub; }
 
+// makes `kernels` (B200RT_BATCH_KERNELS_*; AUTO: the first the frames allow) the family in use
+void use_family(b200rt_batch& b, int kernels) {
+  int f = kernels;
+  if (f == B200RT_BATCH_KERNELS_AUTO)
+    for (int c : {B200RT_BATCH_KERNELS_PATHS, B200RT_BATCH_KERNELS_TOF_GROUPED, B200RT_BATCH_KERNELS_PACKED,
+                  B200RT_BATCH_KERNELS_BASIC_BINS})
+      if (b.avail[c]) {
+        f = c;
+        break;
+      }
+  if (f < B200RT_BATCH_KERNELS_PATHS || f > B200RT_BATCH_KERNELS_BASIC_BINS || !b.avail[f])
+    throw std::invalid_argument("the batch's frames do not allow that kernel family");
+  if (b.max_f[f] < 1 || b.max_b[f] < 1) throw std::runtime_error("batched projector does not fit on an SM");
+  b.family = f;
+  b.max_fwd = b.max_f[f];
+  b.max_back = b.max_b[f];
+}
+
 // device tables and per-frame scratch; done once after the last add_frame
 void batch_finalize(b200rt_batch& b) {
   if (b.ready) return;
@@ -92,15 +112,22 @@ void batch_finalize(b200rt_batch& b) {
   b.smem = b200::proj_smem_bytes(max_row);
   cudaStream_t st = b.capture_stream;
   b.d_geoms.upload(gp, st);
-  b.paths = true;
-  for (auto* h : b.geoms) b.paths = b.paths && h->use_paths;
-  b.tof_grouped = !b.paths;
+  bool paths = true, tof_grouped = true, packed = true, deterministic = false;
   b.num_tof = b.geoms.empty() ? 1 : b.geoms[0]->params.num_tof;
-  for (auto* h : b.geoms)  // one timing-bin count for the whole batch (the kernels' group size)
-    b.tof_grouped = b.tof_grouped && h->params.tof_w != nullptr && h->params.num_tof == b.num_tof;
-  b.packed = !b.paths && !b.tof_grouped;
-  for (auto* h : b.geoms) b.packed = b.packed && h->params.max_nax <= b200::kPackedMaxNax;
-  if (b.paths) {
+  for (auto* h : b.geoms) {
+    paths = paths && h->use_paths;
+    // one timing-bin count for the whole batch (the kernels' group size)
+    tof_grouped = tof_grouped && h->params.tof_w != nullptr && h->params.num_tof == b.num_tof;
+    packed = packed && h->params.max_nax <= b200::kPackedMaxNax;
+  }
+  for (auto& fp : b.frames) deterministic = deterministic || fp->mode == B200RT_BACKPROJECT_DETERMINISTIC;
+  if (deterministic && !paths) throw std::invalid_argument("deterministic batched frames need the column-staged kernels");
+  // the fixed-point numerators exist in the column-staged kernels only
+  b.avail[B200RT_BATCH_KERNELS_PATHS] = paths;
+  b.avail[B200RT_BATCH_KERNELS_TOF_GROUPED] = tof_grouped && !deterministic;
+  b.avail[B200RT_BATCH_KERNELS_PACKED] = packed && !deterministic;
+  b.avail[B200RT_BATCH_KERNELS_BASIC_BINS] = !deterministic;
+  if (paths) {
     std::vector<b200::PathParams> pg;
     b.smem_f = b.smem_b = 0;
     for (auto* h : b.geoms) {
@@ -133,7 +160,6 @@ void batch_finalize(b200rt_batch& b) {
       subset_views(*f.h, 0, 1, nv);  // all views, for the thresholds
     }
     if (f.mode == B200RT_BACKPROJECT_DETERMINISTIC) {
-      if (!b.paths) throw std::invalid_argument("deterministic batched frames need the column-staged kernels");
       f.acc64.alloc(g.image_size());
       f.fixed_scale.alloc(1);
       f.det_partial.alloc(1);
@@ -160,27 +186,30 @@ void batch_finalize(b200rt_batch& b) {
   b.d_frames.upload(fd, st);
   b.counters.alloc(2);
   ck(cudaDeviceGetAttribute(&b.num_sms, cudaDevAttrMultiProcessorCount, b.device), "device attribute");
-  if (b.paths) {
-    b.max_fwd = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
-    b.max_back = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
-  } else if (b.tof_grouped) {
-    b.max_fwd = b200::batch_tof_max_ctas_per_sm(b.num_tof, true);
-    b.max_back = b200::batch_tof_max_ctas_per_sm(b.num_tof, false);
-  } else if (b.packed) {
-    b.max_fwd = b200::batch_packed_max_ctas_per_sm(true);
-    b.max_back = b200::batch_packed_max_ctas_per_sm(false);
-  } else {
-    b.max_fwd = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
-    b.max_back = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
+  if (b.avail[B200RT_BATCH_KERNELS_PATHS]) {
+    b.max_f[B200RT_BATCH_KERNELS_PATHS] = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_f, true);
+    b.max_b[B200RT_BATCH_KERNELS_PATHS] = b200::batch_paths_max_ctas_per_sm(b.npa, b.smem_b, false);
   }
-  if (b.max_fwd < 1 || b.max_back < 1) throw std::runtime_error("batched projector does not fit on an SM");
+  if (b.avail[B200RT_BATCH_KERNELS_TOF_GROUPED]) {
+    b.max_f[B200RT_BATCH_KERNELS_TOF_GROUPED] = b200::batch_tof_max_ctas_per_sm(b.num_tof, true);
+    b.max_b[B200RT_BATCH_KERNELS_TOF_GROUPED] = b200::batch_tof_max_ctas_per_sm(b.num_tof, false);
+  }
+  if (b.avail[B200RT_BATCH_KERNELS_PACKED]) {
+    b.max_f[B200RT_BATCH_KERNELS_PACKED] = b200::batch_packed_max_ctas_per_sm(true);
+    b.max_b[B200RT_BATCH_KERNELS_PACKED] = b200::batch_packed_max_ctas_per_sm(false);
+  }
+  if (b.avail[B200RT_BATCH_KERNELS_BASIC_BINS]) {
+    b.max_f[B200RT_BATCH_KERNELS_BASIC_BINS] = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
+    b.max_b[B200RT_BATCH_KERNELS_BASIC_BINS] = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
+  }
+  use_family(b, b.cfg.kernels);
   ck(cudaStreamSynchronize(st), "batch set-up");
   b.ready = true;
 }
 
 // the (frame, basic bin) work of batched sub-iteration k, uploaded on first use
 const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
-  std::vector<int> key{order};
+  std::vector<int> key{order, b.family};
   for (auto& f : b.frames) key.push_back(k <= f->num_subiters ? frame_subset(*f, k) : -1);
   auto it = b.items.find(key);
   if (it != b.items.end()) {
@@ -189,13 +218,13 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
   }
   std::vector<BatchItem> list;
   for (size_t fi = 0; fi < b.frames.size(); ++fi) {
-    if (key[fi + 1] < 0) continue;
+    if (key[fi + 2] < 0) continue;
     const auto& f = *b.frames[fi];
     const b200rt_projector& h = *f.h;
     std::vector<int> bins;  // basic bins, or path items with the column-staged kernels
-    if (b.paths) {
+    if (b.family == B200RT_BATCH_KERNELS_PATHS) {
       for (int i = 0; i < static_cast<int>(h.h_item_view.size()); ++i)
-        if (h.h_item_view[i] % f.nsub == key[fi + 1]) bins.push_back(i);
+        if (h.h_item_view[i] % f.nsub == key[fi + 2]) bins.push_back(i);
       if (order == 1) {
         std::stable_sort(bins.begin(), bins.end(), [&](int a, int c) {
           const auto& pa = h.h_path_items[a];
@@ -203,12 +232,12 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
           return static_cast<int64_t>(pa.ncols) * pa.num_lines > static_cast<int64_t>(pc.ncols) * pc.num_lines;
         });
       }
-    } else if (b.tof_grouped) {
+    } else if (b.family == B200RT_BATCH_KERNELS_TOF_GROUPED) {
       for (int bin = 0; bin < static_cast<int>(h.h_tof_basic_view.size()); ++bin)
-        if (h.h_tof_basic_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
+        if (h.h_tof_basic_view[bin] % f.nsub == key[fi + 2]) bins.push_back(bin);
     } else {
       for (int bin = 0; bin < static_cast<int>(h.h_bins.size()); ++bin)
-        if (h.h_bin_view[bin] % f.nsub == key[fi + 1]) bins.push_back(bin);
+        if (h.h_bin_view[bin] % f.nsub == key[fi + 2]) bins.push_back(bin);
       if (order == 1) {
         std::stable_sort(bins.begin(), bins.end(), [&](int a, int c) {
           const auto& pa = h.h_bins[a];
@@ -264,17 +293,17 @@ void batch_zero(b200rt_batch& b, int k, cudaStream_t st) {
 
 // one batched launch of one direction (0 forward with the ratio epilogue, 1 back projection of the ratios)
 cudaError_t batch_launch(b200rt_batch& b, int dir, const BatchItem* items, int n, int grid, cudaStream_t st) {
-  if (b.paths)
+  if (b.family == B200RT_BATCH_KERNELS_PATHS)
     return dir == 0 ? b200::launch_forward_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.npa, b.smem_f, b.d_frames.p, items,
                                                        n, b.counters.p, grid, st)
                     : b200::launch_back_batch_paths(b.d_geoms.p, b.d_pgeoms.p, b.smem_b, b.d_frames.p, items, n,
                                                     b.counters.p + 1, grid, st);
-  if (b.tof_grouped)
+  if (b.family == B200RT_BATCH_KERNELS_TOF_GROUPED)
     return dir == 0 ? b200::launch_forward_batch_tof(b.d_geoms.p, b.num_tof, b.d_frames.p, items, n, b.counters.p, grid,
                                                      st)
                     : b200::launch_back_batch_tof(b.d_geoms.p, b.num_tof, b.d_frames.p, items, n, b.counters.p + 1,
                                                   grid, st);
-  if (b.packed)
+  if (b.family == B200RT_BATCH_KERNELS_PACKED)
     return dir == 0 ? b200::launch_forward_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p, grid, st)
                     : b200::launch_back_batch_packed(b.d_geoms.p, b.d_frames.p, items, n, b.counters.p + 1, grid, st);
   return dir == 0 ? b200::launch_forward_batch(b.d_geoms.p, b.npa, b.smem, b.d_frames.p, items, n, b.counters.p, grid, st)
@@ -520,24 +549,30 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
     };
     float best_total = 1e30f;
     b200rt_batch_config best = b->cfg;
-    for (int order = 0; order <= 1; ++order) {
-      int n = 0;
-      const BatchItem* items = batch_items(*b, subiteration, order, n);
-      float tdir[2] = {1e30f, 1e30f};
-      int cdir[2] = {1, 1};
-      for (int dir = 0; dir < 2; ++dir)
-        for (int c = 1; c <= (dir == 0 ? b->max_fwd : b->max_back); ++c) {
-          const float t = time_launch(dir, items, n, c * b->num_sms);
-          if (t < tdir[dir]) {
-            tdir[dir] = t;
-            cdir[dir] = c;
+    for (int fam = B200RT_BATCH_KERNELS_PATHS; fam <= B200RT_BATCH_KERNELS_BASIC_BINS; ++fam) {
+      if (!b->avail[fam]) continue;
+      use_family(*b, fam);
+      // the TOF-grouped items keep basic-bin order
+      for (int order = 0; order <= (fam == B200RT_BATCH_KERNELS_TOF_GROUPED ? 0 : 1); ++order) {
+        int n = 0;
+        const BatchItem* items = batch_items(*b, subiteration, order, n);
+        float tdir[2] = {1e30f, 1e30f};
+        int cdir[2] = {1, 1};
+        for (int dir = 0; dir < 2; ++dir)
+          for (int c = 1; c <= (dir == 0 ? b->max_fwd : b->max_back); ++c) {
+            const float t = time_launch(dir, items, n, c * b->num_sms);
+            if (t < tdir[dir]) {
+              tdir[dir] = t;
+              cdir[dir] = c;
+            }
           }
+        if (tdir[0] + tdir[1] < best_total) {
+          best_total = tdir[0] + tdir[1];
+          best = b200rt_batch_config{cdir[0], cdir[1], order, fam};
         }
-      if (tdir[0] + tdir[1] < best_total) {
-        best_total = tdir[0] + tdir[1];
-        best = b200rt_batch_config{cdir[0], cdir[1], order};
       }
     }
+    use_family(*b, best.kernels);
     b->cfg = best;
     if (out) *out = best;
     cudaEventDestroy(e0);
@@ -554,8 +589,16 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
 int b200rt_batch_set_config(b200rt_batch* b, const b200rt_batch_config* config) {
   if (!b) return B200RT_ERR_INVALID_ARGUMENT;
   if (!config || config->ctas_per_sm_forward < 0 || config->ctas_per_sm_back < 0 || config->order < 0 ||
-      config->order > 1)
+      config->order > 1 || config->kernels < B200RT_BATCH_KERNELS_AUTO || config->kernels > B200RT_BATCH_KERNELS_BASIC_BINS)
     return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "invalid batch configuration");
+  if (b->ready) {  // otherwise checked when the batch is set up
+    try {
+      use_family(*b, config->kernels);
+    } catch (const std::exception& e) {
+      use_family(*b, b->cfg.kernels);
+      return bfail(b, B200RT_ERR_UNSUPPORTED, e.what());
+    }
+  }
   b->cfg = *config;
   drop_graphs(*b);
   return B200RT_OK;

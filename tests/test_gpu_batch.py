@@ -118,6 +118,7 @@ def test_batch_runs_in_pieces_and_autotunes(frames):
         xs.append(x)
     cfg = batch.autotune(1)
     assert cfg["ctas_per_sm_forward"] >= 1 and cfg["ctas_per_sm_back"] >= 1 and cfg["order"] in (0, 1)
+    assert cfg["kernels"] in (1, 2, 3, 4)  # the tuner names the family it chose
     assert batch.get_config() == cfg
     x0 = [x.clone() for x in xs]
     batch.run(1, 2, use_graph=True)
@@ -137,6 +138,31 @@ def test_batch_runs_in_pieces_and_autotunes(frames):
     batch.close()
 
 
+@pytest.mark.parametrize("kernels", [1, 3, 4])
+def test_batch_kernel_families(frames, kernels):
+    """Each kernel family the autotuner chooses among (column-staged path items, packed warp per basic bin, CTA per
+    basic bin; the 8-ring frames allow all three) reconstructs the frames as frame by frame does."""
+    import torch
+    from stir_b200.batch import BatchedOSMAPOSL
+    specs = _specs()
+    refs = _references(frames, specs)
+    batch = BatchedOSMAPOSL()
+    xs = []
+    for sp, (rec, _) in zip(specs, refs):
+        x = frames[sp["geom"]][0].empty_image().fill_(1.0)
+        brec = _recon(frames, sp)
+        brec.sensitivities = rec.sensitivities
+        batch.add(brec, x)
+        xs.append(x)
+    batch.set_config(order=1, kernels=kernels)
+    batch.run(1, None, use_graph=True)
+    torch.cuda.synchronize()
+    assert batch.get_config()["kernels"] == kernels
+    for sp, x, (_, ref) in zip(specs, xs, refs):
+        assert rel_l2(x.cpu().numpy(), ref) < BATCH_TOL, (kernels, sp)
+    batch.close()
+
+
 def test_batch_rejects_bad_frames(frames):
     import torch
     from stir_b200 import _abi
@@ -150,6 +176,8 @@ def test_batch_rejects_bad_frames(frames):
         batch.add(rec, x)
     with pytest.raises(_abi.B200Error):
         batch.set_config(order=5)
+    with pytest.raises(_abi.B200Error):
+        batch.set_config(kernels=7)
     batch.close()
 
 

@@ -142,6 +142,7 @@ def test_tof_osmaposl_quadratic_prior(cuda_device, oracle_lib):
     proj = RayTracingProjector(*G.tof_small_3d_pet(num_tof_bins=33), device=cuda_device)
     nt = proj.non_tof_projector()
     orc, orc_nt = oracle_lib.Oracle(proj.geometry), oracle_lib.Oracle(nt.geometry)
+    o64 = oracle_lib.Oracle(proj.geometry, 64)
     hpd, himg, dev = _host(proj)
     d = workloads.tof_data(proj)
     y, a, m = hpd(d["y"]), hpd(d["additive"]), hpd(d["mult"])
@@ -158,9 +159,11 @@ def test_tof_osmaposl_quadratic_prior(cuda_device, oracle_lib):
     rec = OSMAPOSLReconstruction(proj, d["y"], additive=d["additive"], mult=d["mult"], num_subsets=nsub,
                                  num_subiterations=n, prior=prior, use_tofsens=True).set_up()
     sens = [orc.sensitivity(m, s, nsub) for s in range(nsub)]
+    sens64 = [o64.sensitivity(m, s, nsub) for s in range(nsub)]
     for s in range(nsub):
         assert rel_l2(himg(rec.sensitivities[s]), sens[s]) <= SENS_TOL
     abi_prior = prior.as_abi(rec.map_model)
+    step64 = []
     xo = np.ones(proj.image_shape, np.float32)
     x_traj = proj.empty_image().fill_(1.0)
     step_errs = []
@@ -170,13 +173,18 @@ def test_tof_osmaposl_quadratic_prior(cuda_device, oracle_lib):
         x = dev(xo)
         rec.update_estimate(x)
         rec.update_estimate(x_traj)
+        # the same step in double from the same input: the float algorithm's own error
+        x64, _ = o64.osmaposl_update(xo.astype(np.float64), y, a, sens64[sub], sub, nsub, it, prior=abi_prior,
+                                     max_rel=3.4028234663852886e38)
         xo, _ = orc.osmaposl_update(xo, y, a, sens[sub], sub, nsub, it, prior=abi_prior,
                                     max_rel=3.4028234663852886e38)
         step_errs.append(rel_l2(himg(x), xo))
+        step64.append(rel_l2(himg(x), x64))
         assert step_errs[-1] <= 1e-5, (it, step_errs[-1])
     torch.cuda.synchronize()
-    _report("TOF OSMAPOSL QP 0.5, 21x3", max_step_vs_oracle=max(step_errs),
+    _report("TOF OSMAPOSL QP 0.5, 21x3", max_step_vs_oracle=max(step_errs), max_step_vs_fp64_oracle=max(step64),
             trajectory_vs_oracle=rel_l2(himg(x_traj), xo))
+    assert max(step64) <= FP64_BOUND
 
 
 def test_dynamic_frames_batched_vs_oracle(clinical, cuda_device, oracle_lib):
@@ -191,6 +199,7 @@ def test_dynamic_frames_batched_vs_oracle(clinical, cuda_device, oracle_lib):
     proj172 = RayTracingProjector(*G.clinical_3d_pet_half(), device=cuda_device)
     projs = {344: proj344, 172: proj172}
     orcs = {344: orc344, 172: oracle_lib.Oracle(proj172.geometry)}
+    o64s = {344: oracle_lib.Oracle(proj344.geometry, 64), 172: oracle_lib.Oracle(proj172.geometry, 64)}
     frames = workloads.dynamic_frames(projs, cuda_device)
     chosen = [frames[1], frames[21]]
     del frames
@@ -207,7 +216,7 @@ def test_dynamic_frames_batched_vs_oracle(clinical, cuda_device, oracle_lib):
         batch.add(rec, x)
         hpd, himg, _ = _host(p)
         state.append(dict(p=p, f=f, rec=rec, x=x, himg=himg, y=hpd(f["y"]), a=hpd(f["additive"]),
-                          xo=np.ones(p.image_shape, np.float32)))
+                          xo=np.ones(p.image_shape, np.float32), x64=np.ones(p.image_shape, np.float64)))
     errs = {344: [], 172: []}
     for k in range(1, n + 1):
         batch.run(k, 1, use_graph=False)
@@ -219,10 +228,15 @@ def test_dynamic_frames_batched_vs_oracle(clinical, cuda_device, oracle_lib):
             assert rel_l2(s["himg"](s["rec"].sensitivities[sub]), sens) <= SENS_TOL
             s["xo"], _ = orcs[size].osmaposl_update(s["xo"], s["y"], s["a"], sens, sub, nsub, k,
                                                     max_rel=3.4028234663852886e38)
+            s["x64"], _ = o64s[size].osmaposl_update(s["x64"], s["y"], s["a"], o64s[size].sensitivity(None, sub, nsub),
+                                                     sub, nsub, k, max_rel=3.4028234663852886e38)
             errs[size].append(rel_l2(s["himg"](s["x"]), s["xo"]))
             assert errs[size][-1] <= OSEM_TOL, (size, k, errs[size])
     batch.close()
-    _report("dynamic frames batched, 3 sub-iterations", frame_344=max(errs[344]), frame_172=max(errs[172]))
+    e64 = {s["f"]["size"]: rel_l2(s["himg"](s["x"]), s["x64"]) for s in state}
+    _report("dynamic frames batched, 3 sub-iterations", frame_344=max(errs[344]), frame_172=max(errs[172]),
+            frame_344_vs_fp64_oracle=e64[344], frame_172_vs_fp64_oracle=e64[172])
+    assert max(e64.values()) <= FP64_BOUND
 
 
 @pytest.fixture(scope="module")

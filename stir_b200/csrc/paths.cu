@@ -68,20 +68,24 @@ __device__ __forceinline__ void setup_path_lines(const ProjParams& p, const Path
   }
 }
 
-// image offsets of the chunk's columns under the item's symmetry operation (-1 outside the image)
-__device__ __forceinline__ void chunk_columns(const ProjParams& p, const PathParams& pp, const PathItemDev& it, int c0,
-                                              int kc, int* colbase) {
+// image offset of path column `col` under the item's symmetry operation (-1 outside the image)
+__device__ __forceinline__ int column_image_offset(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
+                                                   int col) {
   const int swap = it.flags & 1;
   const int sx = (it.flags & 2) ? -1 : 1;
   const int sy = (it.flags & 4) ? -1 : 1;
-  for (int i = threadIdx.x; i < kc; i += blockDim.x) {
-    const uint32_t pk = pp.cols[it.col_offset + c0 + i];
-    const int x = static_cast<int>(pk & 2047u) - 1024;
-    const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
-    const int xi = (swap ? y : x) * sx - p.min_x;
-    const int yi = (swap ? x : y) * sy - p.min_y;
-    colbase[i] = (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * p.nz : -1;
-  }
+  const uint32_t pk = pp.cols[it.col_offset + col];
+  const int x = static_cast<int>(pk & 2047u) - 1024;
+  const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
+  const int xi = (swap ? y : x) * sx - p.min_x;
+  const int yi = (swap ? x : y) * sy - p.min_y;
+  return (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * p.nz : -1;
+}
+
+// image offsets of the chunk's columns (-1 outside the image)
+__device__ __forceinline__ void chunk_columns(const ProjParams& p, const PathParams& pp, const PathItemDev& it, int c0,
+                                              int kc, int* colbase) {
+  for (int i = threadIdx.x; i < kc; i += blockDim.x) colbase[i] = column_image_offset(p, pp, it, c0 + i);
 }
 
 // the element range of unit (line, part) in chunk c; P = 1 << lgP parts
@@ -107,8 +111,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_al
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
@@ -284,9 +288,10 @@ __device__ __forceinline__ int pair_lines(const PathLineSmem* ls, int nl, int2* 
        ? gather_pass<NPA, NJ, TWO, true>(E, e0, e1, c0, cols, colbase, nz, cstride, coff, LA, LB, __VA_ARGS__)    \
        : gather_pass<NPA, NJ, TWO, false>(E, e0, e1, c0, cols, colbase, nz, cstride, coff, LA, LB, __VA_ARGS__))
 
-// One path item.  With padded staging the columns are copied by bulk copies completed on `bar` (phase parity
-// `phase`, flipped once per chunk); false when a copy was not seen to complete within the wait limit: the item is
-// then abandoned (no output written) and the projector's status word records it.
+// One path item.  With padded staging the columns are copied by bulk copies completed on `bar` (initialised for an
+// arrival by every thread of the CTA; phase parity `phase`, flipped once per chunk); false when a copy was not seen
+// to complete within the wait limit: the item is then abandoned (no output written) and the projector's status
+// word records it.
 template <int NPA, int EPI>
 __device__ __forceinline__ bool forward_path_item(const ProjParams& p, const PathParams& pp, const PathItemDev& it,
                                                   unsigned char* smem, const float* __restrict__ img,
@@ -328,17 +333,19 @@ __device__ __forceinline__ bool forward_path_item(const ProjParams& p, const Pat
   const int nch = (it.ncols + pp.K - 1) / pp.K;
   for (int c = 0; c < nch; ++c) {
     const int c0 = c * pp.K, kc = min(pp.K, it.ncols - c0);
-    // the previous chunk's reads and the zeroing come before this chunk's bulk copies into the same slots
+    // every thread's generic accesses to the staging buffer (the previous chunk's reads, the zeroing) come before
+    // the bulk copies that any thread issues after the barrier
     if (bulk) fence_proxy_async_smem();
     __syncthreads();  // previous chunk done (and the zeroing visible)
-    chunk_columns(p, pp, it, c0, kc, colbase);
-    __syncthreads();
     if (bulk) {
-      // one bulk copy per column: the whole 16-byte blocks that hold its nz planes, to its slot's 16-byte
-      // boundary, so plane 0 lands at the column's phase (its address mod 16, in floats), which colbase[ci]
-      // records as the column's staged start; columns outside the image are zeroed instead
+      // Thread t owns columns t, t + blockDim.x, ...: one bulk copy each, of the whole 16-byte blocks that hold its
+      // nz planes, to its slot's 16-byte boundary, so plane 0 lands at the column's phase (its address mod 16, in
+      // floats), which colbase[ci] records as the column's staged start; a column outside the image is zeroed
+      // instead.  Every thread then arrives on the barrier (after its byte counts), so the phase completes when all
+      // the chunk's copies have landed.
+      const int ext = (nz + 6) & ~3;  // a slot's copies reach at most round_up4(nz + 3) floats from its start
       for (int ci = threadIdx.x; ci < kc; ci += blockDim.x) {
-        const int b = colbase[ci];
+        const int b = column_image_offset(p, pp, it, c0 + ci);
         const int d = ci * cstride + coff;
         float* slot = cols + d;
         int start = d;
@@ -350,13 +357,22 @@ __device__ __forceinline__ bool forward_path_item(const ProjParams& p, const Pat
           bulk_copy_to_smem(slot, src - ph, bytes, bar);
           start += ph;
         } else {
-          for (int z = 0; z < ((nz + 6) & ~3); ++z) slot[z] = 0.f;
+          for (int z = 0; z < ext; ++z) slot[z] = 0.f;
         }
         colbase[ci] = start;
       }
-      __syncthreads();  // every byte count is on the barrier before its arrival
-      if (threadIdx.x == 0) mbar_arrive(bar);
+      mbar_arrive(bar);
       const bool done = mbar_wait_bounded(bar, phase);
+      if (done) {
+        // the owner puts back to zeros everything of its slots' [0, ext) that is not this chunk's column (the
+        // neighbouring planes copied with the blocks, and what an earlier chunk's column with another phase left
+        // there): at most 3 planes below plane 0, 6 above nz - 1
+        for (int ci = threadIdx.x; ci < kc; ci += blockDim.x) {
+          const int d = ci * cstride + coff, ph = colbase[ci] - d;
+          for (int k = 0; k < ph; ++k) cols[d + k] = 0.f;
+          for (int z = ph + nz; z < ext; ++z) cols[d + z] = 0.f;
+        }
+      }
       if (!__syncthreads_and(done)) {
         // not seen to complete: record it, give the copies in flight one more bounded wait, abandon the item
         if (threadIdx.x == 0 && pp.status) atomicOr(pp.status, 1u);
@@ -364,21 +380,10 @@ __device__ __forceinline__ bool forward_path_item(const ProjParams& p, const Pat
         return false;
       }
       phase ^= 1u;
-      // a slot's copies reach at most ext = round_up4(nz + 3) floats from its start: everything of [0, ext) that is
-      // not this chunk's column (the neighbouring planes copied with the blocks, and what an earlier chunk's
-      // column with another phase left there) back to zeros -- at most 3 planes below plane 0, 6 above nz - 1
-      const int ext = (nz + 6) & ~3;
-      for (int i = threadIdx.x; i < kc * 16; i += blockDim.x) {
-        const int ci = i >> 4, k = i & 15;
-        const int d = ci * cstride + coff, ph = colbase[ci] - d;
-        if (k < 4) {
-          if (k < ph) cols[d + k] = 0.f;
-        } else {
-          const int z = ph + nz + (k - 4);
-          if (z < ext) cols[d + z] = 0.f;
-        }
-      }
+      // every column and its zeros are visible (the barrier above): the gather follows
     } else {
+      chunk_columns(p, pp, it, c0, kc, colbase);
+      __syncthreads();
       for (int ci = warp; ci < kc; ci += kPathWarps) {
         const int b = colbase[ci];
         float* dst = cols + ci * cstride + coff;
@@ -389,8 +394,8 @@ __device__ __forceinline__ bool forward_path_item(const ProjParams& p, const Pat
         }
       }
       cp_async_wait();
+      __syncthreads();
     }
-    __syncthreads();
     for (int u = warp; u < U; u += kPathWarps) {
       const int pr = u >> lgP, part = u & (P - 1);
       const int2 pl = pairs[pr];
@@ -734,7 +739,7 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
     if (ep.small_value) ep.small_value += b * ep.sv_stride;
   }
   __shared__ __align__(8) uint64_t bar;
-  if (threadIdx.x == 0) mbar_init(&bar);
+  if (threadIdx.x == 0) mbar_init(&bar, blockDim.x);
   __syncthreads();
   double ll = 0.0;
   unsigned ncancel = 0;
@@ -830,7 +835,7 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ BatchPathStage st;
   __shared__ __align__(8) uint64_t bar;
-  if (threadIdx.x == 0) mbar_init(&bar);
+  if (threadIdx.x == 0) mbar_init(&bar, blockDim.x);
   unsigned phase = 0;  // next_path_item synchronises the CTA before the barrier's first use
   while (next_path_item(counter, items, nitems, geoms, pgeoms, frames, st)) {
     double ll = 0.0;

@@ -359,7 +359,9 @@ void batch_subiteration(b200rt_batch& b, int k, cudaStream_t st) {
   // every frame's update (OSMAPOSLReconstruction.cxx:394-510) in three launches
   int n = 0, max_blocks = 1;
   const b200::BatchUpdateDev* upd = batch_updates(b, k, n, max_blocks);
-  ck(b200::launch_batch_update(upd, n, max_blocks, st), "update");
+  bool any_prior = false;
+  for (auto& fp : b.frames) any_prior = any_prior || (k <= fp->num_subiters && fp->has_prior);
+  ck(b200::launch_batch_update(upd, n, max_blocks, any_prior, st), "update");
 }
 
 }  // namespace

@@ -313,7 +313,8 @@ void fill_batch_update(BatchUpdateDev& d, float* u, float* x, const float* sens,
                        const float prior_weights[27], int num_subsets, int subiteration_num, float min_rel, float max_rel,
                        int ny, int nx, int nz, float* partial_max, float* umax);
 // the updates of several frames: three launches (grid.y = frame), max_blocks = the largest nblocks
-cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, cudaStream_t st);
+cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, bool any_prior,
+                                cudaStream_t st);
 
 // launchers (project.cu)
 cudaError_t launch_forward(const ProjParams& p, const int* bin_list, int nbins, const float* image, float* projdata,

@@ -149,42 +149,78 @@ __global__ void reduce_max_kernel(const float* __restrict__ partial, int n, floa
   reduce_max_body(partial, n, out);
 }
 
-// pass 2: u /= denominator with divide()'s threshold, clamp, x *= u
+// pass 2: u /= denominator with divide()'s threshold, clamp, x *= u -- one voxel
+__device__ __forceinline__ void update_apply_one(float& uv, float& xv, float s, float gv, int prior, int map_model,
+                                                 float num_subsets, float sv, int clamp, float min_rel, float max_rel) {
+  float den;
+  if (!prior) {
+    den = s;
+  } else if (map_model == 0) {
+    // additive MAP model (OSMAPOSLReconstruction.cxx:415-433)
+    den = gv / num_subsets + s;
+    den = fmaxf(fminf(den, s * 10), s / 10);
+  } else {
+    // multiplicative MAP model (:436-453)
+    den = gv + 1;
+    den = fmaxf(fminf(den, 10.F), 1 / 10.F);
+    den *= s;
+  }
+  float v = uv;
+  if (fabsf(den) <= sv && fabsf(v) <= sv)
+    v = 0;
+  else
+    v /= den;
+  if (clamp) {
+    // threshold_upper_lower (thresholding.h:45-54)
+    if (v > max_rel)
+      v = max_rel;
+    else if (min_rel > v)
+      v = min_rel;
+  }
+  uv = v;
+  xv *= v;
+}
+
+// pass 2 over the image: 16-byte loads and stores where every array allows them (elementwise, so the same results)
 __device__ __forceinline__ void update_apply_body(int blk, int nblk, float* __restrict__ u, float* __restrict__ x,
                                                   const float* __restrict__ sens, const float* __restrict__ g, int prior,
                                                   int map_model, float num_subsets, const float* __restrict__ umax,
                                                   float small_num, int clamp, float min_rel, float max_rel, int64_t n) {
-  float sv = *umax * small_num;
-  sv = sv > 0 ? sv : 0;
-  for (int64_t i = blk * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<int64_t>(nblk) * blockDim.x) {
-    const float s = sens[i];
-    float den;
-    if (!prior) {
-      den = s;
-    } else if (map_model == 0) {
-      // additive MAP model (OSMAPOSLReconstruction.cxx:415-433)
-      den = g[i] / num_subsets + s;
-      den = fmaxf(fminf(den, s * 10), s / 10);
-    } else {
-      // multiplicative MAP model (:436-453)
-      den = g[i] + 1;
-      den = fmaxf(fminf(den, 10.F), 1 / 10.F);
-      den *= s;
+  // divide()'s threshold small_num x max(u); without a prior small_num is 0 and max(u) is not needed (or computed)
+  float sv = 0.f;
+  if (small_num > 0.f) {
+    sv = *umax * small_num;
+    sv = sv > 0 ? sv : 0;
+  }
+  const int64_t stride = static_cast<int64_t>(nblk) * blockDim.x;
+  const int64_t t0 = blk * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const uintptr_t al = reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(x) |
+                       reinterpret_cast<uintptr_t>(sens) | (prior ? reinterpret_cast<uintptr_t>(g) : 0);
+  int64_t i0 = 0;
+  if ((al & 15) == 0) {
+    const int64_t n4 = n / 4;
+    float4* u4 = reinterpret_cast<float4*>(u);
+    float4* x4 = reinterpret_cast<float4*>(x);
+    const float4* s4 = reinterpret_cast<const float4*>(sens);
+    const float4* g4 = reinterpret_cast<const float4*>(g);
+    for (int64_t i = t0; i < n4; i += stride) {
+      float4 U = u4[i], X = x4[i];
+      const float4 S = s4[i];
+      const float4 G = prior ? g4[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      update_apply_one(U.x, X.x, S.x, G.x, prior, map_model, num_subsets, sv, clamp, min_rel, max_rel);
+      update_apply_one(U.y, X.y, S.y, G.y, prior, map_model, num_subsets, sv, clamp, min_rel, max_rel);
+      update_apply_one(U.z, X.z, S.z, G.z, prior, map_model, num_subsets, sv, clamp, min_rel, max_rel);
+      update_apply_one(U.w, X.w, S.w, G.w, prior, map_model, num_subsets, sv, clamp, min_rel, max_rel);
+      u4[i] = U;
+      x4[i] = X;
     }
-    float v = u[i];
-    if (fabsf(den) <= sv && fabsf(v) <= sv)
-      v = 0;
-    else
-      v /= den;
-    if (clamp) {
-      // threshold_upper_lower (thresholding.h:45-54)
-      if (v > max_rel)
-        v = max_rel;
-      else if (min_rel > v)
-        v = min_rel;
-    }
-    u[i] = v;
-    x[i] *= v;
+    i0 = n4 * 4;
+  }
+  for (int64_t i = i0 + t0; i < n; i += stride) {
+    float uv = u[i], xv = x[i];
+    update_apply_one(uv, xv, sens[i], prior ? g[i] : 0.f, prior, map_model, num_subsets, sv, clamp, min_rel, max_rel);
+    u[i] = uv;
+    x[i] = xv;
   }
 }
 
@@ -200,13 +236,15 @@ __global__ void update_apply_kernel(float* __restrict__ u, float* __restrict__ x
 // count of its own launch, so the results are those of launch_update frame by frame
 __global__ void batch_update_prepare_kernel(const BatchUpdateDev* __restrict__ frames) {
   const BatchUpdateDev& f = frames[blockIdx.y];
-  if (static_cast<int>(blockIdx.x) >= f.nblocks) return;
+  // frames without a prior need neither the prior gradient nor max(u) (divide()'s threshold is 0 for them)
+  if (static_cast<int>(blockIdx.x) >= f.nblocks || f.prior_type == 0) return;
   PriorDev pr;
   prior_dev_from(f, pr);
   update_prepare_body(blockIdx.x, f.nblocks, f.u, f.x, f.g, pr, f.ny, f.nx, f.nz, f.partial_max);
 }
 __global__ void batch_reduce_max_kernel(const BatchUpdateDev* __restrict__ frames) {
   const BatchUpdateDev& f = frames[blockIdx.x];
+  if (f.prior_type == 0) return;
   reduce_max_body(f.partial_max, f.nblocks, f.umax);
 }
 __global__ void batch_update_apply_kernel(const BatchUpdateDev* __restrict__ frames) {
@@ -706,12 +744,13 @@ cudaError_t launch_update(float* u, float* x, const float* sens, float* g, const
     for (int k = 0; k < 27; ++k) pr.w[k] = prior_weights[k];
     pr.kappa = prior->kappa_dev;
   }
-  update_prepare_kernel<<<blocks, 256, 0, st>>>(u, x, g, pr, ny, nx, nz, partial_max);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  reduce_max_kernel<<<1, 1024, 0, st>>>(partial_max, blocks, umax);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if (has_prior) {  // the prior gradient and max(u) for divide()'s threshold (0 without a prior: not needed)
+    update_prepare_kernel<<<blocks, 256, 0, st>>>(u, x, g, pr, ny, nx, nz, partial_max);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    reduce_max_kernel<<<1, 1024, 0, st>>>(partial_max, blocks, umax);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   update_apply_kernel<<<blocks, 256, 0, st>>>(u, x, sens, g, has_prior ? 1 : 0, has_prior ? prior->map_model : 0,
                                                static_cast<float>(num_subsets), umax, has_prior ? 0.000001F : 0.F,
                                                subiteration_num != 1, min_rel, max_rel, n);
@@ -752,14 +791,16 @@ void fill_batch_update(BatchUpdateDev& d, float* u, float* x, const float* sens,
   d.max_rel = max_rel;
 }
 
-cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, cudaStream_t st) {
+cudaError_t launch_batch_update(const BatchUpdateDev* frames_dev, int nframes, int max_blocks, bool any_prior,
+                                cudaStream_t st) {
   if (nframes <= 0) return cudaSuccess;
-  batch_update_prepare_kernel<<<dim3(max_blocks, nframes), 256, 0, st>>>(frames_dev);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  batch_reduce_max_kernel<<<nframes, 1024, 0, st>>>(frames_dev);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  if (any_prior) {  // prior gradients and max(u) of the frames with a prior
+    batch_update_prepare_kernel<<<dim3(max_blocks, nframes), 256, 0, st>>>(frames_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    batch_reduce_max_kernel<<<nframes, 1024, 0, st>>>(frames_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   batch_update_apply_kernel<<<dim3(max_blocks, nframes), 256, 0, st>>>(frames_dev);
   return cudaGetLastError();
 }

@@ -417,7 +417,8 @@ typedef struct b200rt_batch b200rt_batch;
 typedef struct {
   int ctas_per_sm_forward; /* persistent CTAs per SM; 0 = as many as fit */
   int ctas_per_sm_back;
-  int order;               /* work order inside a frame: 0 = basic-bin order, 1 = longest rows first */
+  int order;               /* work order: 0 = frame by frame in basic-bin order, 1 = frame by frame, longest rows
+                            * first, 2 = item by item across the frames of one geometry and subset */
   int kernels;             /* kernel family, B200RT_BATCH_KERNELS_* */
 } b200rt_batch_config;
 /* Kernel families of the batched projectors (how the work of a frame is cut into work items):

@@ -217,6 +217,7 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
     return it->second->p;
   }
   std::vector<BatchItem> list;
+  std::vector<std::vector<int>> per_frame(b.frames.size());
   for (size_t fi = 0; fi < b.frames.size(); ++fi) {
     if (key[fi + 2] < 0) continue;
     const auto& f = *b.frames[fi];
@@ -246,7 +247,27 @@ const BatchItem* batch_items(b200rt_batch& b, int k, int order, int& count) {
         });
       }
     }
-    for (int bin : bins) list.push_back(BatchItem{static_cast<int>(fi), bin});
+    per_frame[fi] = std::move(bins);
+  }
+  if (order == 2) {
+    // item-major: frames of one geometry in the same subset take each work item in turn, so that its row is read
+    // from HBM once for all of them
+    std::vector<bool> done(b.frames.size(), false);
+    for (size_t fi = 0; fi < b.frames.size(); ++fi) {
+      if (done[fi] || key[fi + 2] < 0) continue;
+      std::vector<size_t> group;
+      for (size_t fj = fi; fj < b.frames.size(); ++fj)
+        if (!done[fj] && key[fj + 2] == key[fi + 2] && b.frames[fj]->geom == b.frames[fi]->geom &&
+            b.frames[fj]->nsub == b.frames[fi]->nsub) {
+          group.push_back(fj);
+          done[fj] = true;
+        }
+      for (size_t i = 0; i < per_frame[fi].size(); ++i)
+        for (size_t fj : group) list.push_back(BatchItem{static_cast<int>(fj), per_frame[fj][i]});
+    }
+  } else {
+    for (size_t fi = 0; fi < b.frames.size(); ++fi)
+      for (int bin : per_frame[fi]) list.push_back(BatchItem{static_cast<int>(fi), bin});
   }
   auto buf = std::make_unique<DevBuf<BatchItem>>();
   buf->upload(list, b.capture_stream);
@@ -554,8 +575,8 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
     for (int fam = B200RT_BATCH_KERNELS_PATHS; fam <= B200RT_BATCH_KERNELS_BASIC_BINS; ++fam) {
       if (!b->avail[fam]) continue;
       use_family(*b, fam);
-      // the TOF-grouped items keep basic-bin order
-      for (int order = 0; order <= (fam == B200RT_BATCH_KERNELS_TOF_GROUPED ? 0 : 1); ++order) {
+      for (int order = 0; order <= 2; ++order) {
+        if (order == 1 && fam == B200RT_BATCH_KERNELS_TOF_GROUPED) continue;  // TOF-grouped items: no length sort
         int n = 0;
         const BatchItem* items = batch_items(*b, subiteration, order, n);
         float tdir[2] = {1e30f, 1e30f};
@@ -591,7 +612,7 @@ int b200rt_batch_autotune(b200rt_batch* b, int subiteration, b200rt_batch_config
 int b200rt_batch_set_config(b200rt_batch* b, const b200rt_batch_config* config) {
   if (!b) return B200RT_ERR_INVALID_ARGUMENT;
   if (!config || config->ctas_per_sm_forward < 0 || config->ctas_per_sm_back < 0 || config->order < 0 ||
-      config->order > 1 || config->kernels < B200RT_BATCH_KERNELS_AUTO || config->kernels > B200RT_BATCH_KERNELS_BASIC_BINS)
+      config->order > 2 || config->kernels < B200RT_BATCH_KERNELS_AUTO || config->kernels > B200RT_BATCH_KERNELS_BASIC_BINS)
     return bfail(b, B200RT_ERR_INVALID_ARGUMENT, "invalid batch configuration");
   if (b->ready) {  // otherwise checked when the batch is set up
     try {

@@ -74,7 +74,7 @@ __device__ __forceinline__ int column_image_offset(const ProjParams& p, const Pa
   const int swap = it.flags & 1;
   const int sx = (it.flags & 2) ? -1 : 1;
   const int sy = (it.flags & 4) ? -1 : 1;
-  const uint32_t pk = pp.cols[it.col_offset + col];
+  const uint32_t pk = __ldg(pp.cols + it.col_offset + col);
   const int x = static_cast<int>(pk & 2047u) - 1024;
   const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
   const int xi = (swap ? y : x) * sx - p.min_x;
@@ -480,17 +480,6 @@ struct FixedCols {
   }
 };
 
-// image offset of column `slot` of the item's path under its symmetry operation (-1 outside the image)
-__device__ __forceinline__ int column_base(const ProjParams& p, const PathParams& pp, const PathItemDev& it, int slot) {
-  const uint32_t pk = __ldg(pp.cols + it.col_offset + slot);
-  const int x = static_cast<int>(pk & 2047u) - 1024;
-  const int y = static_cast<int>((pk >> 11) & 2047u) - 1024;
-  const int swap = it.flags & 1;
-  const int xi = (swap ? y : x) * ((it.flags & 2) ? -1 : 1) - p.min_x;
-  const int yi = (swap ? x : y) * ((it.flags & 4) ? -1 : 1) - p.min_y;
-  return (xi >= 0 && xi < p.nx && yi >= 0 && yi < p.ny) ? (yi * p.nx + xi) * p.nz : -1;
-}
-
 // Planes [zp, zp + 128) of the columns whose elements are [e_begin, e_end) of the path in column order, when every
 // window of every (element, line) meets the image (checked at set-up, PathParams::zpad >= 0; an inactive line's
 // data are all zero).  One warp streams through the elements of a contiguous range of columns, 32 at a time: each
@@ -560,7 +549,7 @@ __device__ __forceinline__ void back_span(const ProjParams& p, const PathParams&
       const unsigned pk = static_cast<unsigned>(w.w);
       if (pk & 4u) {
         flush();
-        b = column_base(p, pp, it, static_cast<int>(pk >> 3));
+        b = column_image_offset(p, pp, it, static_cast<int>(pk >> 3));
       }
       const float ev = __int_as_float(w.x);
       const unsigned n = pk & 3u;
@@ -717,7 +706,7 @@ __device__ __forceinline__ void back_path_item(const ProjParams& p, const PathPa
     return;
   }
   for (int ci = warp; ci < it.ncols; ci += kPathWarps) {
-    const int b = column_base(p, pp, it, ci);
+    const int b = column_image_offset(p, pp, it, ci);
     const int k0 = __ldg(cs + ci), k1 = __ldg(cs + ci + 1);
     for (int zp = 0; zp < nz; zp += 128) back_column<Cols, false>(E, k0, k1, lz, members, dl, zp, nz, lane, b, acc, eb);
   }

@@ -117,7 +117,7 @@ def test_batch_runs_in_pieces_and_autotunes(frames):
         batch.add(brec, x)
         xs.append(x)
     cfg = batch.autotune(1)
-    assert cfg["ctas_per_sm_forward"] >= 1 and cfg["ctas_per_sm_back"] >= 1 and cfg["order"] in (0, 1)
+    assert cfg["ctas_per_sm_forward"] >= 1 and cfg["ctas_per_sm_back"] >= 1 and cfg["order"] in (0, 1, 2)
     assert cfg["kernels"] in (1, 2, 3, 4)  # the tuner names the family it chose
     assert batch.get_config() == cfg
     x0 = [x.clone() for x in xs]
@@ -154,7 +154,7 @@ def test_batch_kernel_families(frames, kernels):
         brec.sensitivities = rec.sensitivities
         batch.add(brec, x)
         xs.append(x)
-    batch.set_config(order=1, kernels=kernels)
+    batch.set_config(order=2 if kernels == 1 else 1, kernels=kernels)  # item by item across frames, or longest first
     batch.run(1, None, use_graph=True)
     torch.cuda.synchronize()
     assert batch.get_config()["kernels"] == kernels

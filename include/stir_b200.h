@@ -310,6 +310,17 @@ int b200rt_log_likelihood_batch_dev(b200rt_projector* h, const float* images_dev
                                     int64_t additive_stride, const float* mult_dev, int64_t mult_stride, int batch,
                                     int subset_num, int num_subsets, int zero_seg0_end_planes, double* values,
                                     void* stream);
+/* The log-likelihood of every image of the batch (as b200rt_log_likelihood_batch_dev, the same sums in the same
+ * order) and, from the same projection, each image's gradient ratio divide_and_truncate(y, A x + a) - m written to
+ * ratio_dev + b * ratio_stride (device layout; bins outside the subset are not written), so that the gradient is then
+ * one b200rt_back_project_batch_dev of the ratios, without projecting again.  No STIR counterpart: STIR computes
+ * the value (accumulate_loglikelihood, ...AndProjData.cxx:1483-1515) and the sub-gradient (:1421-1481) in separate
+ * passes.  Column-staged projectors only (B200RT_ERR_UNSUPPORTED otherwise).  Synchronises and writes values[b]. */
+int b200rt_log_likelihood_and_ratio_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
+                                               const float* y_dev, int64_t y_stride, const float* additive_dev,
+                                               int64_t additive_stride, const float* mult_dev, int64_t mult_stride,
+                                               int batch, int subset_num, int num_subsets, int zero_seg0_end_planes,
+                                               double* values, float* ratio_dev, int64_t ratio_stride, void* stream);
 int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
                                              const float* y_dev, int64_t y_stride, const float* additive_dev,
                                              int64_t additive_stride, const float* mult_dev, int64_t mult_stride,

@@ -285,6 +285,8 @@ EXPORTS = [
     ("b200rt_forward_project_batch_dev", _I, [_P, _P, _I64, _P, _I64, _I, _I, _I, _P]),
     ("b200rt_back_project_batch_dev", _I, [_P, _P, _I64, _P, _I64, _I, _I, _I, _I, _P]),
     ("b200rt_log_likelihood_batch_dev", _I, [_P, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _I, _P, _P]),
+    ("b200rt_log_likelihood_and_ratio_batch_dev", _I, [_P, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _I,
+                                                    ctypes.POINTER(ctypes.c_double), _P, _I64, _P]),
     ("b200rt_log_likelihood_gradient_batch_dev", _I, [_P, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I, _I, _I, _I, _I,
                                                      _P, _I64, _P]),
     ("b200rt_gibbs_last_error", ctypes.c_char_p, [_P]),

@@ -5,8 +5,9 @@
   A batch [B][...] goes through the batch entry points: one launch over (path item, image) per direction.
 * `PoissonLogLikelihood`: the objective of PoissonLogLikelihoodWithLinearModelForMeanAndProjData
   (value: accumulate_loglikelihood in FP64; gradient: A^T[divide_and_truncate(y, A x + a) - m],
-  ...AndProjData.cxx:1421-1515).  Only x is saved for backward: the projection A x is recomputed
-  there, so a batch needs no stored sinograms however large it is.
+  ...AndProjData.cxx:1421-1515).  The forward pass projects once and, when the batch's gradient ratios fit in
+  free device memory, keeps them for backward, which is then one back projection; otherwise only x is saved and
+  backward projects again (`store_ratio`: None decides by the free memory, True / False force either).
 * `Prior`: QuadraticPrior / RelativeDifferencePrior value and gradient on the device.
 
 Images are torch float32 CUDA tensors in the device layout [y][x][z] (or a batch [B][y][x][z]);
@@ -119,17 +120,39 @@ def _data_strides(proj, B, y, additive, mult):
     return one(y, "y"), one(additive, "additive"), one(mult, "mult")
 
 
+def _ratio_fits(proj, B, device):
+    """Whether B gradient ratios (projection data of each image) fit in the free device memory with room to spare."""
+    free, _ = torch.cuda.mem_get_info(device)
+    need = 4 * B * proj.projdata_size
+    return need + need // 4 + (512 << 20) <= free
+
+
 class _LogLikelihood(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode):
+    def forward(ctx, x, proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode, store_ratio):
         n_img = _n_img(proj)
         xs = x.detach().contiguous().reshape(-1, n_img)
         B = xs.shape[0]
         (yy, ys), (aa, as_), (mm, ms) = _data_strides(proj, B, y, additive, mult)
         values = (ctypes.c_double * B)()
-        _abi.check(proj.lib.b200rt_log_likelihood_batch_dev(proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B,
-                                                            subset_num, num_subsets, int(zero_ends), values,
-                                                            _stream_ptr(None)), proj.h, "b200rt_log_likelihood_batch_dev")
+        ctx.ratio = None
+        keep = ctx.needs_input_grad[0] and proj.info.num_tof_bins <= 1 and \
+            (store_ratio if store_ratio is not None else _ratio_fits(proj, B, x.device))
+        if keep:
+            # value and gradient ratios from one projection (bins outside the subset are never read back)
+            n_pd = proj.projdata_size
+            ratio = torch.empty((B, n_pd), dtype=torch.float32, device=x.device)
+            st = proj.lib.b200rt_log_likelihood_and_ratio_batch_dev(
+                proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B, subset_num, num_subsets, int(zero_ends),
+                values, _p(ratio), n_pd, _stream_ptr(None))
+            if st == _abi.OK:
+                ctx.ratio = ratio
+            elif st != _abi.ERR_UNSUPPORTED:
+                _abi.check(st, proj.h, "b200rt_log_likelihood_and_ratio_batch_dev")
+        if ctx.ratio is None:
+            _abi.check(proj.lib.b200rt_log_likelihood_batch_dev(proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms,
+                                                                B, subset_num, num_subsets, int(zero_ends), values,
+                                                                _stream_ptr(None)), proj.h, "b200rt_log_likelihood_batch_dev")
         ctx.save_for_backward(x)
         ctx.args = (proj, y, additive, mult, subset_num, num_subsets, zero_ends, mode)
         return torch.tensor(sum(values[b] for b in range(B)), dtype=torch.float64, device=x.device)
@@ -141,12 +164,18 @@ class _LogLikelihood(torch.autograd.Function):
         n_img = _n_img(proj)
         xs = x.detach().contiguous().reshape(-1, n_img)
         B = xs.shape[0]
+        if ctx.ratio is not None:
+            grad = torch.empty_like(xs)
+            _back_batch(proj, ctx.ratio, grad, subset_num, num_subsets, mode)
+            ctx.ratio = None
+            return ((grad.reshape(x.shape) * gout.to(torch.float32)), None, None, None, None, None, None, None, None,
+                    None)
         (yy, ys), (aa, as_), (mm, ms) = _data_strides(proj, B, y, additive, mult)
         grad = torch.empty_like(xs)
         _abi.check(proj.lib.b200rt_log_likelihood_gradient_batch_dev(
             proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B, subset_num, num_subsets, int(zero_ends), mode,
             _p(grad), n_img, _stream_ptr(None)), proj.h, "b200rt_log_likelihood_gradient_batch_dev")
-        return (grad.reshape(x.shape) * gout.to(torch.float32)), None, None, None, None, None, None, None, None
+        return (grad.reshape(x.shape) * gout.to(torch.float32)), None, None, None, None, None, None, None, None, None
 
 
 class PoissonLogLikelihood(torch.nn.Module):
@@ -154,16 +183,17 @@ class PoissonLogLikelihood(torch.nn.Module):
     STIR's accumulate_loglikelihood.  Differentiable in x; `forward` returns a float64 scalar tensor."""
 
     def __init__(self, projector: RayTracingProjector, y, additive=None, mult=None, subset_num=0, num_subsets=1,
-                 zero_seg0_end_planes=False, mode=_abi.BACKPROJECT_ATOMIC):
+                 zero_seg0_end_planes=False, mode=_abi.BACKPROJECT_ATOMIC, store_ratio=None):
         super().__init__()
         self.proj = projector
         self.y, self.additive, self.mult = y.contiguous(), additive, mult
         self.subset_num, self.num_subsets = subset_num, num_subsets
         self.zero_ends, self.mode = zero_seg0_end_planes, mode
+        self.store_ratio = store_ratio
 
     def forward(self, x):
         return _LogLikelihood.apply(x, self.proj, self.y, self.additive, self.mult, self.subset_num, self.num_subsets,
-                                    self.zero_ends, self.mode)
+                                    self.zero_ends, self.mode, self.store_ratio)
 
 
 class _Prior(torch.autograd.Function):

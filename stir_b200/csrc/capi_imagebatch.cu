@@ -139,6 +139,53 @@ int b200rt_log_likelihood_batch_dev(b200rt_projector* h, const float* images_dev
   }
 }
 
+int b200rt_log_likelihood_and_ratio_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
+                                               const float* y_dev, int64_t y_stride, const float* additive_dev,
+                                               int64_t additive_stride, const float* mult_dev, int64_t mult_stride,
+                                               int batch, int subset_num, int num_subsets, int zero_seg0_end_planes,
+                                               double* values, float* ratio_dev, int64_t ratio_stride, void* stream) {
+  if (!h || !images_dev || !y_dev || !values || !ratio_dev) return fail(h, B200RT_ERR_INVALID_ARGUMENT, "null argument");
+  if (int st = check_subset(h, subset_num, num_subsets)) return st;
+  if (int st = check_batch(h, batch, image_stride, ratio_stride)) return st;
+  if (!h->use_paths)
+    return fail(h, B200RT_ERR_UNSUPPORTED,
+                "b200rt_log_likelihood_and_ratio_batch_dev needs the column-staged kernels (non-TOF projector)");
+  try {
+    DeviceGuard dg(h->device);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int n = 0;
+    const int* list = path_list(*h, subset_num, num_subsets, n);
+    h->cancelled.alloc(1);
+    ck(cudaMemsetAsync(h->cancelled.p, 0, sizeof(unsigned int), st), "memset");
+    FwdEpilogue ep{};
+    ep.mode = kEpiLoglikRatio;
+    ep.zero_ends = zero_seg0_end_planes;
+    ep.y = y_dev;
+    ep.y_stride = y_stride;
+    ep.add = additive_dev;
+    ep.add_stride = additive_stride;
+    ep.mult = mult_dev;
+    ep.mult_stride = mult_stride;
+    ep.cancelled = h->cancelled.p;
+    ep.small_value = batch_thresholds(*h, y_dev, y_stride, batch, subset_num, num_subsets, zero_seg0_end_planes, st,
+                                      ep.sv_stride);
+    const size_t np = static_cast<size_t>(std::max(n, 1)) * batch;
+    if (h->ll_partials.n < np) h->ll_partials.alloc(np);
+    if (h->ll_sum.n < static_cast<size_t>(batch)) h->ll_sum.alloc(batch);
+    ep.partials = h->ll_partials.p;
+    ck(launch_forward_paths_batch(h->params, h->pparams, list, n, images_dev, image_stride, ratio_dev, ratio_stride,
+                                  batch, st, &ep),
+       "log-likelihood");
+    for (int b = 0; b < batch; ++b)
+      ck(launch_reduce_sum(h->ll_partials.p + static_cast<int64_t>(b) * n, n, h->ll_sum.p + b, st), "reduce");
+    ck(cudaMemcpyAsync(values, h->ll_sum.p, sizeof(double) * batch, cudaMemcpyDeviceToHost, st), "D2H");
+    ck(cudaStreamSynchronize(st), "log-likelihood");
+    return B200RT_OK;
+  } catch (const std::exception& e) {
+    return fail(h, status_of(e), e.what());
+  }
+}
+
 int b200rt_log_likelihood_gradient_batch_dev(b200rt_projector* h, const float* images_dev, int64_t image_stride,
                                              const float* y_dev, int64_t y_stride, const float* additive_dev,
                                              int64_t additive_stride, const float* mult_dev, int64_t mult_stride,

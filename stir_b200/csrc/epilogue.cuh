@@ -21,7 +21,7 @@ __device__ __forceinline__ void forward_store(const ProjParams& p, int seg, int 
   const float y = zend ? 0.f : __ldg(ep.y + idx);
   const float av = (ep.add && !zend) ? __ldg(ep.add + idx) : 0.f;
   const float sv = ep.small_value[(tofi * (2 * p.S + 1) + seg + p.S) * p.num_views + view];
-  if (EPI == kEpiRatio || EPI == kEpiGradient) {
+  if (EPI == kEpiRatio || EPI == kEpiGradient || EPI == kEpiLoglikRatio) {
     // divide_and_truncate (recon_array_functions.cxx:171-266) of y by A x + a
     const float den = ax + av;
     float r;
@@ -33,9 +33,10 @@ __device__ __forceinline__ void forward_store(const ProjParams& p, int seg, int 
     } else {
       r = y / den;
     }
-    if (EPI == kEpiGradient) r -= zend ? 0.f : (ep.mult ? __ldg(ep.mult + idx) : 1.f);
+    if (EPI == kEpiGradient || EPI == kEpiLoglikRatio) r -= zend ? 0.f : (ep.mult ? __ldg(ep.mult + idx) : 1.f);
     out[idx] = r;
-  } else {
+  }
+  if (EPI == kEpiLoglik || EPI == kEpiLoglikRatio) {
     // accumulate_loglikelihood (recon_array_functions.cxx:335-377) of ybar = (A x + a) * m
     float e = ax + av;
     if (zend)
@@ -44,7 +45,7 @@ __device__ __forceinline__ void forward_store(const ProjParams& p, int seg, int 
       e *= __ldg(ep.mult + idx);
     const float ne = fmaxf(e, y / 10000.F);
     ll += (y <= sv) ? -static_cast<double>(ne) : y * log(static_cast<double>(ne)) - static_cast<double>(ne);
-    if (out) out[idx] = e;
+    if (EPI == kEpiLoglik && out) out[idx] = e;
   }
 }
 

@@ -102,10 +102,12 @@ constexpr int kPackedMaxNax = 16;
 //   kEpiLoglik: accumulate the Poisson log-likelihood of y given (A x + a) m in FP64, per CTA.
 //   kEpiGradient: store divide_and_truncate(y, A x + a) - m (m = mult or 1): back-projected, the gradient of
 //                the log-likelihood (RPC_process_related_viewgrams_gradient<false>, ...AndProjData.cxx:1462-1477).
+//   kEpiLoglikRatio: both kEpiLoglik (the partial sums) and kEpiGradient (the stored ratio) from one projection.
 constexpr int kEpiNone = 0;
 constexpr int kEpiRatio = 1;
 constexpr int kEpiLoglik = 2;
 constexpr int kEpiGradient = 3;
+constexpr int kEpiLoglikRatio = 4;
 struct FwdEpilogue {
   int mode;
   int zero_ends;               // zero the first/last axial position of segment 0

@@ -735,16 +735,16 @@ __global__ void __launch_bounds__(kPathThreads, kPathMinCtas)
   unsigned phase = 0;
   if (!forward_path_item<NPA, EPI>(p, pp, it, smem, img, out, ep, ll, ncancel, &bar, phase)) {
     // abandoned (the status word says so): the item's log-likelihood partial is NaN rather than stale
-    if (EPI == kEpiLoglik && threadIdx.x == 0)
+    if ((EPI == kEpiLoglik || EPI == kEpiLoglikRatio) && threadIdx.x == 0)
       ep.partials[static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x] = __longlong_as_double(-1ll);
     return;
   }
-  if (EPI == kEpiRatio || EPI == kEpiGradient) {
+  if (EPI == kEpiRatio || EPI == kEpiGradient || EPI == kEpiLoglikRatio) {
     // cancelled singularities (distributable.cxx:590-594)
     for (int o = 16; o > 0; o >>= 1) ncancel += __shfl_xor_sync(0xffffffffu, ncancel, o);
     if ((threadIdx.x & 31) == 0 && ncancel && ep.cancelled) atomicAdd(ep.cancelled, ncancel);
   }
-  if (EPI == kEpiLoglik) {
+  if (EPI == kEpiLoglik || EPI == kEpiLoglikRatio) {
     // per-CTA partial sums, reduced in a fixed order by the caller: deterministic
     __shared__ double red[kPathWarps];
     for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
@@ -922,6 +922,9 @@ cudaError_t launch_forward_paths_batch(const ProjParams& p, const PathParams& pp
     case kEpiLoglik:
       return launch_forward_paths_epi<kEpiLoglik>(p, pp, items, nitems, images, img_stride, projdata, pd_stride, batch,
                                                   st, e);
+    case kEpiLoglikRatio:
+      return launch_forward_paths_epi<kEpiLoglikRatio>(p, pp, items, nitems, images, img_stride, projdata, pd_stride,
+                                                       batch, st, e);
     default: return cudaErrorInvalidValue;
   }
 }

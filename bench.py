@@ -340,9 +340,9 @@ def autograd_workload(device, batch=8):
             total += float(loss)
         return total
 
-    ms_b = time_dev(batched, warm=2, reps=3)
-    ms_rc = time_dev(lambda: batched(L_rc), warm=1, reps=3)
-    ms_1 = time_dev(one_by_one, warm=1, reps=3)
+    ms_b = time_dev(batched, warm=2, reps=5)
+    ms_rc = time_dev(lambda: batched(L_rc), warm=2, reps=5)
+    ms_1 = time_dev(one_by_one, warm=2, reps=5)
     v_b, v_1 = batched(), one_by_one()
     res = {"metric": "differentiable projector loss+gradient steps/s", "value": 1e3 / ms_b, "unit": "steps/s",
            "ms_per_step": ms_b, "images_per_s": batch * 1e3 / ms_b, "one_launch_per_image_ms": ms_1,

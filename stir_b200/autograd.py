@@ -121,8 +121,10 @@ def _data_strides(proj, B, y, additive, mult):
 
 
 def _ratio_fits(proj, B, device):
-    """Whether B gradient ratios (projection data of each image) fit in the free device memory with room to spare."""
+    """Whether B gradient ratios (projection data of each image) fit in the free device memory with room to spare:
+    the driver's free memory plus what torch's caching allocator holds unused."""
     free, _ = torch.cuda.mem_get_info(device)
+    free += torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
     need = 4 * B * proj.projdata_size
     return need + need // 4 + (512 << 20) <= free
 

@@ -89,6 +89,8 @@ struct b200rt_projector {
   DevBuf<ProjBinDev> bins;
   DevBuf<LineDev> lines;
   DevBuf<SegDev> segs;
+  // per segment of the whole data: STIR-order offset, device-layout offset, axial positions (layout changes)
+  DevBuf<int64_t> layout_tab;
   ProjParams params{};
   // host copies
   std::vector<ProjBinDev> h_bins;
@@ -195,8 +197,8 @@ void back_project_into(b200rt_projector& h, const float* pd, float* image, int s
                        cudaStream_t st, float max_abs = 0.f);
 int check_subset(b200rt_projector* h, int subset, int nsub);
 void ensure_colmax(b200rt_projector& h, float* scratch, cudaStream_t st);
-cudaError_t projdata_layout(const Geometry& g, const float* in, float* out, bool to_dev, cudaStream_t st);
-cudaError_t projdata_layout_views(const Geometry& g, const float* in, float* out, bool to_dev, int v0, int v1,
+cudaError_t projdata_layout(const b200rt_projector& h, const float* in, float* out, bool to_dev, cudaStream_t st);
+cudaError_t projdata_layout_views(const b200rt_projector& h, const float* in, float* out, bool to_dev, int v0, int v1,
                                   cudaStream_t st);
 cudaError_t copy_views(const Geometry& g, float* dst, const float* src, int v0, int v1, cudaMemcpyKind kind,
                        cudaStream_t st);

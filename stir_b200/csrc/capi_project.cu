@@ -149,7 +149,7 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
           ck(launch_forward_paths(h->params, h->pparams, vg.list->p + vg.off[gi], n, h->st_img_b.p, h->st_pd_b.p, st,
                                   nullptr),
              "forward projection");
-        ck(projdata_layout_views(g, h->st_pd_b.p, h->st_pd_a.p, false, vg.v0[gi], vg.v0[gi + 1], st), "layout");
+        ck(projdata_layout_views(*h, h->st_pd_b.p, h->st_pd_a.p, false, vg.v0[gi], vg.v0[gi + 1], st), "layout");
         ck(cudaEventRecord(h->copy_events[gi], st), "cudaEventRecord");
         ck(cudaStreamWaitEvent(h->copy_stream, h->copy_events[gi], 0), "cudaStreamWaitEvent");
         ck(copy_views(g, projdata_host, h->st_pd_a.p, vg.v0[gi], vg.v0[gi + 1], cudaMemcpyDeviceToHost, h->copy_stream),
@@ -160,7 +160,7 @@ int b200rt_forward_project(b200rt_projector* h, const float* image_host, float* 
       return B200RT_OK;
     }
     forward_subset(*h, h->st_img_b.p, h->st_pd_b.p, subset_num, num_subsets, st);
-    ck(projdata_layout(g, h->st_pd_b.p, h->st_pd_a.p, false, st), "layout");
+    ck(projdata_layout(*h, h->st_pd_b.p, h->st_pd_a.p, false, st), "layout");
     ck(cudaMemcpyAsync(projdata_host, h->st_pd_a.p, sizeof(float) * g.projdata_size(), cudaMemcpyDeviceToHost, st), "D2H");
     ck(cudaStreamSynchronize(st), "forward projection");
     return B200RT_OK;
@@ -200,7 +200,7 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
       ck(cudaMemsetAsync(h->st_img_b.p, 0, sizeof(float) * g.image_size(), st), "memset");
       for (size_t gi = 0; gi < G; ++gi) {
         ck(cudaStreamWaitEvent(st, h->copy_events[gi], 0), "cudaStreamWaitEvent");
-        ck(projdata_layout_views(g, h->st_pd_a.p, h->st_pd_b.p, true, vg.v0[gi], vg.v0[gi + 1], st), "layout");
+        ck(projdata_layout_views(*h, h->st_pd_a.p, h->st_pd_b.p, true, vg.v0[gi], vg.v0[gi + 1], st), "layout");
         const int n = vg.off[gi + 1] - vg.off[gi];
         if (n > 0)
           ck(launch_back_paths_atomic(h->params, h->pparams, vg.list->p + vg.off[gi], n, h->st_pd_b.p, h->st_img_b.p,
@@ -210,7 +210,7 @@ int b200rt_back_project(b200rt_projector* h, const float* projdata_host, float* 
     } else {
       ck(cudaMemcpyAsync(h->st_pd_a.p, projdata_host, sizeof(float) * g.projdata_size(), cudaMemcpyHostToDevice, st),
          "H2D");
-      ck(projdata_layout(g, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
+      ck(projdata_layout(*h, h->st_pd_a.p, h->st_pd_b.p, true, st), "layout");
       back_project_into(*h, h->st_pd_b.p, h->st_img_b.p, subset_num, num_subsets, mode, 0, st);
     }
     ck(launch_image_from_dev(h->st_img_b.p, h->st_img_a.p, g.desc().nz, g.desc().ny, g.desc().nx, st), "layout");

@@ -555,6 +555,13 @@ void setup_projector(b200rt_projector& h) {
   }
   h.segs.upload(sd, h.stream);
   h.h_segs_full = sd;
+  std::vector<int64_t> lt;
+  for (int s = -g.S(); s <= g.S(); ++s) {
+    lt.push_back(g.stir_segment_offset(s));
+    lt.push_back(g.dev_segment_offset(s));
+    lt.push_back(g.nax(s));
+  }
+  h.layout_tab.upload(lt, h.stream);
 
   ProjParams& p = h.params;
   p.rows = h.rows.p;
@@ -842,34 +849,27 @@ int check_subset(b200rt_projector* h, int subset, int nsub) {
   return B200RT_OK;
 }
 
-cudaError_t projdata_layout(const Geometry& g, const float* in, float* out, bool to_dev, cudaStream_t st) {
-  const int64_t nvt = static_cast<int64_t>(g.num_views()) * g.num_tang();
-  for (int k = 0; k < g.num_tof(); ++k)
-    for (int s = -g.S(); s <= g.S(); ++s) {
-      const int64_t so = k * g.tof_stride() + g.stir_segment_offset(s);
-      const int64_t dv = k * g.tof_stride() + g.dev_segment_offset(s);
-      const cudaError_t e = to_dev ? launch_projdata_to_dev(in + so, out + dv, g.nax(s), nvt, st)
-                                   : launch_projdata_from_dev(in + dv, out + so, g.nax(s), nvt, st);
-      if (e != cudaSuccess) return e;
-    }
-  return cudaSuccess;
+int max_nax(const Geometry& g) {
+  int m = 0;
+  for (int s = -g.S(); s <= g.S(); ++s) m = std::max(m, g.nax(s));
+  return m;
 }
 
-// projection data layout change of the views [v0, v1) only (STIR order <-> device layout)
-cudaError_t projdata_layout_views(const Geometry& g, const float* in, float* out, bool to_dev, int v0, int v1,
+cudaError_t projdata_layout(const b200rt_projector& h, const float* in, float* out, bool to_dev, cudaStream_t st) {
+  const Geometry& g = *h.geo;
+  return launch_projdata_layout_views(in, out, h.layout_tab.p, 2 * g.S() + 1, g.num_tof(), max_nax(g), g.tof_stride(),
+                                      static_cast<int64_t>(g.num_views()) * g.num_tang(), 0,
+                                      static_cast<int64_t>(g.num_views()) * g.num_tang(), to_dev, st);
+}
+
+// projection data layout change of the views [v0, v1) only (STIR order <-> device layout): one launch over every
+// (timing bin, segment)
+cudaError_t projdata_layout_views(const b200rt_projector& h, const float* in, float* out, bool to_dev, int v0, int v1,
                                   cudaStream_t st) {
-  const int64_t nt = g.num_tang(), nvt = static_cast<int64_t>(g.num_views()) * nt;
-  const int64_t c0 = v0 * nt, nc = (v1 - v0) * nt;
-  for (int k = 0; k < g.num_tof(); ++k)
-    for (int s = -g.S(); s <= g.S(); ++s) {
-      const int64_t so = k * g.tof_stride() + g.stir_segment_offset(s) + c0;
-      const int64_t dv = k * g.tof_stride() + g.dev_segment_offset(s) + c0 * g.nax(s);
-      const int nax = g.nax(s);
-      const cudaError_t e = to_dev ? launch_transpose(in + so, out + dv, nax, nc, nvt, nax, st)
-                                   : launch_transpose(in + dv, out + so, static_cast<int>(nc), nax, nax, nvt, st);
-      if (e != cudaSuccess) return e;
-    }
-  return cudaSuccess;
+  const Geometry& g = *h.geo;
+  const int64_t nt = g.num_tang();
+  return launch_projdata_layout_views(in, out, h.layout_tab.p, 2 * g.S() + 1, g.num_tof(), max_nax(g), g.tof_stride(),
+                                      static_cast<int64_t>(g.num_views()) * nt, v0 * nt, (v1 - v0) * nt, to_dev, st);
 }
 
 // copy of the views [v0, v1) of projection data in STIR order (rows of views x tangential positions for every
@@ -1171,14 +1171,14 @@ int b200rt_projdata_to_device_layout(b200rt_projector* h, const float* stir_dev,
   if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_to_device_layout");
   if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(h->device);
-  const cudaError_t e = projdata_layout(*h->geo, stir_dev, dev, true, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = projdata_layout(*h, stir_dev, dev, true, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
 }
 int b200rt_projdata_from_device_layout(b200rt_projector* h, const float* dev, float* stir_dev, void* stream) {
   if (h && sharded(*h)) return refuse_shard(h, "b200rt_projdata_from_device_layout");
   if (!h || !stir_dev || !dev) return B200RT_ERR_INVALID_ARGUMENT;
   DeviceGuard dg(h->device);
-  const cudaError_t e = projdata_layout(*h->geo, dev, stir_dev, false, static_cast<cudaStream_t>(stream));
+  const cudaError_t e = projdata_layout(*h, dev, stir_dev, false, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? B200RT_OK : fail(h, B200RT_ERR_CUDA, cudaGetErrorString(e));
 }
 

@@ -409,6 +409,11 @@ cudaError_t launch_gibbs_hessian_voxel(const GibbsDev& g, const float* x, int z,
 cudaError_t launch_gibbs_gradient_cuda(const GibbsDev& g, const float* x, float* out, cudaStream_t st);
 
 // out[c * ld_out + r] = in[r * ld_in + c], r < rows, c < cols
+// STIR order <-> device layout of the columns [c0, c0 + nc) (views x tangential positions) of every (timing bin,
+// segment) of projection data, in one launch; tab: per segment (STIR offset, device offset, axial positions)
+cudaError_t launch_projdata_layout_views(const float* in, float* out, const int64_t* tab, int nsegs, int ntof,
+                                         int max_nax, int64_t tof_stride, int64_t nvt, int64_t c0, int64_t nc,
+                                         bool to_dev, cudaStream_t st);
 cudaError_t launch_transpose(const float* in, float* out, int rows, int64_t cols, int64_t ld_in, int64_t ld_out,
                              cudaStream_t st);
 

@@ -584,6 +584,35 @@ __global__ void transpose_kernel(const float* __restrict__ in, float* __restrict
   }
 }
 
+// the layout change of columns [c0, c0 + nc) of every (timing bin, segment): blockIdx.z = timing bin x segment; the
+// same 32 x 32 tiles as transpose_kernel (STIR order: rows = axial positions, columns = views x tangential
+// positions, leading dimension nvt; device layout: rows = views x tangential, columns = axial positions)
+__global__ void projdata_layout_kernel(const float* __restrict__ in, float* __restrict__ out, const int64_t* __restrict__ tab,
+                                       int nsegs, int64_t tof_stride, int64_t nvt, int64_t c0, int64_t nc, int to_dev) {
+  __shared__ float tile[32][33];
+  const int k = blockIdx.z / nsegs, si = blockIdx.z % nsegs;
+  const int nax = static_cast<int>(tab[3 * si + 2]);
+  const int64_t so = k * tof_stride + tab[3 * si] + c0;
+  const int64_t dv = k * tof_stride + tab[3 * si + 1] + c0 * nax;
+  // rows x cols of the input, and its leading dimensions in and out
+  const int64_t rows = to_dev ? nax : nc, cols = to_dev ? nc : nax;
+  const int64_t ld_in = to_dev ? nvt : nax, ld_out = to_dev ? nax : nvt;
+  const float* src = in + (to_dev ? so : dv);
+  float* dst = out + (to_dev ? dv : so);
+  const int64_t cb = static_cast<int64_t>(blockIdx.x) * 32, rb = static_cast<int64_t>(blockIdx.y) * 32;
+  if (cb >= cols || rb >= rows) return;  // a tile past this segment's extent
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t r = rb + i, c = cb + tx;
+    if (r < rows && c < cols) tile[i][tx] = src[r * ld_in + c];
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t c = cb + i, r = rb + tx;
+    if (r < rows && c < cols) dst[c * ld_out + r] = tile[tx][i];
+  }
+}
+
 cudaError_t transpose(const float* in, float* out, int rows, int64_t cols, cudaStream_t st) {
   return launch_transpose(in, out, rows, cols, cols, rows, st);
 }
@@ -1126,6 +1155,20 @@ cudaError_t launch_projdata_to_dev(const float* stir, float* dev, int nax, int64
 }
 cudaError_t launch_projdata_from_dev(const float* dev, float* stir, int nax, int64_t nvt, cudaStream_t st) {
   return transpose(dev, stir, static_cast<int>(nvt), nax, st);
+}
+
+cudaError_t launch_projdata_layout_views(const float* in, float* out, const int64_t* tab, int nsegs, int ntof,
+                                         int max_nax, int64_t tof_stride, int64_t nvt, int64_t c0, int64_t nc,
+                                         bool to_dev, cudaStream_t st) {
+  if (nc <= 0 || nsegs <= 0 || ntof <= 0 || max_nax <= 0) return cudaSuccess;
+  // the grid covers the segment with the most axial positions; tiles past a smaller segment's extent return at once
+  const int64_t rows = to_dev ? max_nax : nc, cols = to_dev ? nc : max_nax;
+  const int64_t gx = (cols + 31) / 32, gy = (rows + 31) / 32;
+  const int64_t gz = static_cast<int64_t>(nsegs) * ntof;
+  if (gy > 65535 || gz > 65535 || gx > 2147483647LL) return cudaErrorInvalidValue;
+  projdata_layout_kernel<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy), static_cast<unsigned>(gz)),
+                           dim3(32, 8), 0, st>>>(in, out, tab, nsegs, tof_stride, nvt, c0, nc, to_dev ? 1 : 0);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_transpose(const float* in, float* out, int rows, int64_t cols, int64_t ld_in, int64_t ld_out,

@@ -202,6 +202,8 @@ void batch_finalize(b200rt_batch& b) {
     b.max_f[B200RT_BATCH_KERNELS_BASIC_BINS] = b200::batch_max_ctas_per_sm(b.npa, b.smem, true);
     b.max_b[B200RT_BATCH_KERNELS_BASIC_BINS] = b200::batch_max_ctas_per_sm(b.npa, b.smem, false);
   }
+  for (int f = B200RT_BATCH_KERNELS_PATHS; f <= B200RT_BATCH_KERNELS_BASIC_BINS; ++f)  // a family that does not fit
+    if (b.avail[f] && (b.max_f[f] < 1 || b.max_b[f] < 1)) b.avail[f] = false;      // an SM is not offered
   use_family(b, b.cfg.kernels);
   ck(cudaStreamSynchronize(st), "batch set-up");
   b.ready = true;

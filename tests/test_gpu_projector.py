@@ -230,3 +230,23 @@ def test_host_api_matches_device_api(which, subset, small, rpt):
     _abi.check(proj.lib.b200rt_back_project(proj.h, ctypes.c_void_p(y_pin.data_ptr()), ctypes.c_void_p(b_pin.data_ptr()),
                                             *subset, _abi.BACKPROJECT_ATOMIC), proj.h, "back")
     assert rel_l2(b_pin.numpy(), bd) < 1e-6
+
+
+def test_intrinsic_tilt_and_depth_of_interaction(cuda_device, oracle_lib):
+    """A scanner with an intrinsic azimuthal tilt (views start at phi = tilt: STIR then disables the 90- and
+    180-degree symmetries, DataSymmetriesForBins_PET_CartesianGrid.cxx:302-360) and a non-zero average depth of
+    interaction: forward and back projection of a subset against the oracle, and the symmetries used."""
+    import dataclasses
+    from stir_b200.projectors import RayTracingProjector
+    pdi, img = G.small_3d_pet()
+    sc = dataclasses.replace(pdi.scanner, intrinsic_tilt=0.05, average_depth_of_interaction=7.0)
+    pdi = dataclasses.replace(pdi, scanner=sc)
+    proj = RayTracingProjector(pdi, img, device=cuda_device)
+    orc = oracle_lib.Oracle(proj.geometry)
+    assert proj.info.symmetries_used == orc.symmetries_used
+    assert not (proj.info.symmetries_used & 3)  # no 90 / 180 degree symmetry
+    x = np.random.default_rng(21).uniform(0, 1, img.shape).astype(np.float32)
+    assert rel_l2(proj.forward_host(x, 1, 3), orc.forward(x, 1, 3)) <= 1e-5
+    y = np.random.default_rng(22).uniform(0, 1, proj.projdata_size).astype(np.float32)
+    assert rel_l2(proj.back_host(y, 1, 3), orc.back(y, 1, 3)) <= 1e-5
+    proj.close()

@@ -99,6 +99,17 @@ __device__ __forceinline__ void unit_range(const PathParams& pp, const PathLineS
 
 __device__ __forceinline__ int log2_parts(int P) { return P == 2 ? 1 : (P == 4 ? 2 : 3); }
 
+// a * b + c on two float lanes at once (sm_100's packed FP32 FMA): each lane rounds as fmaf does
+__device__ __forceinline__ void fma2(float& c0, float& c1, float a0, float a1, float b0, float b1) {
+  unsigned long long r;
+  const unsigned long long a = (static_cast<unsigned long long>(__float_as_uint(a1)) << 32) | __float_as_uint(a0);
+  const unsigned long long b = (static_cast<unsigned long long>(__float_as_uint(b1)) << 32) | __float_as_uint(b0);
+  const unsigned long long c = (static_cast<unsigned long long>(__float_as_uint(c1)) << 32) | __float_as_uint(c0);
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  c0 = __uint_as_float(static_cast<unsigned>(r));
+  c1 = __uint_as_float(static_cast<unsigned>(r >> 32));
+}
+
 // 4-byte asynchronous copy global -> shared (completed by cp_async_wait)
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -160,8 +171,10 @@ __device__ __forceinline__ void padded_fma(const float* cols, uint32_t idx, floa
   const float* q2 = cols + ((static_cast<int>(idx) >> 16) + zo0);
 #pragma unroll
   for (int j = 0; j < NJ; ++j) {
-    acc1[j] += q1[j * 32 * npa] * v;
-    if (TWO) acc2[j] += q2[j * 32 * npa] * v;
+    if (TWO)
+      fma2(acc1[j], acc2[j], q1[j * 32 * npa], q2[j * 32 * npa], v, v);  // both lines' sums in one instruction
+    else
+      acc1[j] += q1[j * 32 * npa] * v;
   }
 }
 

@@ -845,8 +845,9 @@ def b200_main(args):
     bk3 = proj.back_dev(y, mode=_abi.BACKPROJECT_DETERMINISTIC)
     deterministic = {"back_ms": det_ms, "atomic_back_ms": back_ms, "bit_identical_across_runs": bool(torch.equal(bk2, bk3)),
                      "rel_l2_vs_atomic": float((bk2 - bk).double().norm() / bk.double().norm()),
-                     "method": "each contribution rounded to a 64-bit fixed-point integer (scale from the data's bound "
-                               "and the largest column sum), integers added atomically, converted once"}
+                     "method": "each item's contributions to a voxel summed in float in a fixed order, the sum rounded "
+                               "to a 64-bit fixed-point integer (scale from the data's bound and the largest column "
+                               "sum), integers added atomically, converted once"}
     del bk2, bk3
 
     cpu = None

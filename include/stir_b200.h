@@ -52,8 +52,8 @@ extern "C" {
 
 /* back-projection accumulation modes */
 #define B200RT_BACKPROJECT_ATOMIC 0        /* scatter with float atomics (fast; order-dependent rounding)  */
-#define B200RT_BACKPROJECT_DETERMINISTIC 1 /* contributions summed as 64-bit fixed point: order-independent,
-                                              bit-identical from run to run */
+#define B200RT_BACKPROJECT_DETERMINISTIC 1 /* fixed-order float sums per work item, combined as 64-bit fixed
+                                              point: order-independent, bit-identical from run to run */
 
 /* attenuation modes (BinNormalisationFromAttenuationImage.cxx:138-170) */
 #define B200RT_ATTENUATION_FACTORS 0 /* projdata = undo of ones: 1 / exp(A mu), the multiplicative factors */

@@ -141,9 +141,11 @@ class _LogLikelihood(torch.autograd.Function):
         keep = ctx.needs_input_grad[0] and proj.info.num_tof_bins <= 1 and \
             (store_ratio if store_ratio is not None else _ratio_fits(proj, B, x.device))
         if keep:
-            # value and gradient ratios from one projection (bins outside the subset are never read back)
+            # value and gradient ratios from one projection; zeros where none is written (bins outside the subset and
+            # of inactive lines), as in the projection the backward would otherwise make: the deterministic back
+            # projection takes its fixed-point scale from the largest |value| of the whole array
             n_pd = proj.projdata_size
-            ratio = torch.empty((B, n_pd), dtype=torch.float32, device=x.device)
+            ratio = torch.zeros((B, n_pd), dtype=torch.float32, device=x.device)
             st = proj.lib.b200rt_log_likelihood_and_ratio_batch_dev(
                 proj.h, _p(xs), n_img, _p(yy), ys, _p(aa), as_, _p(mm), ms, B, subset_num, num_subsets, int(zero_ends),
                 values, _p(ratio), n_pd, _stream_ptr(None))

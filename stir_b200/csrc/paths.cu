@@ -18,8 +18,9 @@
 //     scatter: no shared-memory atomics, and a fixed order within the item).
 //
 // Sums are taken in path order rather than in the stored row order of ProjMatrixElemsForOneBin, so the
-// results differ from the per-basic-bin kernels by float rounding only; the fixed-point back projection
-// gives the same integers (each contribution is rounded the same way, integer addition is associative).
+// results differ from the per-basic-bin kernels by float rounding only.  The fixed-point back projection sums
+// each item's contributions to a voxel in float in a fixed order and adds the rounded sums as integers, so its
+// image does not depend on the order of the items (the per-basic-bin kernels round every contribution instead).
 #include "internal.hpp"
 #include "epilogue.cuh"
 
@@ -474,7 +475,7 @@ struct FloatCols {
   }
 };
 struct FixedCols {
-  using T = long long;
+  using T = float;
   unsigned long long* acc;
   const double* scale_ptr;  // 2^k of the fixed-point format, computed on the device
   double scale;
@@ -484,12 +485,13 @@ struct FixedCols {
     scale_f = static_cast<float>(scale);
   }
   __device__ __forceinline__ void offset(int64_t) {}  // one image per launch
-  // the same rounding of each contribution as the per-basic-bin fixed-point kernel: the scale is a power of two of
-  // at most 2^126 and |v| x scale <= 2^62, so v x scale is exact in float as in double and rounds to the same
-  // integer, without the double multiply
-  __device__ __forceinline__ T term(float v) const { return __float2ll_rn(v * scale_f); }
-  __device__ __forceinline__ void flush(int64_t i, long long v) const {
-    if (v != 0) atomicAdd(acc + i, static_cast<unsigned long long>(v));
+  // An item's contributions to a voxel are summed in float in a fixed order (the elements of the voxel's column in
+  // the item, one warp per column), and the sum is rounded once to the fixed-point grid and added as a 64-bit
+  // integer: integer addition is associative, so the image does not depend on the order of the items.  The scale
+  // is a power of two of at most 2^126 and every partial sum times it is at most 2^62, so the product is exact.
+  __device__ __forceinline__ T term(float v) const { return v; }
+  __device__ __forceinline__ void flush(int64_t i, float v) const {
+    if (v != 0.f) atomicAdd(acc + i, static_cast<unsigned long long>(__float2ll_rn(v * scale_f)));
   }
 };
 

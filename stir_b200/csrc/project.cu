@@ -630,7 +630,7 @@ size_t proj_smem_bytes(int max_row_len) {
 // elements in shared memory) from registers.  Forward: each (line, axial position, timing bin) sum adds the same
 // products in the same order as the TOF row (elements outside the TOF row have weight 0 and add +-0), so the
 // results are bit-identical.  Back: the contributions of the group's timing bins to a voxel are summed before the
-// one atomic (float), or rounded one by one and summed as integers (fixed point: the same integers).
+// one atomic (float), or, in fixed point, summed in float in that fixed order and rounded once to an integer.
 constexpr int kTofWarps = 4;
 constexpr int kTofMinCtas = 8;  // 64 registers: 32 warps per SM (79 registers left 24)
 constexpr int kTofGroupMax = 32;  // timing bins per pass: KG in {8, 16, 20, 24, 32}, chosen from their number
@@ -753,13 +753,15 @@ struct TofFloatSum {
     if (v != 0.f) atomicAdd(img + i, v);
   }
 };
+// the group's contributions to a voxel summed in float in a fixed order (the timing bins of the group), the sum
+// rounded once to the fixed-point grid (a power-of-two scale: exact) and added as a 64-bit integer
 struct TofFixedSum {
   unsigned long long* acc;
-  double scale;
-  using T = long long;
-  __device__ __forceinline__ T term(float v) const { return __double2ll_rn(static_cast<double>(v) * scale); }
+  float scale;
+  using T = float;
+  __device__ __forceinline__ T term(float v) const { return v; }
   __device__ __forceinline__ void flush(int64_t i, T v) const {
-    if (v != 0) atomicAdd(acc + i, static_cast<unsigned long long>(v));
+    if (v != 0.f) atomicAdd(acc + i, static_cast<unsigned long long>(__float2ll_rn(v * scale)));
   }
 };
 
@@ -826,7 +828,7 @@ __global__ void __launch_bounds__(kTofWarps * 32, kTofMinCtas) back_tof_grouped_
   const int bi = blockIdx.x * kTofWarps + warp;
   if (bi >= nitems) return;
   Sum o = out;
-  if constexpr (std::is_same<Sum, TofFixedSum>::value) o.scale = *scale;
+  if constexpr (std::is_same<Sum, TofFixedSum>::value) o.scale = static_cast<float>(*scale);
   back_tof_grouped_body<KG, Sum>(p, p.tof_basic[items[bi]], stage[warp], pd, o, zero_ends, lane);
 }
 
@@ -1095,7 +1097,7 @@ cudaError_t launch_back_tof_grouped(const ProjParams& p, const int* items, int n
   const int grid = (nitems + kTofWarps - 1) / kTofWarps;
   if (acc) {
     TOF_KG_SWITCH(p.num_tof, (back_tof_grouped_kernel<KG, TofFixedSum><<<grid, kTofWarps * 32, 0, st>>>(
-                                 p, items, nitems, projdata, TofFixedSum{acc, 0.0}, scale, zero_ends)));
+                                 p, items, nitems, projdata, TofFixedSum{acc, 0.f}, scale, zero_ends)));
   } else {
     TOF_KG_SWITCH(p.num_tof, (back_tof_grouped_kernel<KG, TofFloatSum><<<grid, kTofWarps * 32, 0, st>>>(
                                  p, items, nitems, projdata, TofFloatSum{image}, scale, zero_ends)));

@@ -48,3 +48,16 @@ def test_null_arguments_are_rejected_without_touching_the_gpu():
     assert lib.b200rt_forward_project_dev(None, None, None, 0, 1, None) == _abi.ERR_INVALID_ARGUMENT
     assert lib.b200rt_get_info(None, None) == _abi.ERR_INVALID_ARGUMENT
     lib.b200rt_destroy(None)
+
+
+def test_python_constants_match_header():
+    """Every B200RT_* constant the header defines that the Python binding mirrors (same name without the prefix)
+    has the same value there."""
+    src = open(os.path.join(ROOT, "include", "stir_b200.h")).read()
+    defines = dict(re.findall(r"^#define B200RT_([A-Z0-9_]+)\s+\(?(-?\d+)u?\)?", src, flags=re.M))
+    checked = 0
+    for name, value in defines.items():
+        if hasattr(_abi, name):
+            assert getattr(_abi, name) == int(value), name
+            checked += 1
+    assert checked >= 20

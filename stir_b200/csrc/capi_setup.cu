@@ -144,7 +144,12 @@ void build_paths(b200rt_projector& h, const std::vector<RowElem>& hr, const std:
   // the forward needs no per-lane range tests (a cap keeps the staging buffer small, and at most 2048 planes
   // per staged column keep every staged index within the 16 bits the padded kernels store it in)
   const int zpad = over <= 64 && nz + ((over + 3) & ~3) <= 2048 ? (over + 3) & ~3 : -1;
-  const int K = std::max(8, 32768 / (4 * (nz + std::max(zpad, 0))));  // 32 KB of staged float columns
+  // 34.25 KB of staged float columns: on the clinical geometry (nz 127, padding 24 planes) K = 58, the largest chunk
+  // with which 4 forward CTAs still fit on an SM.  Forward projection of all its bins, measured: K 40 11.17 ms, 47
+  // 10.22, 54 9.55, 58 9.20 (4 CTAs per SM); 61 9.01, 66-74 10.41-9.87, 81 9.51 (3 CTAs per SM; the batched
+  // persistent forward then loses a quarter of its CTAs: dynamic OSEM 26.8 -> 24.6 frames/s at K 61); 94-135
+  // 11.4-12.2 (2 CTAs per SM); 162 19.5 (1 CTA per SM)
+  const int K = std::max(8, 35072 / (4 * (nz + std::max(zpad, 0))));
   // chunk c of a row covers its elements with slot in [c K, (c + 1) K)
   for (Group& G : groups) {
     const int ncols = static_cast<int>(G.cols.size());
